@@ -1,0 +1,470 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FX-correlation path on the full-rate plain workload:
+1024 Msps, 2-bit, FFT 8192, a 10-s scan (10 sectors x 125000 frame pairs),
+seeded non-identity 32-bit shuffle, station 1 LSB / station 2 USB with band
+centres 16 MHz apart, geometric delay with a 0.5 Hz fringe rate, residual
+delay 0.3 samples and residual rate 0.01 Hz, products ACF x2 + XCF.
+
+A step is one pass of the hot path over the whole 10-s scan.  Prints one JSON
+line (rank 0).  `--impl reference` times the CPU restatement of the
+reference's rayon path (oracle/fxc_oracle.c, OpenMP over all host threads)
+on a bounded sample of the same workload instead.
+
+Multi-GPU (torchrun, N ranks): the path does not shard within a scan, so each
+rank correlates its own replica scan (weak scaling, no data-path collective);
+timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "fx-corr_b200"))
+
+# ---------------------------------------------------------------- workload
+
+N = 8192
+FS = 1024e6
+BITS = 2
+SCAN_S = 10
+SECTORS = 10
+NF_SECTOR = int(FS / N)  # 125000 frames per 1-s sector
+LEVELS = [-3.0, -1.0, 1.0, 3.0]
+OBS_MHZ = 8400.0
+ROT1_HZ, ROT2_HZ = 0.0, 16e6
+RHO = 0.05
+WORKLOAD = ("full-rate plain scan: 1024 Msps, 2-bit, FFT 8192, 10 s (10 sectors x 125000 frame "
+            "pairs), generic shuffle, ant1 LSB / ant2 USB, 16 MHz band offset, ACFx2+XCF")
+
+
+def shuffle_internal(seed: int):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    while True:
+        p = [int(v) for v in rng.permutation(32)]
+        if p != list(range(32)) and p != [i ^ 1 for i in range(32)]:
+            return p
+
+
+def scan_config(fxc):
+    """Resolve the scan the way run_once does (src/main.rs:1186-1212,
+    1317-1328, 1618-1673) for the synthetic schedule above."""
+    bw = FS / 2e6
+    c1 = OBS_MHZ + ROT1_HZ / 1e6 + 0.5 * bw
+    c2 = OBS_MHZ + ROT2_HZ / 1e6 + 0.5 * bw
+    band = fxc.band_alignment(N, FS, c1, c2, bw, bw)
+    grid = 0 if abs(ROT1_HZ) <= abs(ROT2_HZ) else 1
+    df = FS / N
+    rot_residual = (ROT1_HZ - ROT2_HZ) - band[0] * df
+    rate_user = 0.01  # --resrate
+    extra_rate = (-rot_residual + rate_user) / (OBS_MHZ * 1e6)
+    gr = -0.5 / (OBS_MHZ * 1e6)  # geometric rate giving a 0.5 Hz fringe at obs freq
+    gd0 = 2.1e-7
+    table = gd0 + gr * np.arange(SCAN_S + 1, dtype=np.float64)
+    user = 0.3  # --resdelay
+    net_d0 = gd0 + user / FS
+    init = int(round(net_d0 * FS))
+    start2 = max(init, 0)
+    spw = 32 // BITS
+    d_seek = ((start2 // spw) * spw - 0) / FS
+    delay = dict(time_offset_s=0.0, delay_user_samples=user, extra_delay_rate_sps=extra_rate,
+                 d_seek=d_seek, lo1_hz=(OBS_MHZ + ROT1_HZ / 1e6) * 1e6,
+                 lo2_hz=(OBS_MHZ + ROT2_HZ / 1e6) * 1e6)
+    return fxc.ScanConfig(fft=N, fs=FS, bits1=BITS, bits2=BITS, levels1=LEVELS, levels2=LEVELS,
+                          shuffle1=shuffle_internal(101), shuffle2=shuffle_internal(102),
+                          lsb1=True, lsb2=False, band=tuple(band), grid=grid,
+                          products=fxc.PROD_ACF | fxc.PROD_XCF, delay=delay, geom_table=table)
+
+
+def gen_station_pair_gpu(torch, nsamp, seed, cfg, lag=7):
+    """Seeded quantised Gaussian streams (+-0.98 sigma thresholds, levels
+    +-1/+-3) sharing a common component at rho=0.05, station 2 lagging by
+    `lag` samples, packed into the .raw layout each station's decoder reads."""
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    chunk = 1 << 26
+    a, b = math.sqrt(RHO), math.sqrt(1 - RHO)
+    outs = [torch.empty(nsamp * BITS // 8, dtype=torch.uint8, device="cuda") for _ in range(2)]
+    prev_tail = torch.randn(lag, device="cuda", generator=g)
+    for s0 in range(0, nsamp, chunk):
+        m = min(chunk, nsamp - s0)
+        c = torch.randn(m, device="cuda", generator=g)
+        c_lag = torch.cat([prev_tail, c])[:m]
+        prev_tail = c[m - lag:]
+        xs = (a * c + b * torch.randn(m, device="cuda", generator=g),
+              a * c_lag + b * torch.randn(m, device="cuda", generator=g))
+        for st, (x, lsb, sh) in enumerate(zip(xs, (cfg.lsb1, cfg.lsb2),
+                                              (cfg.shuffle1, cfg.shuffle2))):
+            if lsb:
+                x = x.view(-1, 2)
+                x[:, 1].neg_()
+                x = x.view(-1)
+            code = ((x >= -0.98).int() + (x >= 0).int() + (x >= 0.98).int()).view(-1, 16)
+            shifts = torch.arange(16, device="cuda", dtype=torch.int64) * 2
+            w = (code.long() << shifts).sum(1)
+            out = torch.zeros_like(w)
+            for pos in range(32):
+                out |= ((w >> pos) & 1) << sh[pos]
+            outs[st][s0 * BITS // 8:(s0 + m) * BITS // 8] = (
+                out.to(torch.int32).view(torch.uint8))
+    return outs
+
+
+# ------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        self.lines += [ln for ln in out.splitlines() if ln.strip()]
+        return self.summary()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- peaks
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic_per_frame_pair():
+    """DRAM bytes per frame pair of the correlation kernel from the committed
+    ncu summary (profiles/corr_kernel_n8192.md), or None."""
+    f = ROOT / "profiles" / "corr_kernel_n8192.md"
+    if not f.exists():
+        return None
+    for ln in f.read_text().splitlines():
+        if ln.strip().startswith("dram_bytes_per_frame_pair:"):
+            try:
+                return float(ln.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def flops_per_station_sample(n):
+    return 2.5 * math.log2(n) + 6.5
+
+
+# -------------------------------------------------------------- CPU legs
+
+def cpu_sample(cfg_o, raw1, raw2, target_s=8.0, max_frames=NF_SECTOR):
+    """Times the oracle port (all host threads) on a bounded sample and returns
+    (Gsample/s, frames, threads, seconds)."""
+    import oracle
+
+    oracle.build()
+    threads = os.cpu_count() or 1
+    nf = 256
+    t0 = time.perf_counter()
+    oracle.c_sector_corr(cfg_o, raw1, raw2, nf, 0, threads)
+    dt = time.perf_counter() - t0
+    nf = int(min(max_frames, max(256, nf * target_s / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    oracle.c_sector_corr(cfg_o, raw1, raw2, nf, 0, threads)
+    dt = time.perf_counter() - t0
+    return 2 * nf * N / dt / 1e9, nf, threads, dt
+
+
+def to_oracle_scan(cfg):
+    import dataclasses
+
+    import oracle
+
+    d = dataclasses.asdict(cfg)
+    d["geom_table"] = cfg.geom_table
+    return oracle.Scan(**d)
+
+
+def cpu_inputs_numpy(cfg, nf):
+    import oracle
+
+    x1, x2 = oracle.synth_station_pair(nf * N, 7, rho=RHO, delay_samples=7.0)
+    r1 = oracle.encode_station(x1, BITS, LEVELS, cfg.shuffle1, cfg.lsb1)
+    r2 = oracle.encode_station(x2, BITS, LEVELS, cfg.shuffle2, cfg.lsb2)
+    return r1, r2
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU restatement of the reference path on this
+    box's host cores, K bounded-sample steps."""
+    if rank != 0:
+        return 0
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import fxc
+
+    cfg = scan_config(fxc)
+    cfg_o = to_oracle_scan(cfg)
+    import oracle
+
+    oracle.build()
+    threads = os.cpu_count() or 1
+    probe_nf = 512
+    r1, r2 = cpu_inputs_numpy(cfg, probe_nf)
+    t0 = time.perf_counter()
+    oracle.c_sector_corr(cfg_o, r1, r2, probe_nf, 0, threads)
+    per_frame = (time.perf_counter() - t0) / probe_nf
+    # each step is a bounded sample sized so that warmup + steps take ~2 minutes
+    budget = 120.0 / max(1, args.steps + args.warmup)
+    nf = int(max(256, min(NF_SECTOR, budget / max(per_frame, 1e-7))))
+    r1, r2 = cpu_inputs_numpy(cfg, nf)
+    for _ in range(args.warmup):
+        oracle.c_sector_corr(cfg_o, r1, r2, nf, 0, threads)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        oracle.c_sector_corr(cfg_o, r1, r2, nf, k * nf, threads)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = 2 * nf * N / dt / 1e9
+    sample = f"{nf} frame pairs of the workload per step (of 1250000 per 10-s scan)"
+    line = {
+        "impl": "reference", "metric": "Gsample/s (2-bit, FFT 8192)", "value": value,
+        "unit": "Gsample/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, quantised Gaussian)",
+        "config": {"workload": WORKLOAD, "fft": N, "fs_hz": FS, "bits": BITS,
+                   "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "Gsample/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "Gsample/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ main
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fxc", choices=["fxc", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+
+    import fxc
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    cfg = scan_config(fxc)
+    eng = fxc.Engine(local, max_inflight=3)
+    scan = eng.open_scan(cfg)
+    stream = torch.cuda.Stream()
+
+    # ---- inputs resident in HBM: 10 sectors x 2 stations x 256 MB
+    nsamp = SECTORS * NF_SECTOR * N
+    d1, d2 = gen_station_pair_gpu(torch, nsamp, seed=1000 + rank, cfg=cfg)
+    bpf = N * BITS // 8
+    sec_bytes = NF_SECTOR * bpf
+    sec1 = [d1[i * sec_bytes:(i + 1) * sec_bytes] for i in range(SECTORS)]
+    sec2 = [d2[i * sec_bytes:(i + 1) * sec_bytes] for i in range(SECTORS)]
+    h = cfg.h
+    accs = [torch.empty(5 * h, dtype=torch.float64, device="cuda") for _ in range(SECTORS)]
+
+    def step():
+        for i in range(SECTORS):
+            scan.run_device(sec1[i], sec2[i], NF_SECTOR, i * NF_SECTOR, accs[i], stream=stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    scan.check()
+    scan.profile(reset=True)
+    scan.set_profiling(True)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    kern_ms, kern_launches, all_launches = scan.profile(reset=True)
+    scan.set_profiling(False)
+    scan.check()
+    ms = max_over_ranks(ms)
+    samples_per_step = 2 * SECTORS * NF_SECTOR * N
+    value = world * samples_per_step / (ms * 1e-3) / 1e9
+
+    # ---- end to end through the host-buffer C ABI (pinned host inputs)
+    e2e_value, bi, bo = None, 0, 0
+    h1 = [s.cpu().pin_memory() for s in sec1]
+    h2 = [s.cpu().pin_memory() for s in sec2]
+    n1 = [t.numpy() for t in h1]
+    n2 = [t.numpy() for t in h2]
+
+    def e2e_step():
+        ids = []
+        res = []
+        for i in range(SECTORS):
+            if len(ids) == 3:
+                res.append(scan.wait(ids.pop(0)))
+            ids.append(scan.submit(n1[i], n2[i], NF_SECTOR, i * NF_SECTOR))
+        while ids:
+            res.append(scan.wait(ids.pop(0)))
+        return res
+
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    t1 = time.perf_counter()
+    barrier()
+    e2e_ms = max_over_ranks((t1 - t0) * 1e3 / args.e2e_steps)
+    e2e_value = world * samples_per_step / (e2e_ms * 1e-3) / 1e9
+    bi = 2 * SECTORS * sec_bytes
+    bo = SECTORS * (5 * h * 8 + 4)
+    clk = clocks.stop()
+
+    # ---- roofline of the dominant kernel (correlation kernel, one sector per launch)
+    launch_ms = kern_ms / max(1, kern_launches)
+    flops_launch = flops_per_station_sample(N) * 2 * NF_SECTOR * N
+    fp32_peak = fxc.probe_fp32_peak(local)
+    hbm_peak, peak_kind = measured_peaks()
+    bytes_launch = 2 * sec_bytes + 5 * h * 8
+    tpf = profile_traffic_per_frame_pair()
+    roofline = {
+        "bound": "fp32", "achieved": flops_launch / (launch_ms * 1e-3) / 1e12,
+        "peak": fp32_peak, "unit": "TFLOP/s",
+        "frac": flops_launch / (launch_ms * 1e-3) / 1e12 / fp32_peak,
+        "traffic": None if tpf is None else tpf * NF_SECTOR,
+        "kernel": "corr_kernel<8192,1,0>", "launch_ms": launch_ms,
+        "algorithmic_flops_per_launch": flops_launch,
+        "peak_source": "live FMA probe of this GPU (fxc_probe_fp32_peak)",
+        "hbm": {"achieved": bytes_launch / (launch_ms * 1e-3) / 1e9, "peak": hbm_peak,
+                "unit": "GB/s", "frac": bytes_launch / (launch_ms * 1e-3) / 1e9 / hbm_peak,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6650 GB/s",
+                "algorithmic_bytes_per_launch": bytes_launch},
+    }
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        cfg_o = to_oracle_scan(cfg)
+        r1 = sec1[0].cpu().numpy()
+        r2 = sec2[0].cpu().numpy()
+        v, nf_cpu, thr, dt = cpu_sample(cfg_o, r1, r2)
+        cpu = {"value": v, "unit": "Gsample/s", "cores": thr, "kind": "port",
+               "sample": f"{nf_cpu} frame pairs of sector 0 ({dt:.1f} s, OpenMP, all threads)"}
+
+    if rank == 0:
+        line = {
+            "metric": "Gsample/s (2-bit, FFT 8192)", "value": value, "unit": "Gsample/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded quantised Gaussian, rho=0.05, generated on device)",
+            "config": {"workload": WORKLOAD, "fft": N, "fs_hz": FS, "bits": BITS,
+                       "scan_s": SCAN_S, "sectors": SECTORS, "frames_per_sector": NF_SECTOR,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (512 MB per sector, 5.12 GB per step)"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "Gsample/s", "h2d_bytes_per_step": bi,
+                    "d2h_bytes_per_step": bo, "ms_per_step": e2e_ms,
+                    "path": "fxc_sector_submit/fxc_sector_wait, pinned host buffers"},
+            "gpu_launches": all_launches,
+            "clocks": clk,
+            "realtime_factor": value / (2 * FS / 1e9),
+        }
+        print(json.dumps(line), flush=True)
+    scan.close()
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

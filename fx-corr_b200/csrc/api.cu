@@ -1,0 +1,705 @@
+// api.cu — the C ABI of libfxc (include/fxc.h): engine, scans, per-sector
+// submission on host buffers, device-resident sector calls, stage entry
+// points and host helpers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "fxc.h"
+#include "fxc_kernels.h"
+
+using namespace fxc;
+
+namespace {
+
+thread_local std::string g_err;
+
+fxc_status fail(fxc_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return s;
+}
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(e_ == cudaErrorMemoryAllocation ? FXC_ENOMEM : FXC_ECUDA, "%s: %s", \
+                  #call, cudaGetErrorString(e_));                                      \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+struct fxc_engine {
+  int device = 0;
+  int sm_count = 0;
+  int max_inflight = 2;
+  uint64_t budget = 0;
+  uint64_t in_use = 0;
+  std::mutex mu;
+};
+
+struct SectorSlot {
+  uint8_t* d_raw1 = nullptr;
+  uint8_t* d_raw2 = nullptr;
+  uint64_t cap1 = 0, cap2 = 0;
+  double* d_acc = nullptr;
+  uint8_t* d_rawout = nullptr;
+  uint64_t cap_out = 0;
+  double* h_acc = nullptr;     // pinned: 5H doubles + error word
+  uint8_t* h_rawout = nullptr; // pinned
+  uint64_t hcap_out = 0;
+  cudaEvent_t ev_h2d = nullptr, ev_done = nullptr;
+  uint64_t id = 0;
+  uint64_t nf = 0;
+  bool busy = false;
+};
+
+struct fxc_scan {
+  fxc_engine* eng = nullptr;
+  fxc_scan_cfg cfg{};
+  uint32_t n = 0, h = 0;
+  uint32_t bpf1 = 0, bpf2 = 0, bpfo = 0;
+  int shkind[2] = {0, 0};
+  double* d_table = nullptr;
+  uint32_t* d_lut = nullptr;     // [2][1024]
+  float* d_levels = nullptr;     // [2][256]
+  uint8_t* d_shuffle_out = nullptr;
+  double* d_partials = nullptr;
+  uint64_t partials_elems = 0;
+  uint32_t* d_err = nullptr;
+  cudaStream_t stream = nullptr;     // compute
+  cudaStream_t copy_stream = nullptr;
+  std::vector<SectorSlot> slots;
+  uint64_t next_id = 1;
+  uint64_t hbm_bytes = 0;
+  // kernel timing (fxc_scan_set_profiling)
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+  size_t prof_used = 0;
+  uint64_t kernel_launches = 0;
+  uint64_t all_launches = 0;
+};
+
+namespace {
+
+int shuffle_kind(const uint8_t sh[32]) {
+  bool ident = true, pair = true;
+  for (int i = 0; i < 32; ++i) {
+    if (sh[i] != i) ident = false;
+    if (sh[i] != (i ^ 1)) pair = false;
+  }
+  return ident ? SH_IDENTITY : (pair ? SH_PAIRSWAP : SH_GENERIC);
+}
+
+// Byte LUTs for a generic 32-bit shuffle: out bit o takes word bit sh[o].
+void build_lut(const uint8_t sh[32], uint32_t* lut) {
+  std::memset(lut, 0, 1024 * sizeof(uint32_t));
+  for (int o = 0; o < 32; ++o) {
+    const int in = sh[o];
+    const int byte = in >> 3, bit = in & 7;
+    for (int v = 0; v < 256; ++v)
+      if ((v >> bit) & 1) lut[byte * 256 + v] |= (1u << o);
+  }
+}
+
+DelayParams delay_params(const fxc_scan* s) {
+  const fxc_delay_cfg& c = s->cfg.delay;
+  DelayParams p;
+  p.frame_dt = c.frame_dt;
+  p.fs = c.fs;
+  p.time_offset_s = c.time_offset_s;
+  p.table = s->d_table;
+  p.table_len = s->d_table ? c.geom_len : 0;
+  p.coarse = c.coarse_delay_s;
+  p.user_samples = c.delay_user_samples;
+  p.extra_rate = c.extra_delay_rate_sps;
+  p.c1d = c.clock1_delay_s;
+  p.c1r = c.clock1_rate_sps;
+  p.c2d = c.clock2_delay_s;
+  p.c2r = c.clock2_rate_sps;
+  p.d_seek = c.d_seek;
+  p.d1 = c.net_d1_base;
+  p.r1 = c.total_rate1_base;
+  p.a1 = c.total_accel1_base;
+  p.d2 = c.net_d2_base;
+  p.r2 = c.total_rate2_base;
+  p.a2 = c.total_accel2_base;
+  p.lo1 = c.lo1_hz;
+  p.lo2 = c.lo2_hz;
+  return p;
+}
+
+void station_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2, StationParams st[2]) {
+  st[0].raw = r1;
+  st[1].raw = r2;
+  for (int k = 0; k < 2; ++k) {
+    st[k].shlut = s->d_lut + 1024 * k;
+    st[k].levels = s->d_levels + 256 * k;
+    st[k].bpf = k ? s->bpf2 : s->bpf1;
+    st[k].bits = (int)(k ? s->cfg.bits2 : s->cfg.bits1);
+    st[k].lsb = k ? s->cfg.lsb2 : s->cfg.lsb1;
+    st[k].shkind = s->shkind[k];
+  }
+}
+
+int corr_grid(const fxc_scan* s, uint64_t nf) {
+  const uint64_t fpc = (uint64_t)corr_frames_per_cta_iter(s->n);
+  const uint64_t iters = (nf + fpc - 1) / fpc;
+  const uint64_t maxg = (uint64_t)s->eng->sm_count * (uint64_t)corr_ctas_per_sm(s->n);
+  return (int)std::max<uint64_t>(1, std::min(iters, maxg));
+}
+
+CorrParams corr_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
+                       uint64_t first) {
+  CorrParams p{};
+  station_params(s, r1, r2, p.st);
+  p.dl = delay_params(s);
+  p.nf = nf;
+  p.first_frame = first;
+  p.a1s = (int32_t)s->cfg.a1s;
+  p.a1e = (int32_t)s->cfg.a1e;
+  p.a2s = (int32_t)s->cfg.a2s;
+  p.grid = s->cfg.grid;
+  p.products = s->cfg.products;
+  const int fpc = corr_frames_per_cta_iter(s->n);
+  p.stage_bytes = (uint32_t)fpc * (s->bpf1 + s->bpf2);
+  p.flush_every = (uint32_t)std::max(1, 32 / fpc);
+  p.df_hz = s->cfg.fs_hz / (double)s->n;
+  p.partials = s->d_partials;
+  p.err = s->d_err;
+  return p;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+fxc_status check_device_inputs(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2) {
+  if (!s) return fail(FXC_EINVAL, "scan is NULL");
+  if (!r1 || !r2) return fail(FXC_EINVAL, "device input pointer is NULL");
+  if (!aligned16(r1) || !aligned16(r2))
+    return fail(FXC_EINVAL, "device inputs must be 16-byte aligned");
+  return FXC_OK;
+}
+
+fxc_status validate_cfg(const fxc_scan_cfg* c) {
+  const uint32_t n = c->fft_len;
+  if (!(n == 1024 || n == 2048 || n == 4096 || n == 8192))
+    return fail(FXC_EUNSUPPORTED, "fft_len %u not supported (1024, 2048, 4096, 8192)", n);
+  for (uint32_t b : {c->bits1, c->bits2})
+    if (!(b == 1 || b == 2 || b == 4 || b == 8))
+      return fail(FXC_EUNSUPPORTED, "bits %u not supported (1, 2, 4, 8)", b);
+  if (c->nlevels1 != (1u << c->bits1) || c->nlevels2 != (1u << c->bits2))
+    return fail(FXC_EINVAL, "Expected %u / %u levels, received %u / %u", 1u << c->bits1,
+                1u << c->bits2, c->nlevels1, c->nlevels2);
+  if (c->bits_out != std::max(c->bits1, c->bits2))
+    return fail(FXC_EINVAL, "bits_out must be max(bits1, bits2)");
+  for (int k = 0; k < 2; ++k) {
+    const uint8_t* sh = k ? c->shuffle2 : c->shuffle1;
+    uint32_t seen = 0;
+    for (int i = 0; i < 32; ++i) {
+      if (sh[i] > 31) return fail(FXC_EINVAL, "Shuffle map must be a permutation of 0..31");
+      seen |= 1u << sh[i];
+    }
+    if (seen != 0xFFFFFFFFu) return fail(FXC_EINVAL, "Shuffle map must be a permutation of 0..31");
+  }
+  const uint32_t h = n / 2 + 1;
+  if (c->a1e <= c->a1s) return fail(FXC_EINVAL, "No band overlap");
+  if (c->a1e > h || c->a2s + (c->a1e - c->a1s) > h)
+    return fail(FXC_EINVAL, "band alignment outside the spectrum");
+  if ((int64_t)c->a2s - (int64_t)c->a1s != (int64_t)c->shift_bins)
+    return fail(FXC_EINVAL, "a2s must equal a1s + shift_bins");
+  if (c->grid != 0 && c->grid != 1) return fail(FXC_EINVAL, "grid must be 0 (ant1) or 1 (ant2)");
+  if (!(c->fs_hz > 0.0) || !(c->delay.fs > 0.0)) return fail(FXC_EINVAL, "sample rate must be > 0");
+  if (c->delay.geom_table && c->delay.geom_len == 0)
+    return fail(FXC_EINVAL, "geometric delay table is empty");
+  if (c->products & ~31u) return fail(FXC_EINVAL, "unknown product flags");
+  if (c->products & (FXC_PROD_PHASED | FXC_PROD_RAW))
+    return fail(FXC_EUNSUPPORTED, "phased products are not available in this build");
+  return FXC_OK;
+}
+
+fxc_status grow(uint8_t** p, uint64_t* cap, uint64_t need) {
+  if (*cap >= need) return FXC_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  const uint64_t want = std::max<uint64_t>(need, 16);
+  CK(cudaMalloc(p, want));
+  *cap = want;
+  return FXC_OK;
+}
+
+fxc_status grow_host(uint8_t** p, uint64_t* cap, uint64_t need) {
+  if (*cap >= need) return FXC_OK;
+  if (*p) cudaFreeHost(*p);
+  *p = nullptr;
+  *cap = 0;
+  const uint64_t want = std::max<uint64_t>(need, 16);
+  CK(cudaMallocHost(p, want));
+  *cap = want;
+  return FXC_OK;
+}
+
+fxc_status run_corr_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
+                           uint64_t first, double* d_acc, cudaStream_t st) {
+  const uint32_t h = s->h;
+  if (nf == 0 || !(s->cfg.products & (FXC_PROD_ACF | FXC_PROD_XCF))) {
+    CK(cudaMemsetAsync(d_acc, 0, sizeof(double) * 5 * h, st));
+    return FXC_OK;
+  }
+  const int grid = corr_grid(s, nf);
+  CorrParams p = corr_params(s, r1, r2, nf, first);
+  std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
+  if (s->profiling) {
+    if (s->prof_used == s->prof_events.size()) {
+      std::pair<cudaEvent_t, cudaEvent_t> pr;
+      CK(cudaEventCreate(&pr.first));
+      CK(cudaEventCreate(&pr.second));
+      s->prof_events.push_back(pr);
+    }
+    ev = &s->prof_events[s->prof_used++];
+    CK(cudaEventRecord(ev->first, st));
+  }
+  CK(launch_corr(s->n, MODE_CORR, p, grid, st));
+  if (ev) CK(cudaEventRecord(ev->second, st));
+  CK(launch_reduce(s->d_partials, grid, (int)h, d_acc, st));
+  s->kernel_launches += 1;
+  s->all_launches += 2;
+  return FXC_OK;
+}
+
+}  // namespace
+
+// ======================================================================= ABI
+
+extern "C" {
+
+int32_t fxc_abi_version(void) { return FXC_ABI_VERSION; }
+
+const char* fxc_status_string(fxc_status s) {
+  switch (s) {
+    case FXC_OK: return "ok";
+    case FXC_EINVAL: return "invalid argument";
+    case FXC_ENOMEM: return "out of memory";
+    case FXC_ECUDA: return "CUDA error";
+    case FXC_ETIMEDOUT: return "timed out";
+    case FXC_ENOTFOUND: return "not found";
+    case FXC_EBUSY: return "busy";
+    case FXC_EUNSUPPORTED: return "unsupported";
+    case FXC_EDEVICE: return "device-reported error";
+    default: return "unknown status";
+  }
+}
+
+const char* fxc_last_error(void) { return g_err.c_str(); }
+
+fxc_status fxc_engine_create(const fxc_device_opts* opts, fxc_engine** out) {
+  if (!out) return fail(FXC_EINVAL, "out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  const int dev = opts ? opts->device : 0;
+  if (dev < 0 || dev >= ndev) return fail(FXC_EINVAL, "device %d out of range (0..%d)", dev, ndev - 1);
+  DeviceGuard g(dev);
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major < 10)
+    return fail(FXC_EUNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a", dev,
+                prop.major, prop.minor);
+  auto* e = new fxc_engine();
+  e->device = dev;
+  e->sm_count = prop.multiProcessorCount;
+  e->max_inflight = (opts && opts->max_inflight > 0) ? opts->max_inflight : 2;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  e->budget = (opts && opts->hbm_budget_bytes) ? opts->hbm_budget_bytes : (uint64_t)(0.8 * free_b);
+  *out = e;
+  return FXC_OK;
+}
+
+fxc_status fxc_engine_destroy(fxc_engine* e) {
+  delete e;
+  return FXC_OK;
+}
+
+fxc_status fxc_scan_open(fxc_engine* e, const fxc_scan_cfg* cfg, fxc_scan** out) {
+  if (!e || !cfg || !out) return fail(FXC_EINVAL, "NULL argument");
+  *out = nullptr;
+  fxc_status st = validate_cfg(cfg);
+  if (st != FXC_OK) return st;
+  DeviceGuard g(e->device);
+  auto* s = new fxc_scan();
+  s->eng = e;
+  s->cfg = *cfg;
+  s->n = cfg->fft_len;
+  s->h = s->n / 2 + 1;
+  s->bpf1 = (uint32_t)fxc_bytes_per_frame(s->n, cfg->bits1);
+  s->bpf2 = (uint32_t)fxc_bytes_per_frame(s->n, cfg->bits2);
+  s->bpfo = (uint32_t)fxc_bytes_per_frame(s->n, cfg->bits_out);
+  s->shkind[0] = shuffle_kind(cfg->shuffle1);
+  s->shkind[1] = shuffle_kind(cfg->shuffle2);
+  const uint64_t maxg = (uint64_t)e->sm_count * (uint64_t)corr_ctas_per_sm(s->n);
+  s->partials_elems = maxg * 4 * s->h;
+  const uint64_t need = s->partials_elems * 8 + 2 * 1024 * 4 + 2 * 256 * 4 + 64 +
+                        (cfg->delay.geom_table ? cfg->delay.geom_len * 8 : 0);
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    if (e->in_use + need > e->budget) {
+      delete s;
+      return fail(FXC_EBUSY, "HBM budget exhausted (%llu + %llu > %llu bytes)",
+                  (unsigned long long)e->in_use, (unsigned long long)need,
+                  (unsigned long long)e->budget);
+    }
+    e->in_use += need;
+  }
+  s->hbm_bytes = need;
+  auto cleanup = [&](fxc_status r) {
+    fxc_scan_close(s);
+    return r;
+  };
+#define CKS(call)                                                                          \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return cleanup(fail(e_ == cudaErrorMemoryAllocation ? FXC_ENOMEM : FXC_ECUDA, "%s: %s", \
+                          #call, cudaGetErrorString(e_)));                                 \
+  } while (0)
+  CKS(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  CKS(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+  CKS(cudaMalloc(&s->d_partials, s->partials_elems * sizeof(double)));
+  CKS(cudaMalloc(&s->d_lut, 2 * 1024 * sizeof(uint32_t)));
+  CKS(cudaMalloc(&s->d_levels, 2 * 256 * sizeof(float)));
+  CKS(cudaMalloc(&s->d_shuffle_out, 32));
+  CKS(cudaMalloc(&s->d_err, 16));
+  CKS(cudaMemset(s->d_err, 0, 16));
+  {
+    std::vector<uint32_t> lut(2048);
+    build_lut(cfg->shuffle1, lut.data());
+    build_lut(cfg->shuffle2, lut.data() + 1024);
+    CKS(cudaMemcpy(s->d_lut, lut.data(), lut.size() * 4, cudaMemcpyHostToDevice));
+    std::vector<float> lv(512, 0.0f);
+    for (uint32_t i = 0; i < cfg->nlevels1; ++i) lv[i] = (float)cfg->levels1[i];
+    for (uint32_t i = 0; i < cfg->nlevels2; ++i) lv[256 + i] = (float)cfg->levels2[i];
+    CKS(cudaMemcpy(s->d_levels, lv.data(), lv.size() * 4, cudaMemcpyHostToDevice));
+    CKS(cudaMemcpy(s->d_shuffle_out, cfg->shuffle1, 32, cudaMemcpyHostToDevice));
+  }
+  if (cfg->delay.geom_table) {
+    CKS(cudaMalloc(&s->d_table, cfg->delay.geom_len * sizeof(double)));
+    CKS(cudaMemcpy(s->d_table, cfg->delay.geom_table, cfg->delay.geom_len * sizeof(double),
+                   cudaMemcpyHostToDevice));
+  }
+  s->cfg.delay.geom_table = nullptr;  // the host pointer is not kept
+  s->slots.resize((size_t)e->max_inflight);
+  for (auto& sl : s->slots) {
+    CKS(cudaEventCreateWithFlags(&sl.ev_h2d, cudaEventDisableTiming));
+    CKS(cudaEventCreateWithFlags(&sl.ev_done, cudaEventDisableTiming));
+    CKS(cudaMalloc(&sl.d_acc, sizeof(double) * 5 * s->h));
+    CKS(cudaMallocHost(&sl.h_acc, sizeof(double) * 5 * s->h + 16));
+  }
+#undef CKS
+  *out = s;
+  return FXC_OK;
+}
+
+fxc_status fxc_scan_close(fxc_scan* s) {
+  if (!s) return FXC_OK;
+  DeviceGuard g(s->eng->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
+  for (auto& sl : s->slots) {
+    cudaFree(sl.d_raw1);
+    cudaFree(sl.d_raw2);
+    cudaFree(sl.d_acc);
+    cudaFree(sl.d_rawout);
+    cudaFreeHost(sl.h_acc);
+    cudaFreeHost(sl.h_rawout);
+    if (sl.ev_h2d) cudaEventDestroy(sl.ev_h2d);
+    if (sl.ev_done) cudaEventDestroy(sl.ev_done);
+  }
+  for (auto& pr : s->prof_events) {
+    cudaEventDestroy(pr.first);
+    cudaEventDestroy(pr.second);
+  }
+  cudaFree(s->d_partials);
+  cudaFree(s->d_lut);
+  cudaFree(s->d_levels);
+  cudaFree(s->d_shuffle_out);
+  cudaFree(s->d_err);
+  cudaFree(s->d_table);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+  {
+    std::lock_guard<std::mutex> lk(s->eng->mu);
+    s->eng->in_use -= std::min(s->eng->in_use, s->hbm_bytes);
+  }
+  delete s;
+  return FXC_OK;
+}
+
+fxc_status fxc_sector_run_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t* d_raw2,
+                                 uint64_t nf, uint64_t first_frame, double* d_acc,
+                                 uint8_t* d_raw_out, void* stream) {
+  (void)d_raw_out;
+  fxc_status st = check_device_inputs(s, d_raw1, d_raw2);
+  if (st != FXC_OK) return st;
+  if (!d_acc) return fail(FXC_EINVAL, "d_acc is NULL");
+  DeviceGuard g(s->eng->device);
+  return run_corr_device(s, d_raw1, d_raw2, nf, first_frame, d_acc, (cudaStream_t)stream);
+}
+
+fxc_status fxc_scan_check(fxc_scan* s) {
+  if (!s) return fail(FXC_EINVAL, "scan is NULL");
+  DeviceGuard g(s->eng->device);
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaDeviceSynchronize());
+  uint32_t err = 0;
+  CK(cudaMemcpy(&err, s->d_err, 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemset(s->d_err, 0, 4));
+  if (err & ERR_WAIT_TIMEOUT) return fail(FXC_ETIMEDOUT, "a bounded device-side wait gave up");
+  if (err) return fail(FXC_EDEVICE, "kernel error word 0x%x", err);
+  return FXC_OK;
+}
+
+fxc_status fxc_scan_set_profiling(fxc_scan* s, int32_t enable) {
+  if (!s) return fail(FXC_EINVAL, "scan is NULL");
+  s->profiling = enable != 0;
+  return FXC_OK;
+}
+
+fxc_status fxc_scan_profile(fxc_scan* s, double* kernel_ms, uint64_t* kernel_launches,
+                            uint64_t* all_launches, int32_t reset) {
+  if (!s) return fail(FXC_EINVAL, "scan is NULL");
+  DeviceGuard g(s->eng->device);
+  double total = 0.0;
+  for (size_t i = 0; i < s->prof_used; ++i) {
+    CK(cudaEventSynchronize(s->prof_events[i].second));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, s->prof_events[i].first, s->prof_events[i].second));
+    total += ms;
+  }
+  if (kernel_ms) *kernel_ms = total;
+  if (kernel_launches) *kernel_launches = s->kernel_launches;
+  if (all_launches) *all_launches = s->all_launches;
+  if (reset) {
+    s->prof_used = 0;
+    s->kernel_launches = 0;
+    s->all_launches = 0;
+  }
+  return FXC_OK;
+}
+
+fxc_status fxc_delay_entries_device(fxc_scan* s, uint64_t first_frame, uint64_t nf,
+                                    fxc_frame_delay* d_out, void* stream) {
+  if (!s || (!d_out && nf)) return fail(FXC_EINVAL, "NULL argument");
+  DeviceGuard g(s->eng->device);
+  CK(launch_delay_entries(delay_params(s), first_frame, nf,
+                          reinterpret_cast<fxc_frame_delay_dev*>(d_out), (cudaStream_t)stream));
+  return FXC_OK;
+}
+
+fxc_status fxc_decode_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t* d_raw2,
+                             uint64_t nf, uint64_t first_frame, float* d_x1, float* d_x2,
+                             void* stream) {
+  fxc_status st = check_device_inputs(s, d_raw1, d_raw2);
+  if (st != FXC_OK) return st;
+  if (nf == 0) return FXC_OK;
+  if (!d_x1 || !d_x2) return fail(FXC_EINVAL, "output pointer is NULL");
+  DeviceGuard g(s->eng->device);
+  CorrParams p = corr_params(s, d_raw1, d_raw2, nf, first_frame);
+  p.out_a = d_x1;
+  p.out_b = d_x2;
+  CK(launch_corr(s->n, MODE_DECODE, p, corr_grid(s, nf), (cudaStream_t)stream));
+  return FXC_OK;
+}
+
+fxc_status fxc_spectra_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t* d_raw2,
+                              uint64_t nf, uint64_t first_frame, float* d_s1, float* d_s2,
+                              void* stream) {
+  fxc_status st = check_device_inputs(s, d_raw1, d_raw2);
+  if (st != FXC_OK) return st;
+  if (nf == 0) return FXC_OK;
+  if (!d_s1 || !d_s2) return fail(FXC_EINVAL, "output pointer is NULL");
+  DeviceGuard g(s->eng->device);
+  CorrParams p = corr_params(s, d_raw1, d_raw2, nf, first_frame);
+  p.out_a = d_s1;
+  p.out_b = d_s2;
+  CK(launch_corr(s->n, MODE_SPECTRA, p, corr_grid(s, nf), (cudaStream_t)stream));
+  return FXC_OK;
+}
+
+fxc_status fxc_sector_submit(fxc_scan* s, const uint8_t* raw1, uint64_t n1, const uint8_t* raw2,
+                             uint64_t n2, uint64_t nf, uint64_t first_frame, uint64_t* sector_id) {
+  if (!s || !sector_id) return fail(FXC_EINVAL, "NULL argument");
+  if (nf && (!raw1 || !raw2)) return fail(FXC_EINVAL, "input buffer is NULL");
+  const uint64_t need1 = nf * s->bpf1, need2 = nf * s->bpf2;
+  if (n1 < need1 || n2 < need2)
+    return fail(FXC_EINVAL, "input too short: need %llu / %llu bytes for %llu frames",
+                (unsigned long long)need1, (unsigned long long)need2, (unsigned long long)nf);
+  SectorSlot* sl = nullptr;
+  for (auto& x : s->slots)
+    if (!x.busy) {
+      sl = &x;
+      break;
+    }
+  if (!sl) return fail(FXC_EBUSY, "all %zu sector slots are in flight; wait for one first",
+                       s->slots.size());
+  DeviceGuard g(s->eng->device);
+  fxc_status st;
+  if ((st = grow(&sl->d_raw1, &sl->cap1, need1)) != FXC_OK) return st;
+  if ((st = grow(&sl->d_raw2, &sl->cap2, need2)) != FXC_OK) return st;
+  if (nf) {
+    CK(cudaMemcpyAsync(sl->d_raw1, raw1, need1, cudaMemcpyHostToDevice, s->copy_stream));
+    CK(cudaMemcpyAsync(sl->d_raw2, raw2, need2, cudaMemcpyHostToDevice, s->copy_stream));
+  }
+  CK(cudaEventRecord(sl->ev_h2d, s->copy_stream));
+  CK(cudaStreamWaitEvent(s->stream, sl->ev_h2d, 0));
+  st = run_corr_device(s, sl->d_raw1, sl->d_raw2, nf, first_frame, sl->d_acc, s->stream);
+  if (st != FXC_OK) return st;
+  CK(cudaMemcpyAsync(sl->h_acc, sl->d_acc, sizeof(double) * 5 * s->h, cudaMemcpyDeviceToHost,
+                     s->stream));
+  CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(sl->h_acc) + sizeof(double) * 5 * s->h, s->d_err,
+                     4, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaEventRecord(sl->ev_done, s->stream));
+  sl->busy = true;
+  sl->nf = nf;
+  sl->id = s->next_id++;
+  *sector_id = sl->id;
+  return FXC_OK;
+}
+
+fxc_status fxc_sector_wait(fxc_scan* s, uint64_t sector_id, int32_t timeout_ms,
+                           fxc_sector_out* out) {
+  if (!s) return fail(FXC_EINVAL, "scan is NULL");
+  SectorSlot* sl = nullptr;
+  for (auto& x : s->slots)
+    if (x.busy && x.id == sector_id) sl = &x;
+  if (!sl) return fail(FXC_ENOTFOUND, "sector id %llu is not in flight", (unsigned long long)sector_id);
+  DeviceGuard g(s->eng->device);
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t q = cudaEventQuery(sl->ev_done);
+    if (q == cudaSuccess) break;
+    if (q != cudaErrorNotReady) return fail(FXC_ECUDA, "sector failed: %s", cudaGetErrorString(q));
+    if (timeout_ms >= 0 &&
+        std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(timeout_ms))
+      return fail(FXC_ETIMEDOUT, "sector %llu not done after %d ms", (unsigned long long)sector_id,
+                  timeout_ms);
+    std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+  sl->busy = false;
+  const uint32_t h = s->h;
+  uint32_t err = 0;
+  std::memcpy(&err, reinterpret_cast<uint8_t*>(sl->h_acc) + sizeof(double) * 5 * h, 4);
+  if (out) {
+    if (out->acf11) std::memcpy(out->acf11, sl->h_acc, sizeof(double) * h);
+    if (out->acf22) std::memcpy(out->acf22, sl->h_acc + h, sizeof(double) * h);
+    if (out->xcf) std::memcpy(out->xcf, sl->h_acc + 2 * h, sizeof(double) * 2 * h);
+    if (out->phased) std::memcpy(out->phased, sl->h_acc + 4 * h, sizeof(double) * h);
+    out->frames_failed = 0;
+  }
+  if (err) {
+    cudaMemsetAsync(s->d_err, 0, 4, s->stream);
+    if (err & ERR_WAIT_TIMEOUT) return fail(FXC_ETIMEDOUT, "a bounded device-side wait gave up");
+    return fail(FXC_EDEVICE, "kernel error word 0x%x", err);
+  }
+  return FXC_OK;
+}
+
+// ---------------------------------------------------------------- helpers
+
+uint64_t fxc_bytes_per_frame(uint32_t fft, uint32_t bits) {
+  return ((uint64_t)fft * bits + 7) / 8;
+}
+
+fxc_status fxc_parse_shuffle(const int32_t ext[32], uint8_t internal[32]) {
+  // args.rs:202-210
+  if (!ext || !internal) return fail(FXC_EINVAL, "NULL argument");
+  uint32_t seen = 0;
+  for (int i = 0; i < 32; ++i) {
+    if (ext[i] < 0 || ext[i] > 31 || ((seen >> ext[i]) & 1u))
+      return fail(FXC_EINVAL, "Shuffle map must be a permutation of 0..31");
+    seen |= 1u << ext[i];
+  }
+  for (int idx = 0; idx < 32; ++idx) internal[31 - idx] = (uint8_t)ext[idx];
+  return FXC_OK;
+}
+
+fxc_status fxc_band_alignment(uint32_t fft, double fs, double c1, double c2, double bw1,
+                              double bw2, int64_t out[4]) {
+  // main.rs:363-372
+  if (!out || fft == 0 || !(fs > 0.0)) return fail(FXC_EINVAL, "invalid argument");
+  const double df = fs / (double)fft;
+  const uint64_t h = fft / 2 + 1;
+  const uint64_t lim = (fft % 2 == 0) ? h - 1 : h;
+  const double q1 = std::floor((bw1 * 1e6) / df), q2 = std::floor((bw2 * 1e6) / df);
+  uint64_t v1 = (q1 > 0.0 ? (uint64_t)q1 : 0) + 1, v2 = (q2 > 0.0 ? (uint64_t)q2 : 0) + 1;
+  v1 = std::min(v1, lim);
+  v2 = std::min(v2, lim);
+  const double sr = (c1 * 1e6 - c2 * 1e6) / df;
+  const int64_t sb = (int64_t)std::llround(sr);
+  const int64_t a1s = std::max<int64_t>(0, -sb);
+  const int64_t a1e = std::min<int64_t>((int64_t)v1, (int64_t)v2 - sb);
+  if (a1e <= a1s) return fail(FXC_EINVAL, "No band overlap");
+  out[0] = sb;
+  out[1] = a1s;
+  out[2] = a1e;
+  out[3] = a1s + sb;
+  return FXC_OK;
+}
+
+fxc_status fxc_level_power(const double* levels, uint32_t n, double* out) {
+  // main.rs:378-387
+  if (!levels || !out || n == 0) return fail(FXC_EINVAL, "levels are empty");
+  double s = 0.0;
+  for (uint32_t i = 0; i < n; ++i) s += levels[i] * levels[i];
+  const double p = s / (double)n;
+  if (!std::isfinite(p) || p <= 0.0) return fail(FXC_EINVAL, "mean-square level is invalid: %g", p);
+  *out = p;
+  return FXC_OK;
+}
+
+fxc_status fxc_normalize(uint32_t fft, uint64_t nf, double level_power, const double* acc_real,
+                         const double* acc_cplx, float* out) {
+  // main.rs:2645-2683
+  if (!out || (!acc_real && !acc_cplx)) return fail(FXC_EINVAL, "NULL argument");
+  const double norm_base = (double)nf * ((double)fft * (double)fft);
+  const double inv = 1.0 / (0.5 * level_power * norm_base);
+  for (uint32_t k = 0; k < fft / 2; ++k) {
+    if (acc_cplx) {
+      out[2 * k] = (float)(acc_cplx[2 * k] * inv);
+      out[2 * k + 1] = (float)(acc_cplx[2 * k + 1] * inv);
+    } else {
+      out[2 * k] = (float)(acc_real[k] * inv);
+      out[2 * k + 1] = 0.0f;
+    }
+  }
+  return FXC_OK;
+}
+
+}  // extern "C"

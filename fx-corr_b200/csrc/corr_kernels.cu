@@ -1,0 +1,382 @@
+// corr_kernels.cu — the fused FX-correlation kernel for sm_100a.
+//
+// One CTA processes a contiguous run of frame pairs of a sector.  Per frame
+// pair (station 1 and 2 share one complex FFT: z = x1 + i*x2):
+//   1. the packed .raw words of both stations arrive in shared memory by
+//      cp.async.bulk (TMA bulk copy) tracked by an mbarrier, two stages deep;
+//   2. decode: 32-bit word shuffle, b-bit codes -> f32 levels, LSB->USB flip
+//      of odd samples (src/utils.rs:215-376);
+//   3. per-frame FP64 delay model (src/main.rs:184-241) -> integer shifts,
+//      fringe phasors and the fractional-delay phase ramp;
+//   4. first radix-16 pass reads the planes with the integer shift and zero
+//      fill (src/utils.rs:126-145), remaining Stockham passes in shared memory;
+//   5. two-for-one split of Z into S1, S2 (the two real FFTs,
+//      src/utils.rs:47-59), band alignment, fringe x phase-ramp rotation and
+//      |S|^2 / S1 conj(S2) accumulation (src/main.rs:2491-2568) into per-thread
+//      f32 registers, flushed every 32 frames into per-CTA f64 partials;
+//   6. a second kernel reduces the per-CTA partials in a fixed order.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fxc_device.cuh"
+#include "fxc_kernels.h"
+
+namespace fxc {
+
+constexpr int kStages = 2;
+constexpr uint32_t kWaitPolls = 1u << 26;  // bounded mbarrier wait
+
+struct SmemLayout {
+  uint32_t off_a, off_b, off_stage, off_lut, off_lv, off_fi, off_bar, off_flag, total;
+};
+
+template <int N, int FPC>
+__host__ __device__ inline SmemLayout smem_layout(uint32_t stage_bytes) {
+  SmemLayout L;
+  const uint32_t cbytes = (uint32_t)(FPC * Geom<N>::CSTRIDE * sizeof(float2));
+  L.off_a = 0;
+  L.off_b = L.off_a + cbytes;
+  L.off_stage = L.off_b + cbytes;
+  L.off_lut = L.off_stage + kStages * ((stage_bytes + 127u) & ~127u);
+  L.off_lv = L.off_lut + 2 * 1024 * 4;
+  L.off_fi = L.off_lv + 2 * 256 * 4;
+  L.off_bar = L.off_fi + ((FPC * (uint32_t)sizeof(FrameInfo) + 15u) & ~15u);
+  L.off_flag = L.off_bar + kStages * 8;
+  L.total = L.off_flag + 16;
+  return L;
+}
+
+template <int N, int FPC, int MODE>
+__global__ void __launch_bounds__(FPC * N / 16, (N >= 8192 ? 1 : 2))
+corr_kernel(const CorrParams p) {
+  constexpr int T1 = N / 16;
+  constexpr int T = FPC * T1;
+  constexpr int H = N / 2 + 1;
+  constexpr int BPT = (N / 2) / T;
+  static_assert(BPT * T == N / 2, "bins per thread");
+
+  extern __shared__ __align__(128) uint8_t smem[];
+  const SmemLayout L = smem_layout<N, FPC>(p.stage_bytes);
+  float2* bufA = reinterpret_cast<float2*>(smem + L.off_a);
+  float2* bufB = reinterpret_cast<float2*>(smem + L.off_b);
+  uint8_t* stage = smem + L.off_stage;
+  const uint32_t stage_stride = (p.stage_bytes + 127u) & ~127u;
+  uint32_t* lut = reinterpret_cast<uint32_t*>(smem + L.off_lut);
+  float* lv = reinterpret_cast<float*>(smem + L.off_lv);
+  FrameInfo* finfo = reinterpret_cast<FrameInfo*>(smem + L.off_fi);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.off_bar);
+  int* flag = reinterpret_cast<int*>(smem + L.off_flag);
+
+  const int tid = threadIdx.x;
+  const int g = tid / T1;  // frame slot of this thread in an iteration
+  const int t = tid % T1;  // thread index within its frame pair
+
+  // ---- constant tables: levels, shuffle byte LUTs
+  for (int i = tid; i < 512; i += T) lv[i] = p.st[i >> 8].levels[i & 255];
+  for (int s = 0; s < 2; ++s)
+    if (p.st[s].shkind == SH_GENERIC)
+      for (int i = tid; i < 1024; i += T) lut[s * 1024 + i] = p.st[s].shlut[i];
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    *flag = 0;
+    fence_proxy_async();
+  }
+  Twiddles<N> tw;
+  tw.init(t);
+
+  // ---- this CTA's iterations (FPC frame pairs each)
+  const uint64_t iters = (p.nf + FPC - 1) / FPC;
+  const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
+  const uint64_t it1 = ((blockIdx.x + 1) * iters) / gridDim.x;
+  const uint32_t bpf1 = p.st[0].bpf, bpf2 = p.st[1].bpf;
+
+  auto issue = [&](uint64_t it) {
+    const int slot = (int)((it - it0) % kStages);
+    const uint64_t f0 = it * FPC;
+    const uint64_t nvalid = (p.nf - f0) < (uint64_t)FPC ? (p.nf - f0) : (uint64_t)FPC;
+    const uint32_t b1 = (uint32_t)(nvalid * bpf1), b2 = (uint32_t)(nvalid * bpf2);
+    uint8_t* dst = stage + slot * stage_stride;
+    mbar_expect_tx(&bars[slot], b1 + b2);
+    bulk_g2s(dst, p.st[0].raw + f0 * bpf1, b1, &bars[slot]);
+    bulk_g2s(dst + FPC * bpf1, p.st[1].raw + f0 * bpf2, b2, &bars[slot]);
+  };
+  __syncthreads();
+  if (tid == 0)
+    for (uint64_t it = it0; it < it1 && it < it0 + kStages; ++it) issue(it);
+
+  float acc[BPT + 1][4];
+#pragma unroll
+  for (int i = 0; i <= BPT; ++i)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[i][v] = 0.f;
+  const int a1s = p.a1s, a1e = p.a1e, a2s = p.a2s;
+  const int ov = a1e - a1s;
+  const int sb = a2s - a1s;
+  const int a_gs = p.grid == 0 ? a1s : a2s;  // grid start of the overlap
+  const bool want_acf = (p.products & 1u) != 0;
+  const bool want_xcf = (p.products & 2u) != 0;
+  const bool ov_only = (p.products & 16u) != 0;
+  bool first_flush = true;
+  uint32_t since_flush = 0;
+  double* part = p.partials + (size_t)blockIdx.x * 4 * H;
+
+  auto flush = [&]() {
+#pragma unroll
+    for (int i = 0; i <= BPT; ++i) {
+      const int bin = (i < BPT) ? (tid + T * i) : N / 2;
+      if (i == BPT && tid != 0) continue;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        double* q = part + (size_t)v * H + bin;
+        *q = (first_flush ? 0.0 : *q) + (double)acc[i][v];
+        acc[i][v] = 0.f;
+      }
+    }
+    first_flush = false;
+    since_flush = 0;
+  };
+
+  for (uint64_t it = it0; it < it1; ++it) {
+    const int slot = (int)((it - it0) % kStages);
+    const uint32_t parity = (uint32_t)(((it - it0) / kStages) & 1u);
+    const uint64_t frame_local = it * FPC + g;
+    const bool valid = frame_local < p.nf;
+
+    if (t == 0)
+      frame_info(p.dl, p.first_frame + frame_local, N, p.df_hz, a1s, a2s, &finfo[g]);
+    if (!mbar_wait(&bars[slot], parity, kWaitPolls)) {
+      atomicOr(flag, 1);
+      atomicOr(p.err, ERR_WAIT_TIMEOUT);
+    }
+    // ---- decode both stations of frame slot g into the planes (aliasing B)
+    float* x1 = reinterpret_cast<float*>(bufB) + g * 2 * Geom<N>::FSTRIDE;
+    float* x2 = x1 + Geom<N>::FSTRIDE;
+    {
+      const uint8_t* st = stage + slot * stage_stride;
+      float xs[16];
+      if (valid) {
+        decode16(reinterpret_cast<const uint32_t*>(st + g * bpf1), p.st[0].bits, p.st[0].shkind,
+                 lut, lv, p.st[0].lsb, t, xs);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) xs[i] = 0.f;
+      }
+#pragma unroll
+      for (int i = 0; i < 16; ++i) x1[fpad(16 * t + i)] = xs[i];
+      if (valid) {
+        decode16(reinterpret_cast<const uint32_t*>(st + FPC * bpf1 + g * bpf2), p.st[1].bits,
+                 p.st[1].shkind, lut + 1024, lv + 256, p.st[1].lsb, t, xs);
+      }
+#pragma unroll
+      for (int i = 0; i < 16; ++i) x2[fpad(16 * t + i)] = xs[i];
+    }
+    __syncthreads();
+    if (*flag) break;
+    // staging slot consumed: refill it with iteration it + kStages
+    if (tid == 0 && it + kStages < it1) {
+      fence_proxy_async();
+      issue(it + kStages);
+    }
+    const FrameInfo fi = finfo[g];
+
+    if constexpr (MODE == MODE_DECODE) {
+      if (valid) {
+        float* o1 = p.out_a + frame_local * N;
+        float* o2 = p.out_b + frame_local * N;
+        for (int n = t; n < N; n += T1) {
+          const int m1 = n - fi.s1, m2 = n - fi.s2;
+          o1[n] = ((unsigned)m1 < (unsigned)N) ? x1[fpad(m1)] : 0.f;
+          o2[n] = ((unsigned)m2 < (unsigned)N) ? x2[fpad(m2)] : 0.f;
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+
+    float2* za = bufA + g * Geom<N>::CSTRIDE;
+    float2* zb = bufB + g * Geom<N>::CSTRIDE;
+    first_pass<N>(x1, x2, fi.s1, fi.s2, za, t);
+    float2* Z0 = fft_rest<N>(za, zb, t, tw);
+    // the final buffer sits at the same offset for every frame slot
+    const int fin_off = (int)(Z0 - za) == 0 ? 0 : 1;
+    __syncthreads();
+
+    if constexpr (MODE == MODE_SPECTRA) {
+      if (valid) {
+        float2* o1 = reinterpret_cast<float2*>(p.out_a) + frame_local * H;
+        float2* o2 = reinterpret_cast<float2*>(p.out_b) + frame_local * H;
+        for (int k = t; k < H; k += T1) {
+          const float2 a = Z0[cpad(k)], b = Z0[cpad((N - k) & (N - 1))];
+          o1[k] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+          o2[k] = make_float2(0.5f * (a.y + b.y), -0.5f * (a.x - b.x));
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+
+    // ---- MODE_CORR: accumulate every valid frame of the iteration
+#pragma unroll 1
+    for (int f = 0; f < FPC; ++f) {
+      if (it * FPC + f >= p.nf) break;
+      const float2* Z = (fin_off ? bufB : bufA) + f * Geom<N>::CSTRIDE;
+      const FrameInfo& F = finfo[f];
+      float sn, cs;
+      sincosf(fmaf((float)(tid - a_gs), F.dphi, F.phi0), &sn, &cs);
+      float2 rot = cmul(F.fr_mix, make_float2(cs, sn));
+      sincosf((float)T * F.dphi, &sn, &cs);
+      const float2 rstep = make_float2(cs, sn);
+      auto bin_acc = [&](int bin, float2 r, float* a) {
+        const float2 u = Z[cpad(bin)], w = Z[cpad((N - bin) & (N - 1))];
+        if (p.grid == 0) {
+          const bool inov = bin >= a1s && bin < a1e;
+          const float2 p1 = make_float2(u.x + w.x, u.y - w.y);  // 2*S1[bin]
+          if (want_acf && (!ov_only || inov)) a[0] += cnorm2(p1);
+          if (inov) {
+            const int i2 = bin + sb;
+            const float2 c = Z[cpad(i2)], d = Z[cpad((N - i2) & (N - 1))];
+            const float2 q2 = make_float2(c.y + d.y, d.x - c.x);  // 2*S2[i2]
+            if (want_acf) a[1] += cnorm2(q2);
+            if (want_xcf) {
+              const float2 x = cmul(cmulc(p1, q2), r);
+              a[2] += x.x;
+              a[3] += x.y;
+            }
+          }
+        } else {
+          const bool inov = bin >= a2s && bin < a2s + ov;
+          const float2 p2 = make_float2(u.y + w.y, w.x - u.x);  // 2*S2[bin]
+          if (want_acf && (!ov_only || inov)) a[1] += cnorm2(p2);
+          if (inov) {
+            const int i1 = bin - sb;
+            const float2 c = Z[cpad(i1)], d = Z[cpad((N - i1) & (N - 1))];
+            const float2 q1 = make_float2(c.x + d.x, c.y - d.y);  // 2*S1[i1]
+            if (want_acf) a[0] += cnorm2(q1);
+            if (want_xcf) {
+              const float2 x = cmul(cmulc(q1, p2), r);
+              a[2] += x.x;
+              a[3] += x.y;
+            }
+          }
+        }
+      };
+#pragma unroll
+      for (int i = 0; i < BPT; ++i) {
+        bin_acc(tid + T * i, rot, acc[i]);
+        rot = cmul(rot, rstep);
+      }
+      if (tid == 0) {
+        sincosf(fmaf((float)(N / 2 - a_gs), F.dphi, F.phi0), &sn, &cs);
+        bin_acc(N / 2, cmul(F.fr_mix, make_float2(cs, sn)), acc[BPT]);
+      }
+    }
+    if (++since_flush >= p.flush_every) flush();
+    __syncthreads();
+  }
+  if constexpr (MODE == MODE_CORR) {
+    if (since_flush > 0 || first_flush) flush();
+  }
+  // never leave a bulk copy in flight into a finished CTA's shared memory
+  if (tid == 0 && *flag) {
+    for (int s = 0; s < kStages; ++s) mbar_wait(&bars[s], 0, kWaitPolls);
+  }
+}
+
+// Fixed-order sum of the per-CTA partials; 0.25 undoes the two-for-one 2x
+// scaling of each spectrum.  Writes acf11, acf22, xcf (re,im) and zeroes the
+// phased slot.
+__global__ void reduce_partials_kernel(const double* __restrict__ part, int nblk, int h,
+                                       double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= h) return;
+  double s[4] = {0, 0, 0, 0};
+  for (int b = 0; b < nblk; ++b) {
+    const double* q = part + (size_t)b * 4 * h;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) s[v] += q[(size_t)v * h + k];
+  }
+  out[k] = 0.25 * s[0];
+  out[h + k] = 0.25 * s[1];
+  out[2 * h + 2 * k] = 0.25 * s[2];
+  out[2 * h + 2 * k + 1] = 0.25 * s[3];
+  out[4 * h + k] = 0.0;
+}
+
+__global__ void delay_entries_kernel(const DelayParams p, uint64_t first, uint64_t nf,
+                                     fxc_frame_delay_dev* out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  int64_t i1, i2;
+  double f1, f2;
+  float2 l1, l2;
+  frame_delay(p, first + i, &i1, &i2, &f1, &f2, &l1, &l2);
+  fxc_frame_delay_dev d;
+  d.int1 = i1;
+  d.int2 = i2;
+  d.frac1 = f1;
+  d.frac2 = f2;
+  d.fr_lo1[0] = l1.x;
+  d.fr_lo1[1] = l1.y;
+  d.fr_lo2[0] = l2.x;
+  d.fr_lo2[1] = l2.y;
+  out[i] = d;
+}
+
+// ------------------------------------------------------------- launchers
+
+template <int N, int FPC, int MODE>
+static cudaError_t launch_one(const CorrParams& p, int grid, cudaStream_t stream) {
+  const SmemLayout L = smem_layout<N, FPC>(p.stage_bytes);
+  auto kern = corr_kernel<N, FPC, MODE>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, FPC * N / 16, L.total, stream>>>(p);
+  return cudaGetLastError();
+}
+
+template <int MODE>
+static cudaError_t launch_mode(uint32_t n, const CorrParams& p, int grid, cudaStream_t s) {
+  switch (n) {
+    case 1024: return launch_one<1024, 4, MODE>(p, grid, s);
+    case 2048: return launch_one<2048, 2, MODE>(p, grid, s);
+    case 4096: return launch_one<4096, 1, MODE>(p, grid, s);
+    case 8192: return launch_one<8192, 1, MODE>(p, grid, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int corr_frames_per_cta_iter(uint32_t n) {
+  return n == 1024 ? 4 : (n == 2048 ? 2 : 1);
+}
+
+int corr_ctas_per_sm(uint32_t n) { return n >= 8192 ? 1 : 2; }
+
+uint32_t corr_smem_bytes(uint32_t n, uint32_t stage_bytes) {
+  switch (n) {
+    case 1024: return smem_layout<1024, 4>(stage_bytes).total;
+    case 2048: return smem_layout<2048, 2>(stage_bytes).total;
+    case 4096: return smem_layout<4096, 1>(stage_bytes).total;
+    case 8192: return smem_layout<8192, 1>(stage_bytes).total;
+    default: return 0;
+  }
+}
+
+cudaError_t launch_corr(uint32_t n, int mode, const CorrParams& p, int grid, cudaStream_t s) {
+  if (mode == MODE_CORR) return launch_mode<MODE_CORR>(n, p, grid, s);
+  if (mode == MODE_SPECTRA) return launch_mode<MODE_SPECTRA>(n, p, grid, s);
+  return launch_mode<MODE_DECODE>(n, p, grid, s);
+}
+
+cudaError_t launch_reduce(const double* part, int nblk, int h, double* out, cudaStream_t s) {
+  reduce_partials_kernel<<<(h + 255) / 256, 256, 0, s>>>(part, nblk, h, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_delay_entries(const DelayParams& p, uint64_t first, uint64_t nf,
+                                 fxc_frame_delay_dev* out, cudaStream_t s) {
+  if (nf == 0) return cudaSuccess;
+  delay_entries_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(p, first, nf, out);
+  return cudaGetLastError();
+}
+
+}  // namespace fxc

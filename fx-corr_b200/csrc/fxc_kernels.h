@@ -1,0 +1,64 @@
+// fxc_kernels.h — host-visible launch interface of the sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fxc_device.cuh"
+
+namespace fxc {
+
+enum { MODE_CORR = 0, MODE_SPECTRA = 1, MODE_DECODE = 2 };
+
+struct CorrParams {
+  StationParams st[2];
+  DelayParams dl;
+  uint64_t nf, first_frame;
+  int32_t a1s, a1e, a2s, grid;
+  uint32_t products;
+  uint32_t stage_bytes;  // FPC * (bpf1 + bpf2)
+  uint32_t flush_every;  // iterations between f32 -> f64 flushes
+  double df_hz;
+  double* partials;      // MODE_CORR: [grid][4][H] f64
+  float* out_a;          // MODE_SPECTRA: S1 [nf][H] complex; MODE_DECODE: x1 [nf][N]
+  float* out_b;          // S2 / x2
+  uint32_t* err;         // device error word (ERR_*)
+};
+
+// Layout-compatible with fxc_frame_delay in include/fxc.h.
+struct fxc_frame_delay_dev {
+  int64_t int1, int2;
+  double frac1, frac2;
+  float fr_lo1[2], fr_lo2[2];
+};
+
+// Phased-array kernel parameters (weighted sum, power, C2R, re-quantise).
+struct PhasedParams {
+  StationParams st[2];
+  DelayParams dl;
+  uint64_t nf, first_frame;
+  int32_t a1s, a1e, a2s, grid;
+  uint32_t stage_bytes;
+  uint32_t flush_every;
+  uint32_t bits_out, bpf_out;
+  int32_t out_lsb;       // negate odd output samples (both stations LSB)
+  int32_t want_raw;
+  float w1, w2;
+  double df_hz;
+  const float* qlevels;  // levels1 as f32 (device)
+  uint32_t nqlevels;
+  const uint8_t* shuffle_out;  // 32 entries (device)
+  double* partials;      // [grid][H] f64
+  uint8_t* raw_out;      // nf * bpf_out
+  uint32_t* err;
+};
+
+int corr_frames_per_cta_iter(uint32_t n);
+int corr_ctas_per_sm(uint32_t n);
+uint32_t corr_smem_bytes(uint32_t n, uint32_t stage_bytes);
+cudaError_t launch_corr(uint32_t n, int mode, const CorrParams& p, int grid, cudaStream_t s);
+cudaError_t launch_reduce(const double* part, int nblk, int h, double* out, cudaStream_t s);
+cudaError_t launch_delay_entries(const DelayParams& p, uint64_t first, uint64_t nf,
+                                 fxc_frame_delay_dev* out, cudaStream_t s);
+
+}  // namespace fxc

@@ -1,0 +1,215 @@
+/*
+ * fxc.h — C ABI of the B200 FX-correlation engine (libfxc.so).
+ *
+ * The reference (fx-corr, a Rust CPU correlator) has no plugin or FFI API;
+ * its hot path is the per-sector body of `run_once` (src/main.rs:2173-2683).
+ * This header exposes that seam as plain C: a caller that today runs the
+ * reference's sector loop hands one sector of packed .raw bytes per station
+ * to the engine and receives the same f64 accumulators the reference's rayon
+ * map/reduce produces (src/main.rs:2413-2591), computed on the GPU.
+ *
+ * Conventions
+ *  - Every function returns fxc_status: 0 = FXC_OK, negative = error.  On
+ *    error, fxc_last_error() returns a message for the calling thread.
+ *  - No C++ types, exceptions or torch types cross this boundary: plain
+ *    pointers and sizes only.  "d_" pointers are device (HBM) pointers,
+ *    everything else is host memory.
+ *  - Bins: H = fft_len/2 + 1 per product, index k = 0..H-1, exactly the
+ *    reference's accumulator length (src/main.rs:2166-2167, 2425).
+ *  - Device accumulator block (fxc_*_device): 5*H doubles laid out as
+ *      [0,H)      acf11          (src/main.rs:2432)
+ *      [H,2H)     acf22          (src/main.rs:2434)
+ *      [2H,4H)    xcf, (re,im) interleaved (src/main.rs:2433)
+ *      [4H,5H)    phased power   (src/main.rs:2427)
+ *  - Thread safety: one fxc_scan per host thread; an fxc_engine may be shared
+ *    by several threads, each with its own scans.
+ */
+#ifndef FXC_H
+#define FXC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FXC_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define FXC_API __attribute__((visibility("default")))
+#else
+#define FXC_API
+#endif
+
+typedef int32_t fxc_status;
+enum {
+  FXC_OK = 0,
+  FXC_EINVAL = -1,       /* invalid argument / configuration */
+  FXC_ENOMEM = -2,       /* device or pinned host allocation failed */
+  FXC_ECUDA = -3,        /* CUDA runtime error */
+  FXC_ETIMEDOUT = -4,    /* fxc_sector_wait ran out of time, or a bounded
+                            device-side wait gave up */
+  FXC_ENOTFOUND = -5,    /* unknown sector id */
+  FXC_EBUSY = -6,        /* admission refused: HBM budget or queue depth */
+  FXC_EUNSUPPORTED = -7, /* configuration outside what the kernels handle */
+  FXC_EDEVICE = -8,      /* a kernel reported an error status */
+};
+
+/* Products (which accumulators a scan computes). */
+enum {
+  FXC_PROD_ACF = 1,              /* write_acf_cor  (src/main.rs:1021) */
+  FXC_PROD_XCF = 2,              /* write_xcf_cor  (src/main.rs:1022) */
+  FXC_PROD_PHASED = 4,           /* phased power   (src/main.rs:2154) */
+  FXC_PROD_RAW = 8,              /* phased .raw    (src/main.rs:1020) */
+  FXC_PROD_ACF_OVERLAP_ONLY = 16 /* yi-acf: both ACFs over overlap bins
+                                    only (src/main.rs:2157-2160) */
+};
+
+/* DelayEvalConfig (src/main.rs:161-182).  geom_table == NULL selects the
+ * polynomial branch (src/main.rs:209-230); otherwise the 1-s geometric-delay
+ * table (src/main.rs:1629-1644) is copied by fxc_scan_open. */
+typedef struct fxc_delay_cfg {
+  double frame_dt, fs, time_offset_s;
+  const double* geom_table;
+  uint64_t geom_len;
+  double coarse_delay_s, delay_user_samples, extra_delay_rate_sps;
+  double clock1_delay_s, clock1_rate_sps, clock2_delay_s, clock2_rate_sps;
+  double d_seek;
+  double net_d1_base, total_rate1_base, total_accel1_base;
+  double net_d2_base, total_rate2_base, total_accel2_base;
+  double lo1_hz, lo2_hz;
+} fxc_delay_cfg;
+
+/* FrameDelayEntry (src/main.rs:151-159). */
+typedef struct fxc_frame_delay {
+  int64_t int1, int2;
+  double frac1, frac2;
+  float fr_lo1[2], fr_lo2[2];
+} fxc_frame_delay;
+
+/* Per-scan configuration: the values run_once resolves before its sector
+ * loop (src/main.rs:1063-1212, 1618-1673, 2073-2074). */
+typedef struct fxc_scan_cfg {
+  uint32_t fft_len;  /* N: power of two, 1024..65536 */
+  uint32_t bits1, bits2, bits_out; /* 1,2,4,8; bits_out = max(bits1,bits2) (main.rs:1067) */
+  double fs_hz;
+  double levels1[256], levels2[256]; /* parse_levels (args.rs:194-200) */
+  uint32_t nlevels1, nlevels2;       /* must equal 1 << bits */
+  uint8_t shuffle1[32], shuffle2[32]; /* internal maps from parse_shuffle
+                                         (args.rs:202-210): decoded bit o =
+                                         raw word bit shuffle[o] */
+  int32_t lsb1, lsb2;                /* LSB input: odd samples negated */
+  int32_t shift_bins;                /* BandAlignment (main.rs:360-372) */
+  uint32_t a1s, a1e, a2s;
+  int32_t grid;                      /* 0 = ant1 grid, 1 = ant2 (main.rs:1212) */
+  uint32_t products;                 /* FXC_PROD_* */
+  double w1, w2;                     /* phased weights (args.rs:212-226) */
+  fxc_delay_cfg delay;
+} fxc_scan_cfg;
+
+typedef struct fxc_device_opts {
+  int32_t device;             /* CUDA ordinal */
+  int32_t max_inflight;       /* sectors in flight per scan (0 = 2) */
+  uint64_t hbm_budget_bytes;  /* admission budget for scans (0 = 80% of free) */
+} fxc_device_opts;
+
+/* Host-side results of one sector.  Any pointer may be NULL to skip it. */
+typedef struct fxc_sector_out {
+  double* acf11;   /* H doubles */
+  double* acf22;   /* H doubles */
+  double* xcf;     /* 2*H doubles, (re,im) interleaved */
+  double* phased;  /* H doubles */
+  uint8_t* raw_out;       /* nf * bytes_per_frame(bits_out) bytes */
+  uint64_t raw_out_len;
+  uint64_t frames_failed; /* frames skipped (src/main.rs:2592-2599) */
+} fxc_sector_out;
+
+typedef struct fxc_engine fxc_engine;
+typedef struct fxc_scan fxc_scan;
+
+/* ---- library ---------------------------------------------------------- */
+FXC_API int32_t fxc_abi_version(void);
+FXC_API const char* fxc_status_string(fxc_status s);
+/* Message of the last error on the calling thread ("" if none). */
+FXC_API const char* fxc_last_error(void);
+
+/* ---- engine (owns device memory, streams, graphs) ---------------------- */
+FXC_API fxc_status fxc_engine_create(const fxc_device_opts* opts, fxc_engine** out);
+FXC_API fxc_status fxc_engine_destroy(fxc_engine* e);
+
+/* ---- scan (replaces run_once's per-scan set-up, src/main.rs:1013-2172) -- */
+FXC_API fxc_status fxc_scan_open(fxc_engine* e, const fxc_scan_cfg* cfg, fxc_scan** out);
+FXC_API fxc_status fxc_scan_close(fxc_scan* s);
+
+/* Asynchronous per-sector call on host buffers (replaces the body of the
+ * sector loop, src/main.rs:2173-2591).  raw1/raw2 hold nf frames of
+ * bytes_per_frame(bits) bytes each, exactly the reader thread's message
+ * (src/main.rs:2135-2147).  first_frame is the scan-global index of frame 0
+ * (the reference's `emitted`).  The buffers must stay unchanged until
+ * fxc_sector_wait returns for the returned id. */
+FXC_API fxc_status fxc_sector_submit(fxc_scan* s, const uint8_t* raw1, uint64_t n1, const uint8_t* raw2,
+                             uint64_t n2, uint64_t nf, uint64_t first_frame, uint64_t* sector_id);
+/* Wait (timeout_ms < 0: no limit) and copy results out. */
+FXC_API fxc_status fxc_sector_wait(fxc_scan* s, uint64_t sector_id, int32_t timeout_ms,
+                           fxc_sector_out* out);
+
+/* ---- device-resident entry points (inputs already in HBM) -------------- */
+/* One sector with inputs resident in device memory; enqueued on `stream`
+ * (a cudaStream_t, NULL = legacy default).  d_acc receives the 5*H-double
+ * accumulator block.  d_raw_out (nf*bytes_per_frame(bits_out) bytes) is
+ * written when the scan has FXC_PROD_RAW.  Device inputs must be 16-byte
+ * aligned.  Asynchronous: call fxc_scan_check(s) after synchronising. */
+FXC_API fxc_status fxc_sector_run_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t* d_raw2,
+                                 uint64_t nf, uint64_t first_frame, double* d_acc,
+                                 uint8_t* d_raw_out, void* stream);
+/* Reads and clears the scan's device error word (bounded waits, bad sizes);
+ * FXC_OK when no kernel reported an error.  Synchronises the scan's work. */
+FXC_API fxc_status fxc_scan_check(fxc_scan* s);
+
+/* Kernel timing: when enabled, every correlation-kernel launch of this scan
+ * is bracketed by CUDA events on its launch stream.  fxc_scan_profile sums
+ * their elapsed device time (synchronising on the last event) and reports the
+ * number of those launches and of all library kernel launches since the last
+ * reset. */
+FXC_API fxc_status fxc_scan_set_profiling(fxc_scan* s, int32_t enable);
+FXC_API fxc_status fxc_scan_profile(fxc_scan* s, double* kernel_ms, uint64_t* kernel_launches,
+                                    uint64_t* all_launches, int32_t reset);
+
+/* Stage entry points, for parity tests of the individual steps. */
+/* Per-frame delay model on the device (src/main.rs:184-241). */
+FXC_API fxc_status fxc_delay_entries_device(fxc_scan* s, uint64_t first_frame, uint64_t nf,
+                                    fxc_frame_delay* d_out, void* stream);
+/* Decode + LSB flip + integer shift of both stations (src/utils.rs:215-376,
+ * 126-145): d_x1, d_x2 = nf*fft_len f32 each, shifted by the delay model's
+ * int1 / int2 for each frame. */
+FXC_API fxc_status fxc_decode_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t* d_raw2,
+                             uint64_t nf, uint64_t first_frame, float* d_x1, float* d_x2,
+                             void* stream);
+/* R2C spectra of both stations after decode+shift (src/utils.rs:47-59):
+ * d_s1, d_s2 = nf*H complex f32 ((re,im) interleaved). */
+FXC_API fxc_status fxc_spectra_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t* d_raw2,
+                              uint64_t nf, uint64_t first_frame, float* d_s1, float* d_s2,
+                              void* stream);
+
+/* ---- host helpers (no GPU needed) --------------------------------------- */
+/* parse_shuffle (args.rs:202-210): external MSB-first list -> internal map. */
+FXC_API fxc_status fxc_parse_shuffle(const int32_t ext[32], uint8_t internal[32]);
+/* compute_band_alignment (main.rs:363-372): out = {shift_bins, a1s, a1e, a2s}. */
+FXC_API fxc_status fxc_band_alignment(uint32_t fft, double fs_hz, double c1_mhz, double c2_mhz,
+                              double bw1_mhz, double bw2_mhz, int64_t out[4]);
+/* quantization_mean_power (main.rs:378-387). */
+FXC_API fxc_status fxc_level_power(const double* levels, uint32_t n, double* out);
+/* Sector normalisation + .cor dump values (main.rs:2645-2683): first fft/2
+ * bins as f32 (re,im) pairs; acc_cplx (2*H doubles) for XCF, else acc_real. */
+FXC_API fxc_status fxc_normalize(uint32_t fft, uint64_t nf, double level_power, const double* acc_real,
+                         const double* acc_cplx, float* out);
+/* bytes per frame, (fft*bits + 7)/8 (main.rs:1214-1215). */
+FXC_API uint64_t fxc_bytes_per_frame(uint32_t fft, uint32_t bits);
+/* Measured FP32 FMA throughput of the device (TFLOP/s), for rooflines. */
+FXC_API fxc_status fxc_probe_fp32_peak(int32_t device, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

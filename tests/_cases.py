@@ -1,0 +1,100 @@
+"""Shared test cases: scan builders, seeded inputs and the spectral
+comparison used by every parity test.
+
+Tolerance (stated against the FP64 oracle, as the correlation path is
+floating point): per-bin relative amplitude error <= 1e-5 and phase error
+<= 1e-4 rad, on every bin whose oracle magnitude is at least 5% of the RMS
+magnitude of that product (bins nearer zero carry absolute errors of the
+same size, which a relative metric would inflate); on all bins the absolute
+error must stay <= 1e-5 * RMS.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+import oracle
+
+REL_AMP_TOL = 1e-5
+PHASE_TOL = 1e-4
+FLOOR = 0.05
+
+
+def make_scan(fft=1024, fs=32e6, bits1=2, bits2=2, shuffle="identity", lsb1=False, lsb2=False,
+              band=None, grid=0, products=oracle.PROD_ACF | oracle.PROD_XCF, delay=None,
+              table=None, levels1=None, levels2=None, seed=0, w1=1.0, w2=1.0):
+    def sh(kind, s):
+        if kind == "identity":
+            return list(range(32))
+        if kind == "pairswap":
+            return [i ^ 1 for i in range(32)]
+        return oracle.random_shuffle(s)
+
+    return oracle.Scan(
+        fft=fft, fs=fs, bits1=bits1, bits2=bits2,
+        levels1=levels1 or oracle.default_levels(bits1),
+        levels2=levels2 or oracle.default_levels(bits2),
+        shuffle1=sh(shuffle, seed + 11), shuffle2=sh(shuffle, seed + 12),
+        lsb1=lsb1, lsb2=lsb2, band=band, grid=grid, products=products, w1=w1, w2=w2,
+        delay=dict(delay or {}), geom_table=None if table is None else np.asarray(table, float))
+
+
+def to_fxc(scan: oracle.Scan):
+    import fxc
+
+    d = dataclasses.asdict(scan)
+    d["geom_table"] = scan.geom_table
+    return fxc.ScanConfig(**d)
+
+
+def random_raw(scan, nf, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    r1 = rng.integers(0, 256, nf * scan.bpf(scan.bits1), dtype=np.uint8)
+    r2 = rng.integers(0, 256, nf * scan.bpf(scan.bits2), dtype=np.uint8)
+    return r1, r2
+
+
+def signal_raw(scan, nf, seed, rho=0.05, delay_samples=0.0, tone_bin=None):
+    """Seeded quantised Gaussian streams with a common component (rho) whose
+    copy at station 2 is delayed by delay_samples."""
+    n = nf * scan.fft
+    x1, x2 = oracle.synth_station_pair(n, seed, rho=rho, delay_samples=delay_samples,
+                                       tone_bin=tone_bin, fft=scan.fft)
+    r1 = oracle.encode_station(x1, scan.bits1, scan.levels1, scan.shuffle1, scan.lsb1)
+    r2 = oracle.encode_station(x2, scan.bits2, scan.levels2, scan.shuffle2, scan.lsb2)
+    return r1, r2
+
+
+def spectral_errors(a, b):
+    """(max relative amplitude error, max phase error, max abs error / rms)
+    of a against reference b, on bins with |b| >= FLOOR * rms(|b|)."""
+    a = np.asarray(a, np.complex128)
+    b = np.asarray(b, np.complex128)
+    mag = np.abs(b)
+    rms = float(np.sqrt(np.mean(mag ** 2))) if mag.size else 0.0
+    if rms == 0.0:
+        return 0.0, 0.0, float(np.abs(a).max()) if a.size else 0.0
+    m = mag >= FLOOR * rms
+    rel = float(np.max(np.abs(np.abs(a[m]) - mag[m]) / mag[m])) if m.any() else 0.0
+    ph = float(np.max(np.abs(np.angle(a[m] * np.conj(b[m]))))) if m.any() else 0.0
+    ab = float(np.max(np.abs(a - b)) / rms)
+    return rel, ph, ab
+
+
+def assert_spectra_close(a, b, what, rel_tol=REL_AMP_TOL, phase_tol=PHASE_TOL):
+    rel, ph, ab = spectral_errors(a, b)
+    assert rel <= rel_tol and ph <= phase_tol and ab <= rel_tol, (
+        f"{what}: rel amp {rel:.3e} (tol {rel_tol}), phase {ph:.3e} rad (tol {phase_tol}), "
+        f"abs/rms {ab:.3e}")
+    return rel, ph, ab
+
+
+def assert_sector_close(got, ref, scan, what):
+    out = {}
+    if scan.products & oracle.PROD_ACF:
+        out["acf11"] = assert_spectra_close(got["acf11"], ref["acf11"], what + " acf11")
+        out["acf22"] = assert_spectra_close(got["acf22"], ref["acf22"], what + " acf22")
+    if scan.products & oracle.PROD_XCF:
+        out["xcf"] = assert_spectra_close(got["xcf"], ref["xcf"], what + " xcf")
+    return out
