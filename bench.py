@@ -297,6 +297,11 @@ def main():
     ap.add_argument("--impl", default="fxc", choices=["fxc", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e leg")
+    ap.add_argument("--sectors", type=int, default=SECTORS,
+                    help="sectors per step (profiling cases only; the workload is 10)")
+    ap.add_argument("--frames-per-sector", type=int, default=NF_SECTOR,
+                    help="frame pairs per sector (profiling cases only; the workload is 125000)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -338,18 +343,20 @@ def main():
     stream = torch.cuda.Stream()
 
     # ---- inputs resident in HBM: 10 sectors x 2 stations x 256 MB
-    nsamp = SECTORS * NF_SECTOR * N
+    SECTORS_, NFS = args.sectors, args.frames_per_sector
+    full = SECTORS_ == SECTORS and NFS == NF_SECTOR
+    nsamp = SECTORS_ * NFS * N
     d1, d2 = gen_station_pair_gpu(torch, nsamp, seed=1000 + rank, cfg=cfg)
     bpf = N * BITS // 8
-    sec_bytes = NF_SECTOR * bpf
-    sec1 = [d1[i * sec_bytes:(i + 1) * sec_bytes] for i in range(SECTORS)]
-    sec2 = [d2[i * sec_bytes:(i + 1) * sec_bytes] for i in range(SECTORS)]
+    sec_bytes = NFS * bpf
+    sec1 = [d1[i * sec_bytes:(i + 1) * sec_bytes] for i in range(SECTORS_)]
+    sec2 = [d2[i * sec_bytes:(i + 1) * sec_bytes] for i in range(SECTORS_)]
     h = cfg.h
-    accs = [torch.empty(5 * h, dtype=torch.float64, device="cuda") for _ in range(SECTORS)]
+    accs = [torch.empty(5 * h, dtype=torch.float64, device="cuda") for _ in range(SECTORS_)]
 
     def step():
-        for i in range(SECTORS):
-            scan.run_device(sec1[i], sec2[i], NF_SECTOR, i * NF_SECTOR, accs[i], stream=stream)
+        for i in range(SECTORS_):
+            scan.run_device(sec1[i], sec2[i], NFS, i * NFS, accs[i], stream=stream)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -373,43 +380,45 @@ def main():
     scan.set_profiling(False)
     scan.check()
     ms = max_over_ranks(ms)
-    samples_per_step = 2 * SECTORS * NF_SECTOR * N
+    samples_per_step = 2 * SECTORS_ * NFS * N
     value = world * samples_per_step / (ms * 1e-3) / 1e9
 
     # ---- end to end through the host-buffer C ABI (pinned host inputs)
-    e2e_value, bi, bo = None, 0, 0
-    h1 = [s.cpu().pin_memory() for s in sec1]
-    h2 = [s.cpu().pin_memory() for s in sec2]
-    n1 = [t.numpy() for t in h1]
-    n2 = [t.numpy() for t in h2]
+    e2e = None
+    if not args.no_e2e:
+        h1 = [s.cpu().pin_memory() for s in sec1]
+        h2 = [s.cpu().pin_memory() for s in sec2]
+        n1 = [t.numpy() for t in h1]
+        n2 = [t.numpy() for t in h2]
 
-    def e2e_step():
-        ids = []
-        res = []
-        for i in range(SECTORS):
-            if len(ids) == 3:
+        def e2e_step():
+            ids = []
+            res = []
+            for i in range(SECTORS_):
+                if len(ids) == 3:
+                    res.append(scan.wait(ids.pop(0)))
+                ids.append(scan.submit(n1[i], n2[i], NFS, i * NFS))
+            while ids:
                 res.append(scan.wait(ids.pop(0)))
-            ids.append(scan.submit(n1[i], n2[i], NF_SECTOR, i * NF_SECTOR))
-        while ids:
-            res.append(scan.wait(ids.pop(0)))
-        return res
+            return res
 
-    e2e_step()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
         e2e_step()
-    t1 = time.perf_counter()
-    barrier()
-    e2e_ms = max_over_ranks((t1 - t0) * 1e3 / args.e2e_steps)
-    e2e_value = world * samples_per_step / (e2e_ms * 1e-3) / 1e9
-    bi = 2 * SECTORS * sec_bytes
-    bo = SECTORS * (5 * h * 8 + 4)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        t1 = time.perf_counter()
+        barrier()
+        e2e_ms = max_over_ranks((t1 - t0) * 1e3 / args.e2e_steps)
+        e2e = {"value": world * samples_per_step / (e2e_ms * 1e-3) / 1e9, "unit": "Gsample/s",
+               "h2d_bytes_per_step": 2 * SECTORS_ * sec_bytes,
+               "d2h_bytes_per_step": SECTORS_ * (5 * h * 8 + 4), "ms_per_step": e2e_ms,
+               "path": "fxc_sector_submit/fxc_sector_wait, pinned host buffers"}
     clk = clocks.stop()
 
     # ---- roofline of the dominant kernel (correlation kernel, one sector per launch)
     launch_ms = kern_ms / max(1, kern_launches)
-    flops_launch = flops_per_station_sample(N) * 2 * NF_SECTOR * N
+    flops_launch = flops_per_station_sample(N) * 2 * NFS * N
     fp32_peak = fxc.probe_fp32_peak(local)
     hbm_peak, peak_kind = measured_peaks()
     bytes_launch = 2 * sec_bytes + 5 * h * 8
@@ -418,7 +427,7 @@ def main():
         "bound": "fp32", "achieved": flops_launch / (launch_ms * 1e-3) / 1e12,
         "peak": fp32_peak, "unit": "TFLOP/s",
         "frac": flops_launch / (launch_ms * 1e-3) / 1e12 / fp32_peak,
-        "traffic": None if tpf is None else tpf * NF_SECTOR,
+        "traffic": None if tpf is None else tpf * NFS,
         "kernel": "corr_kernel<8192,1,0>", "launch_ms": launch_ms,
         "algorithmic_flops_per_launch": flops_launch,
         "peak_source": "live FMA probe of this GPU (fxc_probe_fp32_peak)",
@@ -445,15 +454,15 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded quantised Gaussian, rho=0.05, generated on device)",
-            "config": {"workload": WORKLOAD, "fft": N, "fs_hz": FS, "bits": BITS,
-                       "scan_s": SCAN_S, "sectors": SECTORS, "frames_per_sector": NF_SECTOR,
+            "config": {"workload": WORKLOAD if full else
+                       f"profiling case ({SECTORS_} x {NFS} frame pairs) of: {WORKLOAD}",
+                       "fft": N, "fs_hz": FS, "bits": BITS,
+                       "scan_s": SCAN_S, "sectors": SECTORS_, "frames_per_sector": NFS,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (512 MB per sector, 5.12 GB per step)"},
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "Gsample/s", "h2d_bytes_per_step": bi,
-                    "d2h_bytes_per_step": bo, "ms_per_step": e2e_ms,
-                    "path": "fxc_sector_submit/fxc_sector_wait, pinned host buffers"},
+            "e2e": e2e,
             "gpu_launches": all_launches,
             "clocks": clk,
             "realtime_factor": value / (2 * FS / 1e9),

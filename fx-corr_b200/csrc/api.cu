@@ -63,6 +63,7 @@ struct fxc_engine {
   uint64_t budget = 0;
   uint64_t in_use = 0;
   std::mutex mu;
+  std::vector<fxc_scan*> scans;  // open scans, closed by fxc_engine_destroy
 };
 
 struct SectorSlot {
@@ -87,12 +88,15 @@ struct fxc_scan {
   uint32_t n = 0, h = 0;
   uint32_t bpf1 = 0, bpf2 = 0, bpfo = 0;
   int shkind[2] = {0, 0};
+  float scale[2] = {1.0f, 1.0f};  // exact powers of two (see level_scale)
   double* d_table = nullptr;
   uint32_t* d_lut = nullptr;     // [2][1024]
   float* d_levels = nullptr;     // [2][256]
   uint8_t* d_shuffle_out = nullptr;
   double* d_partials = nullptr;
   uint64_t partials_elems = 0;
+  FrameInfo* d_finfo = nullptr;  // per-frame delay records of the sector in flight
+  uint64_t finfo_cap = 0;
   uint32_t* d_err = nullptr;
   cudaStream_t stream = nullptr;     // compute
   cudaStream_t copy_stream = nullptr;
@@ -127,6 +131,19 @@ void build_lut(const uint8_t sh[32], uint32_t* lut) {
     for (int v = 0; v < 256; ++v)
       if ((v >> bit) & 1) lut[byte * 256 + v] |= (1u << o);
   }
+}
+
+// Power of two nearest 1/RMS of a level table.  Both stations share one
+// complex FFT (z = x1 + i x2), so rounding error scales with the stronger
+// station; equalising the RMS by an exact power of two keeps the weaker
+// station's spectrum at full f32 relative precision and is undone exactly.
+float level_scale(const double* lv, uint32_t n) {
+  double p = 0.0;
+  for (uint32_t i = 0; i < n; ++i) p += lv[i] * lv[i];
+  p /= (double)n;
+  if (!(p > 0.0) || !std::isfinite(p)) return 1.0f;
+  const int e = (int)std::lround(0.5 * std::log2(p));
+  return std::ldexp(1.0f, -e);
 }
 
 DelayParams delay_params(const fxc_scan* s) {
@@ -166,6 +183,7 @@ void station_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2, Sta
     st[k].bits = (int)(k ? s->cfg.bits2 : s->cfg.bits1);
     st[k].lsb = k ? s->cfg.lsb2 : s->cfg.lsb1;
     st[k].shkind = s->shkind[k];
+    st[k].scale = s->scale[k];
   }
 }
 
@@ -193,8 +211,26 @@ CorrParams corr_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2, 
   p.flush_every = (uint32_t)std::max(1, 32 / fpc);
   p.df_hz = s->cfg.fs_hz / (double)s->n;
   p.partials = s->d_partials;
+  p.finfo = s->d_finfo;
   p.err = s->d_err;
   return p;
+}
+
+// Per-frame delay records for nf frames starting at `first` (FP64 delay model,
+// one thread per frame) into the scan's record buffer, on stream st.
+fxc_status stage_frame_info(fxc_scan* s, uint64_t first, uint64_t nf, cudaStream_t st) {
+  if (nf > s->finfo_cap) {
+    // growing frees the old buffer; cudaFree waits for the work that reads it
+    cudaFree(s->d_finfo);
+    s->d_finfo = nullptr;
+    s->finfo_cap = 0;
+    const uint64_t cap = std::max<uint64_t>(nf, 1u << 17);
+    CK(cudaMalloc(&s->d_finfo, cap * sizeof(FrameInfo)));
+    s->finfo_cap = cap;
+  }
+  CK(launch_frame_info(delay_params(s), first, nf, (int)s->n, s->cfg.fs_hz / (double)s->n,
+                       (int)s->cfg.a1s, (int)s->cfg.a2s, s->d_finfo, st));
+  return FXC_OK;
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -274,6 +310,8 @@ fxc_status run_corr_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, ui
     return FXC_OK;
   }
   const int grid = corr_grid(s, nf);
+  fxc_status fst = stage_frame_info(s, first, nf, st);
+  if (fst != FXC_OK) return fst;
   CorrParams p = corr_params(s, r1, r2, nf, first);
   std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
   if (s->profiling) {
@@ -288,9 +326,11 @@ fxc_status run_corr_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, ui
   }
   CK(launch_corr(s->n, MODE_CORR, p, grid, st));
   if (ev) CK(cudaEventRecord(ev->second, st));
-  CK(launch_reduce(s->d_partials, grid, (int)h, d_acc, st));
+  const double u1 = 1.0 / s->scale[0], u2 = 1.0 / s->scale[1];
+  CK(launch_reduce(s->d_partials, grid, (int)h, 0.25 * u1 * u1, 0.25 * u2 * u2, 0.25 * u1 * u2,
+                   d_acc, st));
   s->kernel_launches += 1;
-  s->all_launches += 2;
+  s->all_launches += 3;
   return FXC_OK;
 }
 
@@ -344,6 +384,13 @@ fxc_status fxc_engine_create(const fxc_device_opts* opts, fxc_engine** out) {
 }
 
 fxc_status fxc_engine_destroy(fxc_engine* e) {
+  if (!e) return FXC_OK;
+  std::vector<fxc_scan*> open;
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    open = e->scans;
+  }
+  for (fxc_scan* s : open) fxc_scan_close(s);
   delete e;
   return FXC_OK;
 }
@@ -364,6 +411,8 @@ fxc_status fxc_scan_open(fxc_engine* e, const fxc_scan_cfg* cfg, fxc_scan** out)
   s->bpfo = (uint32_t)fxc_bytes_per_frame(s->n, cfg->bits_out);
   s->shkind[0] = shuffle_kind(cfg->shuffle1);
   s->shkind[1] = shuffle_kind(cfg->shuffle2);
+  s->scale[0] = level_scale(cfg->levels1, cfg->nlevels1);
+  s->scale[1] = level_scale(cfg->levels2, cfg->nlevels2);
   const uint64_t maxg = (uint64_t)e->sm_count * (uint64_t)corr_ctas_per_sm(s->n);
   s->partials_elems = maxg * 4 * s->h;
   const uint64_t need = s->partials_elems * 8 + 2 * 1024 * 4 + 2 * 256 * 4 + 64 +
@@ -423,6 +472,10 @@ fxc_status fxc_scan_open(fxc_engine* e, const fxc_scan_cfg* cfg, fxc_scan** out)
     CKS(cudaMallocHost(&sl.h_acc, sizeof(double) * 5 * s->h + 16));
   }
 #undef CKS
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    e->scans.push_back(s);
+  }
   *out = s;
   return FXC_OK;
 }
@@ -447,6 +500,7 @@ fxc_status fxc_scan_close(fxc_scan* s) {
     cudaEventDestroy(pr.second);
   }
   cudaFree(s->d_partials);
+  cudaFree(s->d_finfo);
   cudaFree(s->d_lut);
   cudaFree(s->d_levels);
   cudaFree(s->d_shuffle_out);
@@ -457,6 +511,8 @@ fxc_status fxc_scan_close(fxc_scan* s) {
   {
     std::lock_guard<std::mutex> lk(s->eng->mu);
     s->eng->in_use -= std::min(s->eng->in_use, s->hbm_bytes);
+    auto& v = s->eng->scans;
+    v.erase(std::remove(v.begin(), v.end(), s), v.end());
   }
   delete s;
   return FXC_OK;
@@ -531,6 +587,8 @@ fxc_status fxc_decode_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t* 
   if (nf == 0) return FXC_OK;
   if (!d_x1 || !d_x2) return fail(FXC_EINVAL, "output pointer is NULL");
   DeviceGuard g(s->eng->device);
+  st = stage_frame_info(s, first_frame, nf, (cudaStream_t)stream);
+  if (st != FXC_OK) return st;
   CorrParams p = corr_params(s, d_raw1, d_raw2, nf, first_frame);
   p.out_a = d_x1;
   p.out_b = d_x2;
@@ -546,6 +604,8 @@ fxc_status fxc_spectra_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t*
   if (nf == 0) return FXC_OK;
   if (!d_s1 || !d_s2) return fail(FXC_EINVAL, "output pointer is NULL");
   DeviceGuard g(s->eng->device);
+  st = stage_frame_info(s, first_frame, nf, (cudaStream_t)stream);
+  if (st != FXC_OK) return st;
   CorrParams p = corr_params(s, d_raw1, d_raw2, nf, first_frame);
   p.out_a = d_s1;
   p.out_b = d_s2;

@@ -1,20 +1,24 @@
 // corr_kernels.cu — the fused FX-correlation kernel for sm_100a.
 //
-// One CTA processes a contiguous run of frame pairs of a sector.  Per frame
-// pair (station 1 and 2 share one complex FFT: z = x1 + i*x2):
-//   1. the packed .raw words of both stations arrive in shared memory by
-//      cp.async.bulk (TMA bulk copy) tracked by an mbarrier, two stages deep;
-//   2. decode: 32-bit word shuffle, b-bit codes -> f32 levels, LSB->USB flip
-//      of odd samples (src/utils.rs:215-376);
-//   3. per-frame FP64 delay model (src/main.rs:184-241) -> integer shifts,
-//      fringe phasors and the fractional-delay phase ramp;
-//   4. first radix-16 pass reads the planes with the integer shift and zero
-//      fill (src/utils.rs:126-145), remaining Stockham passes in shared memory;
-//   5. two-for-one split of Z into S1, S2 (the two real FFTs,
+// frame_info_kernel evaluates the FP64 per-frame delay model
+// (src/main.rs:184-241) for every frame of a sector, one thread per frame, into
+// 48-byte FrameInfo records.
+//
+// corr_kernel: one CTA processes a contiguous run of frame pairs of a sector.
+// Per frame pair (stations 1 and 2 share one complex FFT: z = x1 + i*x2):
+//   1. the frame's FrameInfo and the packed .raw words of both stations arrive
+//      in shared memory by cp.async.bulk (TMA bulk copy) tracked by an
+//      mbarrier, two stages deep;
+//   2. decode: 32-bit word shuffle, b-bit codes -> f32 levels, LSB->USB flip of
+//      odd samples (src/utils.rs:215-376);
+//   3. the first radix-16 pass reads the decoded planes with the integer shift
+//      and zero fill (src/utils.rs:126-145); the remaining Stockham passes run
+//      in padded shared memory;
+//   4. two-for-one split of Z into S1, S2 (the two real FFTs,
 //      src/utils.rs:47-59), band alignment, fringe x phase-ramp rotation and
 //      |S|^2 / S1 conj(S2) accumulation (src/main.rs:2491-2568) into per-thread
 //      f32 registers, flushed every 32 frames into per-CTA f64 partials;
-//   6. a second kernel reduces the per-CTA partials in a fixed order.
+// reduce_partials_kernel then sums the per-CTA partials in a fixed order.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -25,22 +29,25 @@ namespace fxc {
 
 constexpr int kStages = 2;
 constexpr uint32_t kWaitPolls = 1u << 26;  // bounded mbarrier wait
+constexpr uint32_t kFiBytes = sizeof(FrameInfo);
 
 struct SmemLayout {
-  uint32_t off_a, off_b, off_stage, off_lut, off_lv, off_fi, off_bar, off_flag, total;
+  uint32_t off_a, off_b, off_stage, stage_stride, off_lut, off_lv, off_fi, off_bar, off_flag, total;
 };
 
+// Staging slot: [FPC FrameInfo][FPC frames of station 1][FPC frames of station 2]
 template <int N, int FPC>
-__host__ __device__ inline SmemLayout smem_layout(uint32_t stage_bytes) {
+__host__ __device__ inline SmemLayout smem_layout(uint32_t raw_bytes) {
   SmemLayout L;
   const uint32_t cbytes = (uint32_t)(FPC * Geom<N>::CSTRIDE * sizeof(float2));
   L.off_a = 0;
   L.off_b = L.off_a + cbytes;
   L.off_stage = L.off_b + cbytes;
-  L.off_lut = L.off_stage + kStages * ((stage_bytes + 127u) & ~127u);
+  L.stage_stride = (FPC * kFiBytes + raw_bytes + 127u) & ~127u;
+  L.off_lut = L.off_stage + kStages * L.stage_stride;
   L.off_lv = L.off_lut + 2 * 1024 * 4;
   L.off_fi = L.off_lv + 2 * 256 * 4;
-  L.off_bar = L.off_fi + ((FPC * (uint32_t)sizeof(FrameInfo) + 15u) & ~15u);
+  L.off_bar = L.off_fi + FPC * kFiBytes;
   L.off_flag = L.off_bar + kStages * 8;
   L.total = L.off_flag + 16;
   return L;
@@ -53,14 +60,13 @@ corr_kernel(const CorrParams p) {
   constexpr int T = FPC * T1;
   constexpr int H = N / 2 + 1;
   constexpr int BPT = (N / 2) / T;
-  static_assert(BPT * T == N / 2, "bins per thread");
+  static_assert(BPT * T == N / 2 && BPT >= 2, "bins per thread");
 
   extern __shared__ __align__(128) uint8_t smem[];
   const SmemLayout L = smem_layout<N, FPC>(p.stage_bytes);
   float2* bufA = reinterpret_cast<float2*>(smem + L.off_a);
   float2* bufB = reinterpret_cast<float2*>(smem + L.off_b);
   uint8_t* stage = smem + L.off_stage;
-  const uint32_t stage_stride = (p.stage_bytes + 127u) & ~127u;
   uint32_t* lut = reinterpret_cast<uint32_t*>(smem + L.off_lut);
   float* lv = reinterpret_cast<float*>(smem + L.off_lv);
   FrameInfo* finfo = reinterpret_cast<FrameInfo*>(smem + L.off_fi);
@@ -71,8 +77,8 @@ corr_kernel(const CorrParams p) {
   const int g = tid / T1;  // frame slot of this thread in an iteration
   const int t = tid % T1;  // thread index within its frame pair
 
-  // ---- constant tables: levels, shuffle byte LUTs
-  for (int i = tid; i < 512; i += T) lv[i] = p.st[i >> 8].levels[i & 255];
+  // ---- constant tables: levels (scaled by an exact power of two), shuffle LUTs
+  for (int i = tid; i < 512; i += T) lv[i] = p.st[i >> 8].levels[i & 255] * p.st[i >> 8].scale;
   for (int s = 0; s < 2; ++s)
     if (p.st[s].shkind == SH_GENERIC)
       for (int i = tid; i < 1024; i += T) lut[s * 1024 + i] = p.st[s].shlut[i];
@@ -89,16 +95,19 @@ corr_kernel(const CorrParams p) {
   const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
   const uint64_t it1 = ((blockIdx.x + 1) * iters) / gridDim.x;
   const uint32_t bpf1 = p.st[0].bpf, bpf2 = p.st[1].bpf;
+  constexpr uint32_t kRaw1 = FPC * kFiBytes;  // offset of station 1 bytes in a slot
 
   auto issue = [&](uint64_t it) {
     const int slot = (int)((it - it0) % kStages);
     const uint64_t f0 = it * FPC;
     const uint64_t nvalid = (p.nf - f0) < (uint64_t)FPC ? (p.nf - f0) : (uint64_t)FPC;
+    const uint32_t bf = (uint32_t)(nvalid * kFiBytes);
     const uint32_t b1 = (uint32_t)(nvalid * bpf1), b2 = (uint32_t)(nvalid * bpf2);
-    uint8_t* dst = stage + slot * stage_stride;
-    mbar_expect_tx(&bars[slot], b1 + b2);
-    bulk_g2s(dst, p.st[0].raw + f0 * bpf1, b1, &bars[slot]);
-    bulk_g2s(dst + FPC * bpf1, p.st[1].raw + f0 * bpf2, b2, &bars[slot]);
+    uint8_t* dst = stage + slot * L.stage_stride;
+    mbar_expect_tx(&bars[slot], bf + b1 + b2);
+    bulk_g2s(dst, p.finfo + f0, bf, &bars[slot]);
+    bulk_g2s(dst + kRaw1, p.st[0].raw + f0 * bpf1, b1, &bars[slot]);
+    bulk_g2s(dst + kRaw1 + FPC * bpf1, p.st[1].raw + f0 * bpf2, b2, &bars[slot]);
   };
   __syncthreads();
   if (tid == 0)
@@ -142,21 +151,20 @@ corr_kernel(const CorrParams p) {
     const uint64_t frame_local = it * FPC + g;
     const bool valid = frame_local < p.nf;
 
-    if (t == 0)
-      frame_info(p.dl, p.first_frame + frame_local, N, p.df_hz, a1s, a2s, &finfo[g]);
     if (!mbar_wait(&bars[slot], parity, kWaitPolls)) {
       atomicOr(flag, 1);
       atomicOr(p.err, ERR_WAIT_TIMEOUT);
     }
+    const uint8_t* st = stage + slot * L.stage_stride;
+    if (t == 0 && valid) finfo[g] = reinterpret_cast<const FrameInfo*>(st)[g];
     // ---- decode both stations of frame slot g into the planes (aliasing B)
     float* x1 = reinterpret_cast<float*>(bufB) + g * 2 * Geom<N>::FSTRIDE;
     float* x2 = x1 + Geom<N>::FSTRIDE;
     {
-      const uint8_t* st = stage + slot * stage_stride;
       float xs[16];
       if (valid) {
-        decode16(reinterpret_cast<const uint32_t*>(st + g * bpf1), p.st[0].bits, p.st[0].shkind,
-                 lut, lv, p.st[0].lsb, t, xs);
+        decode16(reinterpret_cast<const uint32_t*>(st + kRaw1 + g * bpf1), p.st[0].bits,
+                 p.st[0].shkind, lut, lv, p.st[0].lsb, t, xs);
       } else {
 #pragma unroll
         for (int i = 0; i < 16; ++i) xs[i] = 0.f;
@@ -164,8 +172,8 @@ corr_kernel(const CorrParams p) {
 #pragma unroll
       for (int i = 0; i < 16; ++i) x1[fpad(16 * t + i)] = xs[i];
       if (valid) {
-        decode16(reinterpret_cast<const uint32_t*>(st + FPC * bpf1 + g * bpf2), p.st[1].bits,
-                 p.st[1].shkind, lut + 1024, lv + 256, p.st[1].lsb, t, xs);
+        decode16(reinterpret_cast<const uint32_t*>(st + kRaw1 + FPC * bpf1 + g * bpf2),
+                 p.st[1].bits, p.st[1].shkind, lut + 1024, lv + 256, p.st[1].lsb, t, xs);
       }
 #pragma unroll
       for (int i = 0; i < 16; ++i) x2[fpad(16 * t + i)] = xs[i];
@@ -177,16 +185,18 @@ corr_kernel(const CorrParams p) {
       fence_proxy_async();
       issue(it + kStages);
     }
-    const FrameInfo fi = finfo[g];
+    const int s1 = valid ? finfo[g].s1 : 0;
+    const int s2 = valid ? finfo[g].s2 : 0;
 
     if constexpr (MODE == MODE_DECODE) {
       if (valid) {
         float* o1 = p.out_a + frame_local * N;
         float* o2 = p.out_b + frame_local * N;
+        const float u1 = 1.0f / p.st[0].scale, u2 = 1.0f / p.st[1].scale;  // exact
         for (int n = t; n < N; n += T1) {
-          const int m1 = n - fi.s1, m2 = n - fi.s2;
-          o1[n] = ((unsigned)m1 < (unsigned)N) ? x1[fpad(m1)] : 0.f;
-          o2[n] = ((unsigned)m2 < (unsigned)N) ? x2[fpad(m2)] : 0.f;
+          const int m1 = n - s1, m2 = n - s2;
+          o1[n] = ((unsigned)m1 < (unsigned)N) ? x1[fpad(m1)] * u1 : 0.f;
+          o2[n] = ((unsigned)m2 < (unsigned)N) ? x2[fpad(m2)] * u2 : 0.f;
         }
       }
       __syncthreads();
@@ -195,20 +205,21 @@ corr_kernel(const CorrParams p) {
 
     float2* za = bufA + g * Geom<N>::CSTRIDE;
     float2* zb = bufB + g * Geom<N>::CSTRIDE;
-    first_pass<N>(x1, x2, fi.s1, fi.s2, za, t);
+    first_pass<N>(x1, x2, s1, s2, za, t);
     float2* Z0 = fft_rest<N>(za, zb, t, tw);
     // the final buffer sits at the same offset for every frame slot
-    const int fin_off = (int)(Z0 - za) == 0 ? 0 : 1;
+    const bool fin_b = Z0 != za;
     __syncthreads();
 
     if constexpr (MODE == MODE_SPECTRA) {
       if (valid) {
         float2* o1 = reinterpret_cast<float2*>(p.out_a) + frame_local * H;
         float2* o2 = reinterpret_cast<float2*>(p.out_b) + frame_local * H;
+        const float u1 = 0.5f / p.st[0].scale, u2 = 0.5f / p.st[1].scale;  // exact
         for (int k = t; k < H; k += T1) {
           const float2 a = Z0[cpad(k)], b = Z0[cpad((N - k) & (N - 1))];
-          o1[k] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
-          o2[k] = make_float2(0.5f * (a.y + b.y), -0.5f * (a.x - b.x));
+          o1[k] = make_float2(u1 * (a.x + b.x), u1 * (a.y - b.y));
+          o2[k] = make_float2(u2 * (a.y + b.y), -u2 * (a.x - b.x));
         }
       }
       __syncthreads();
@@ -219,12 +230,16 @@ corr_kernel(const CorrParams p) {
 #pragma unroll 1
     for (int f = 0; f < FPC; ++f) {
       if (it * FPC + f >= p.nf) break;
-      const float2* Z = (fin_off ? bufB : bufA) + f * Geom<N>::CSTRIDE;
+      const float2* Z = (fin_b ? bufB : bufA) + f * Geom<N>::CSTRIDE;
       const FrameInfo& F = finfo[f];
+      // Ramp rotation of owned bin tid + T*i: SFU sin/cos (|angle| <= ~pi,
+      // absolute error < 4e-7) at i = 0 and i = BPT/2, short recurrences between.
       float sn, cs;
-      sincosf(fmaf((float)(tid - a_gs), F.dphi, F.phi0), &sn, &cs);
+      __sincosf(fmaf((float)(tid - a_gs), F.dphi, F.phi0), &sn, &cs);
       float2 rot = cmul(F.fr_mix, make_float2(cs, sn));
-      sincosf((float)T * F.dphi, &sn, &cs);
+      __sincosf(fmaf((float)(tid + T * (BPT / 2) - a_gs), F.dphi, F.phi0), &sn, &cs);
+      const float2 rot_half = cmul(F.fr_mix, make_float2(cs, sn));
+      __sincosf((float)T * F.dphi, &sn, &cs);
       const float2 rstep = make_float2(cs, sn);
       auto bin_acc = [&](int bin, float2 r, float* a) {
         const float2 u = Z[cpad(bin)], w = Z[cpad((N - bin) & (N - 1))];
@@ -262,11 +277,12 @@ corr_kernel(const CorrParams p) {
       };
 #pragma unroll
       for (int i = 0; i < BPT; ++i) {
+        if (i == BPT / 2) rot = rot_half;
         bin_acc(tid + T * i, rot, acc[i]);
         rot = cmul(rot, rstep);
       }
       if (tid == 0) {
-        sincosf(fmaf((float)(N / 2 - a_gs), F.dphi, F.phi0), &sn, &cs);
+        __sincosf(fmaf((float)(N / 2 - a_gs), F.dphi, F.phi0), &sn, &cs);
         bin_acc(N / 2, cmul(F.fr_mix, make_float2(cs, sn)), acc[BPT]);
       }
     }
@@ -282,10 +298,11 @@ corr_kernel(const CorrParams p) {
   }
 }
 
-// Fixed-order sum of the per-CTA partials; 0.25 undoes the two-for-one 2x
-// scaling of each spectrum.  Writes acf11, acf22, xcf (re,im) and zeroes the
-// phased slot.
+// Fixed-order sum of the per-CTA partials.  The multipliers (exact powers of
+// two) undo the two-for-one 2x factor of each spectrum and the per-station
+// level scaling.  Writes acf11, acf22, xcf (re,im) and zeroes the phased slot.
 __global__ void reduce_partials_kernel(const double* __restrict__ part, int nblk, int h,
+                                       double m11, double m22, double m12,
                                        double* __restrict__ out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= h) return;
@@ -295,10 +312,10 @@ __global__ void reduce_partials_kernel(const double* __restrict__ part, int nblk
 #pragma unroll
     for (int v = 0; v < 4; ++v) s[v] += q[(size_t)v * h + k];
   }
-  out[k] = 0.25 * s[0];
-  out[h + k] = 0.25 * s[1];
-  out[2 * h + 2 * k] = 0.25 * s[2];
-  out[2 * h + 2 * k + 1] = 0.25 * s[3];
+  out[k] = m11 * s[0];
+  out[h + k] = m22 * s[1];
+  out[2 * h + 2 * k] = m12 * s[2];
+  out[2 * h + 2 * k + 1] = m12 * s[3];
   out[4 * h + k] = 0.0;
 }
 
@@ -320,6 +337,15 @@ __global__ void delay_entries_kernel(const DelayParams p, uint64_t first, uint64
   d.fr_lo2[0] = l2.x;
   d.fr_lo2[1] = l2.y;
   out[i] = d;
+}
+
+__global__ void frame_info_kernel(const DelayParams p, uint64_t first, uint64_t nf, int n,
+                                  double df_hz, int a1s, int a2s, FrameInfo* out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  FrameInfo fi;
+  frame_info(p, first + i, n, df_hz, a1s, a2s, &fi);
+  out[i] = fi;
 }
 
 // ------------------------------------------------------------- launchers
@@ -351,24 +377,15 @@ int corr_frames_per_cta_iter(uint32_t n) {
 
 int corr_ctas_per_sm(uint32_t n) { return n >= 8192 ? 1 : 2; }
 
-uint32_t corr_smem_bytes(uint32_t n, uint32_t stage_bytes) {
-  switch (n) {
-    case 1024: return smem_layout<1024, 4>(stage_bytes).total;
-    case 2048: return smem_layout<2048, 2>(stage_bytes).total;
-    case 4096: return smem_layout<4096, 1>(stage_bytes).total;
-    case 8192: return smem_layout<8192, 1>(stage_bytes).total;
-    default: return 0;
-  }
-}
-
 cudaError_t launch_corr(uint32_t n, int mode, const CorrParams& p, int grid, cudaStream_t s) {
   if (mode == MODE_CORR) return launch_mode<MODE_CORR>(n, p, grid, s);
   if (mode == MODE_SPECTRA) return launch_mode<MODE_SPECTRA>(n, p, grid, s);
   return launch_mode<MODE_DECODE>(n, p, grid, s);
 }
 
-cudaError_t launch_reduce(const double* part, int nblk, int h, double* out, cudaStream_t s) {
-  reduce_partials_kernel<<<(h + 255) / 256, 256, 0, s>>>(part, nblk, h, out);
+cudaError_t launch_reduce(const double* part, int nblk, int h, double m11, double m22, double m12,
+                          double* out, cudaStream_t s) {
+  reduce_partials_kernel<<<(h + 255) / 256, 256, 0, s>>>(part, nblk, h, m11, m22, m12, out);
   return cudaGetLastError();
 }
 
@@ -376,6 +393,14 @@ cudaError_t launch_delay_entries(const DelayParams& p, uint64_t first, uint64_t 
                                  fxc_frame_delay_dev* out, cudaStream_t s) {
   if (nf == 0) return cudaSuccess;
   delay_entries_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(p, first, nf, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_frame_info(const DelayParams& p, uint64_t first, uint64_t nf, int n,
+                              double df_hz, int a1s, int a2s, FrameInfo* out, cudaStream_t s) {
+  if (nf == 0) return cudaSuccess;
+  frame_info_kernel<<<(unsigned)((nf + 127) / 128), 128, 0, s>>>(p, first, nf, n, df_hz, a1s,
+                                                                   a2s, out);
   return cudaGetLastError();
 }
 

@@ -22,15 +22,17 @@ struct DelayParams {
   double lo1, lo2;
 };
 
-// Per-frame values the kernels consume (FrameDelayEntry, src/main.rs:151-159,
-// plus the XCF phase ramp of src/main.rs:132-149 as f32 angle + slope).
-struct FrameInfo {
-  int32_t s1, s2;     // integer shifts clamped to [-N, N]
-  float2 fr_lo1, fr_lo2, fr_mix;
-  float phi0, dphi;   // ramp angle at overlap bin 0 and per-bin slope
-  double frac1, frac2;
-  int64_t int1, int2;
+// Per-frame values the kernels consume, produced by frame_info_kernel from
+// the FP64 delay model (FrameDelayEntry, src/main.rs:151-159) and staged into
+// shared memory with the frame's packed words.  48 bytes (bulk-copy sized).
+struct __align__(16) FrameInfo {
+  int32_t s1, s2;     // integer shifts int1 / int2 clamped to [-N, N]
+  float phi0, dphi;   // XCF ramp (src/main.rs:132-149): angle at overlap bin 0, slope per bin
+  float2 fr_mix;      // fr_lo1 * conj(fr_lo2) (src/main.rs:2488)
+  float2 fr_lo1, fr_lo2;
+  float st1, st2;     // per-station fractional-delay slopes -2 pi df frac_i (src/utils.rs:114)
 };
+static_assert(sizeof(FrameInfo) == 48, "FrameInfo is staged by 16-byte bulk copies");
 
 struct StationParams {
   const uint8_t* raw;      // first byte of frame 0 of the sector
@@ -40,6 +42,8 @@ struct StationParams {
   int32_t bits;            // 1, 2, 4, 8
   int32_t lsb;             // negate odd samples
   int32_t shkind;          // 0 identity, 1 pair swap, 2 generic
+  float scale;             // power of two equalising the two stations' RMS level
+                           // inside the shared complex FFT (exact to undo)
 };
 
 enum { SH_IDENTITY = 0, SH_PAIRSWAP = 1, SH_GENERIC = 2 };
@@ -224,12 +228,17 @@ __device__ __forceinline__ void stockham_pass(const float2* __restrict__ in, flo
                                               int t, float2 w) {
   constexpr int T1 = N / 16;
   constexpr int WI = 16 / R;
+  static_assert((N / R) % 16 == 0 && NS % 16 == 0, "padded strides");
+  // cpad(j + r*M) = cpad(j) + r*(M + M/16) whenever M is a multiple of 16
+  constexpr int LS = N / R + N / (16 * R);
+  constexpr int SS = NS + NS / 16;
   float2 v[16];
 #pragma unroll
   for (int wi = 0; wi < WI; ++wi) {
     const int j = t + T1 * wi;
+    const float2* src = in + cpad(j);
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[wi * R + r] = in[cpad(j + r * (N / R))];
+    for (int r = 0; r < R; ++r) v[wi * R + r] = src[r * LS];
   }
   if constexpr (NS > 1) {
     if constexpr (R == 16) {
@@ -300,9 +309,9 @@ __device__ __forceinline__ void stockham_pass(const float2* __restrict__ in, flo
   for (int wi = 0; wi < WI; ++wi) {
     const int j = t + T1 * wi;
     const int k = j & (NS - 1);
-    const int base = (j - k) * R + k;
+    float2* dst = out + cpad((j - k) * R + k);
 #pragma unroll
-    for (int r = 0; r < R; ++r) out[cpad(base + r * NS)] = v[wi * R + out_pos<R>(r)];
+    for (int r = 0; r < R; ++r) dst[r * SS] = v[wi * R + out_pos<R>(r)];
   }
 }
 
@@ -321,8 +330,9 @@ __device__ __forceinline__ void first_pass(const float* __restrict__ x1, const f
     v[r].y = ((unsigned)m2 < (unsigned)N) ? x2[fpad(m2)] : 0.0f;
   }
   dft16(v);
+  float2* dst = out + 17 * t;  // cpad(16 t + r) = 17 t + r
 #pragma unroll
-  for (int r = 0; r < 16; ++r) out[cpad(t * 16 + r)] = v[out_pos<16>(r)];
+  for (int r = 0; r < 16; ++r) dst[r] = v[out_pos<16>(r)];
 }
 
 // Runs passes 2..NPASS; `a` holds the first pass output, returns the buffer
@@ -437,10 +447,6 @@ __device__ __forceinline__ void frame_info(const DelayParams& p, uint64_t frame_
   double f1, f2;
   float2 l1, l2;
   frame_delay(p, frame_idx, &i1, &i2, &f1, &f2, &l1, &l2);
-  fi->int1 = i1;
-  fi->int2 = i2;
-  fi->frac1 = f1;
-  fi->frac2 = f2;
   fi->s1 = (int32_t)(i1 > n ? n : (i1 < -n ? -n : i1));
   fi->s2 = (int32_t)(i2 > n ? n : (i2 < -n ? -n : i2));
   fi->fr_lo1 = l1;
@@ -451,6 +457,8 @@ __device__ __forceinline__ void frame_info(const DelayParams& p, uint64_t frame_
   const double st1 = dM(two_pi_df, f1), st2 = dM(two_pi_df, f2);
   fi->phi0 = (float)dS(dM(st1, (double)a1s), dM(st2, (double)a2s));
   fi->dphi = (float)dS(st1, st2);
+  fi->st1 = (float)st1;
+  fi->st2 = (float)st2;
 }
 
 // ----------------------------------------------------------------- decode

@@ -19,6 +19,7 @@ struct CorrParams {
   uint32_t stage_bytes;  // FPC * (bpf1 + bpf2)
   uint32_t flush_every;  // iterations between f32 -> f64 flushes
   double df_hz;
+  const FrameInfo* finfo; // per-frame records of the sector (frame_info_kernel)
   double* partials;      // MODE_CORR: [grid][4][H] f64
   float* out_a;          // MODE_SPECTRA: S1 [nf][H] complex; MODE_DECODE: x1 [nf][N]
   float* out_b;          // S2 / x2
@@ -55,9 +56,11 @@ struct PhasedParams {
 
 int corr_frames_per_cta_iter(uint32_t n);
 int corr_ctas_per_sm(uint32_t n);
-uint32_t corr_smem_bytes(uint32_t n, uint32_t stage_bytes);
 cudaError_t launch_corr(uint32_t n, int mode, const CorrParams& p, int grid, cudaStream_t s);
-cudaError_t launch_reduce(const double* part, int nblk, int h, double* out, cudaStream_t s);
+cudaError_t launch_reduce(const double* part, int nblk, int h, double m11, double m22, double m12,
+                          double* out, cudaStream_t s);
+cudaError_t launch_frame_info(const DelayParams& p, uint64_t first, uint64_t nf, int n,
+                              double df_hz, int a1s, int a2s, FrameInfo* out, cudaStream_t s);
 cudaError_t launch_delay_entries(const DelayParams& p, uint64_t first, uint64_t nf,
                                  fxc_frame_delay_dev* out, cudaStream_t s);
 

@@ -12,6 +12,7 @@ body of the sector loop in src/main.rs:2173-2683.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass, field
 from pathlib import Path
 
@@ -241,12 +242,18 @@ class Engine:
         check(lib().fxc_engine_create(C.byref(o), C.byref(h)))
         self.h = h
         self.device = device
+        self._scans = weakref.WeakSet()
 
     def open_scan(self, cfg: ScanConfig) -> "Scan":
-        return Scan(self, cfg)
+        s = Scan(self, cfg)
+        self._scans.add(s)
+        return s
 
     def close(self):
         if self.h:
+            # the library closes every scan still open on this engine
+            for s in list(self._scans):
+                s.h = None
             lib().fxc_engine_destroy(self.h)
             self.h = None
 
@@ -266,9 +273,9 @@ class Scan:
         self.h = h
 
     def close(self):
-        if self.h:
+        if self.h and self.eng.h:
             lib().fxc_scan_close(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:

@@ -3,10 +3,14 @@ comparison used by every parity test.
 
 Tolerance (stated against the FP64 oracle, as the correlation path is
 floating point): per-bin relative amplitude error <= 1e-5 and phase error
-<= 1e-4 rad, on every bin whose oracle magnitude is at least 5% of the RMS
-magnitude of that product (bins nearer zero carry absolute errors of the
-same size, which a relative metric would inflate); on all bins the absolute
-error must stay <= 1e-5 * RMS.
+<= 1e-4 rad.  A bin's relative error is taken against max(|ref|, floor):
+for auto-spectra floor = 5% of the product's RMS; for a cross-spectrum bin
+floor = sqrt(<acf11>*<acf22>/nf) with <.> a 33-bin running mean, the
+expected amplitude of a noise-only bin after nf frames, because f32 rounding
+errors of a cross-spectrum scale with that noise amplitude and not with the
+(possibly near-zero) realised value.
+Phase errors are checked on bins at or above the floor.  On all bins the
+absolute error must also stay <= 1e-5 * RMS of the product.
 """
 from __future__ import annotations
 
@@ -66,35 +70,59 @@ def signal_raw(scan, nf, seed, rho=0.05, delay_samples=0.0, tone_bin=None):
     return r1, r2
 
 
-def spectral_errors(a, b):
+def spectral_errors(a, b, floor=None):
     """(max relative amplitude error, max phase error, max abs error / rms)
-    of a against reference b, on bins with |b| >= FLOOR * rms(|b|)."""
+    of a against reference b; `floor` (scalar or per bin) bounds the
+    relative-error denominator from below (default 5% of rms(|b|))."""
     a = np.asarray(a, np.complex128)
     b = np.asarray(b, np.complex128)
     mag = np.abs(b)
     rms = float(np.sqrt(np.mean(mag ** 2))) if mag.size else 0.0
     if rms == 0.0:
         return 0.0, 0.0, float(np.abs(a).max()) if a.size else 0.0
-    m = mag >= FLOOR * rms
-    rel = float(np.max(np.abs(np.abs(a[m]) - mag[m]) / mag[m])) if m.any() else 0.0
+    fl = FLOOR * rms if floor is None else np.maximum(np.asarray(floor, float), 1e-300)
+    fl = np.broadcast_to(fl, mag.shape)
+    den = np.maximum(mag, fl)
+    rel = float(np.max(np.abs(np.abs(a) - mag) / den))
+    m = (mag >= fl) & (mag > 0)
     ph = float(np.max(np.abs(np.angle(a[m] * np.conj(b[m]))))) if m.any() else 0.0
     ab = float(np.max(np.abs(a - b)) / rms)
     return rel, ph, ab
 
 
-def assert_spectra_close(a, b, what, rel_tol=REL_AMP_TOL, phase_tol=PHASE_TOL):
-    rel, ph, ab = spectral_errors(a, b)
+def assert_spectra_close(a, b, what, rel_tol=REL_AMP_TOL, phase_tol=PHASE_TOL, floor=None):
+    rel, ph, ab = spectral_errors(a, b, floor)
     assert rel <= rel_tol and ph <= phase_tol and ab <= rel_tol, (
         f"{what}: rel amp {rel:.3e} (tol {rel_tol}), phase {ph:.3e} rad (tol {phase_tol}), "
         f"abs/rms {ab:.3e}")
     return rel, ph, ab
 
 
-def assert_sector_close(got, ref, scan, what):
+def _running_mean(x, w=33):
+    k = np.ones(w)
+    num = np.convolve(x, k, mode="same")
+    den = np.convolve(np.ones_like(x), k, mode="same")
+    return num / den
+
+
+def xcf_floor(ref, nf):
+    """Expected noise amplitude sqrt(<acf11><acf22>/nf) of each cross-spectrum
+    bin (33-bin running means of the auto-spectra), or None when the reference
+    has no auto-spectra."""
+    a11, a22 = np.asarray(ref["acf11"]), np.asarray(ref["acf22"])
+    if not (np.any(a11) and np.any(a22)) or nf <= 0:
+        return None
+    return np.sqrt(np.maximum(_running_mean(a11) * _running_mean(a22), 0.0) / nf)
+
+
+def assert_sector_close(got, ref, scan, what, nf=None, ref_acf=None):
+    """ref_acf: a reference holding both auto-spectra on the grid (defaults
+    to ref) for the cross-spectrum floor."""
     out = {}
     if scan.products & oracle.PROD_ACF:
         out["acf11"] = assert_spectra_close(got["acf11"], ref["acf11"], what + " acf11")
         out["acf22"] = assert_spectra_close(got["acf22"], ref["acf22"], what + " acf22")
     if scan.products & oracle.PROD_XCF:
-        out["xcf"] = assert_spectra_close(got["xcf"], ref["xcf"], what + " xcf")
+        fl = xcf_floor(ref_acf if ref_acf is not None else ref, nf) if nf else None
+        out["xcf"] = assert_spectra_close(got["xcf"], ref["xcf"], what + " xcf", floor=fl)
     return out
