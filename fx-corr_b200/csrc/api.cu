@@ -93,10 +93,15 @@ struct fxc_scan {
   uint32_t* d_lut = nullptr;     // [2][1024]
   float* d_levels = nullptr;     // [2][256]
   uint8_t* d_shuffle_out = nullptr;
+  float* d_qlevels = nullptr;     // levels1 as f32 for the phased re-quantiser
+  uint32_t* d_enc_lut = nullptr;  // [4][256] byte LUTs of ant1's output shuffle
+  int qmonotonic = 0;
   double* d_partials = nullptr;
   uint64_t partials_elems = 0;
   FrameInfo* d_finfo = nullptr;  // per-frame delay records of the sector in flight
   uint64_t finfo_cap = 0;
+  float2* d_big[2] = {nullptr, nullptr};  // FFT lengths > 8192: batch scratch
+  uint64_t big_frames = 0;                // frames per batch
   uint32_t* d_err = nullptr;
   cudaStream_t stream = nullptr;     // compute
   cudaStream_t copy_stream = nullptr;
@@ -245,8 +250,11 @@ fxc_status check_device_inputs(const fxc_scan* s, const uint8_t* r1, const uint8
 
 fxc_status validate_cfg(const fxc_scan_cfg* c) {
   const uint32_t n = c->fft_len;
-  if (!(n == 1024 || n == 2048 || n == 4096 || n == 8192))
-    return fail(FXC_EUNSUPPORTED, "fft_len %u not supported (1024, 2048, 4096, 8192)", n);
+  if (!(n == 1024 || n == 2048 || n == 4096 || n == 8192 || n == 16384 || n == 32768 ||
+        n == 65536))
+    return fail(FXC_EUNSUPPORTED, "fft_len %u not supported (powers of two 1024..65536)", n);
+  if (n > 8192 && (c->products & (FXC_PROD_PHASED | FXC_PROD_RAW)))
+    return fail(FXC_EUNSUPPORTED, "phased products need fft_len <= 8192 in this build");
   for (uint32_t b : {c->bits1, c->bits2})
     if (!(b == 1 || b == 2 || b == 4 || b == 8))
       return fail(FXC_EUNSUPPORTED, "bits %u not supported (1, 2, 4, 8)", b);
@@ -275,8 +283,8 @@ fxc_status validate_cfg(const fxc_scan_cfg* c) {
   if (c->delay.geom_table && c->delay.geom_len == 0)
     return fail(FXC_EINVAL, "geometric delay table is empty");
   if (c->products & ~31u) return fail(FXC_EINVAL, "unknown product flags");
-  if (c->products & (FXC_PROD_PHASED | FXC_PROD_RAW))
-    return fail(FXC_EUNSUPPORTED, "phased products are not available in this build");
+  if ((c->products & (FXC_PROD_PHASED | FXC_PROD_RAW)) && !(c->w1 == c->w1 && c->w2 == c->w2))
+    return fail(FXC_EINVAL, "phased weights must be numbers");
   return FXC_OK;
 }
 
@@ -302,16 +310,112 @@ fxc_status grow_host(uint8_t** p, uint64_t* cap, uint64_t need) {
   return FXC_OK;
 }
 
-fxc_status run_corr_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
-                           uint64_t first, double* d_acc, cudaStream_t st) {
+fxc_status run_corr_stage(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
+                          uint64_t first, int grid, double* d_acc, cudaStream_t st);
+
+LargeParams large_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2) {
+  LargeParams p{};
+  station_params(s, r1, r2, p.st);
+  p.finfo = s->d_finfo;
+  p.n = (int32_t)s->n;
+  p.c = (int32_t)(s->n / 8192);
+  p.a1s = (int32_t)s->cfg.a1s;
+  p.a1e = (int32_t)s->cfg.a1e;
+  p.a2s = (int32_t)s->cfg.a2s;
+  p.grid = s->cfg.grid;
+  p.products = s->cfg.products;
+  return p;
+}
+
+// FFT lengths above 8192: batches of frames through the global-memory path,
+// per-frame-group f64 partials, then the fixed-order reduction.  The frame
+// records of the sector must already be staged.
+fxc_status run_large_corr(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
+                          double* d_acc, cudaStream_t st) {
   const uint32_t h = s->h;
-  if (nf == 0 || !(s->cfg.products & (FXC_PROD_ACF | FXC_PROD_XCF))) {
+  const LargeParams p = large_params(s, r1, r2);
+  const int groups = (int)std::min<uint64_t>((uint64_t)kLargeGroups, s->big_frames);
+  bool first = true;
+  for (uint64_t f0 = 0; f0 < nf; f0 += s->big_frames) {
+    const uint64_t nb = std::min(s->big_frames, nf - f0);
+    CK(launch_large_fft(p, f0, nb, s->d_big[0], s->d_big[1], s->eng->sm_count, st));
+    CK(launch_large_acc(p, s->d_big[1], f0, nb, groups, first ? 1 : 0, s->d_partials, st));
+    s->all_launches += 4;
+    first = false;
+  }
+  const double u1 = 1.0 / s->scale[0], u2 = 1.0 / s->scale[1];
+  CK(launch_reduce(s->d_partials, groups, (int)h, 0.25 * u1 * u1, 0.25 * u2 * u2, 0.25 * u1 * u2,
+                   d_acc, st));
+  s->all_launches += 1;
+  s->kernel_launches += 1;
+  return FXC_OK;
+}
+
+PhasedParams phased_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
+                           uint64_t first, uint8_t* d_raw_out) {
+  PhasedParams p{};
+  station_params(s, r1, r2, p.st);
+  p.dl = delay_params(s);
+  p.nf = nf;
+  p.first_frame = first;
+  p.a1s = (int32_t)s->cfg.a1s;
+  p.a1e = (int32_t)s->cfg.a1e;
+  p.a2s = (int32_t)s->cfg.a2s;
+  p.grid = s->cfg.grid;
+  const int fpc = corr_frames_per_cta_iter(s->n);
+  p.stage_bytes = (uint32_t)fpc * (s->bpf1 + s->bpf2);
+  p.flush_every = (uint32_t)std::max(1, 32 / fpc);
+  p.bits_out = s->cfg.bits_out;
+  p.bpf_out = s->bpfo;
+  p.out_lsb = (s->cfg.lsb1 && s->cfg.lsb2) ? 1 : 0;  // output_lsb (main.rs:1093)
+  p.want_raw = (s->cfg.products & FXC_PROD_RAW) && d_raw_out ? 1 : 0;
+  p.w1 = (float)s->cfg.w1;
+  p.w2 = (float)s->cfg.w2;
+  p.qlevels = s->d_qlevels;
+  p.nqlevels = s->cfg.nlevels1;
+  p.qmonotonic = s->qmonotonic;
+  p.enc_lut = s->d_enc_lut;
+  p.finfo = s->d_finfo;
+  p.partials = s->d_partials;
+  p.raw_out = d_raw_out;
+  p.err = s->d_err;
+  return p;
+}
+
+fxc_status run_sector_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
+                             uint64_t first, double* d_acc, uint8_t* d_raw_out, cudaStream_t st) {
+  const uint32_t h = s->h;
+  const bool corr = (s->cfg.products & (FXC_PROD_ACF | FXC_PROD_XCF)) != 0;
+  const bool phased = (s->cfg.products & (FXC_PROD_PHASED | FXC_PROD_RAW)) != 0;
+  if (nf == 0 || !(corr || phased)) {
     CK(cudaMemsetAsync(d_acc, 0, sizeof(double) * 5 * h, st));
     return FXC_OK;
   }
+  if ((s->cfg.products & FXC_PROD_RAW) && !d_raw_out)
+    return fail(FXC_EINVAL, "the scan writes phased .raw frames but d_raw_out is NULL");
   const int grid = corr_grid(s, nf);
   fxc_status fst = stage_frame_info(s, first, nf, st);
   if (fst != FXC_OK) return fst;
+  s->all_launches += 1;
+  if (s->n > 8192) return run_large_corr(s, r1, r2, nf, d_acc, st);
+  if (!corr) {
+    CK(cudaMemsetAsync(d_acc, 0, sizeof(double) * 5 * h, st));
+  } else {
+    fst = run_corr_stage(s, r1, r2, nf, first, grid, d_acc, st);
+    if (fst != FXC_OK) return fst;
+  }
+  if (phased) {
+    PhasedParams pp = phased_params(s, r1, r2, nf, first, d_raw_out);
+    CK(launch_phased(s->n, pp, grid, st));
+    CK(launch_reduce_phased(s->d_partials, grid, (int)h, d_acc, st));
+    s->all_launches += 2;
+  }
+  return FXC_OK;
+}
+
+fxc_status run_corr_stage(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
+                          uint64_t first, int grid, double* d_acc, cudaStream_t st) {
+  const uint32_t h = s->h;
   CorrParams p = corr_params(s, r1, r2, nf, first);
   std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
   if (s->profiling) {
@@ -330,7 +434,7 @@ fxc_status run_corr_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, ui
   CK(launch_reduce(s->d_partials, grid, (int)h, 0.25 * u1 * u1, 0.25 * u2 * u2, 0.25 * u1 * u2,
                    d_acc, st));
   s->kernel_launches += 1;
-  s->all_launches += 3;
+  s->all_launches += 2;
   return FXC_OK;
 }
 
@@ -413,10 +517,13 @@ fxc_status fxc_scan_open(fxc_engine* e, const fxc_scan_cfg* cfg, fxc_scan** out)
   s->shkind[1] = shuffle_kind(cfg->shuffle2);
   s->scale[0] = level_scale(cfg->levels1, cfg->nlevels1);
   s->scale[1] = level_scale(cfg->levels2, cfg->nlevels2);
-  const uint64_t maxg = (uint64_t)e->sm_count * (uint64_t)corr_ctas_per_sm(s->n);
+  const uint64_t maxg = s->n > 8192 ? (uint64_t)kLargeGroups
+                                    : (uint64_t)e->sm_count * (uint64_t)corr_ctas_per_sm(s->n);
   s->partials_elems = maxg * 4 * s->h;
+  s->big_frames = s->n > 8192 ? (uint64_t)large_batch_frames(s->n) : 0;
   const uint64_t need = s->partials_elems * 8 + 2 * 1024 * 4 + 2 * 256 * 4 + 64 +
-                        (cfg->delay.geom_table ? cfg->delay.geom_len * 8 : 0);
+                        (cfg->delay.geom_table ? cfg->delay.geom_len * 8 : 0) +
+                        2 * s->big_frames * (uint64_t)s->n * sizeof(float2);
   {
     std::lock_guard<std::mutex> lk(e->mu);
     if (e->in_use + need > e->budget) {
@@ -442,6 +549,8 @@ fxc_status fxc_scan_open(fxc_engine* e, const fxc_scan_cfg* cfg, fxc_scan** out)
   CKS(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   CKS(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
   CKS(cudaMalloc(&s->d_partials, s->partials_elems * sizeof(double)));
+  for (int b = 0; b < 2 && s->big_frames; ++b)
+    CKS(cudaMalloc(&s->d_big[b], s->big_frames * (uint64_t)s->n * sizeof(float2)));
   CKS(cudaMalloc(&s->d_lut, 2 * 1024 * sizeof(uint32_t)));
   CKS(cudaMalloc(&s->d_levels, 2 * 256 * sizeof(float)));
   CKS(cudaMalloc(&s->d_shuffle_out, 32));
@@ -457,6 +566,23 @@ fxc_status fxc_scan_open(fxc_engine* e, const fxc_scan_cfg* cfg, fxc_scan** out)
     for (uint32_t i = 0; i < cfg->nlevels2; ++i) lv[256 + i] = (float)cfg->levels2[i];
     CKS(cudaMemcpy(s->d_levels, lv.data(), lv.size() * 4, cudaMemcpyHostToDevice));
     CKS(cudaMemcpy(s->d_shuffle_out, cfg->shuffle1, 32, cudaMemcpyHostToDevice));
+    // phased re-quantiser: ant1's levels as f32 (quantise_frame compares
+    // |x - lv as f32|) and the encode LUT of ant1's shuffle: packed bit pos
+    // goes to bit shuffle1[pos] (utils.rs:395)
+    CKS(cudaMalloc(&s->d_qlevels, 256 * sizeof(float)));
+    CKS(cudaMemcpy(s->d_qlevels, lv.data(), 256 * sizeof(float), cudaMemcpyHostToDevice));
+    std::vector<uint32_t> enc(1024, 0u);
+    for (int pos = 0; pos < 32; ++pos)
+      for (int v = 0; v < 256; ++v)
+        if ((v >> (pos & 7)) & 1) enc[(pos >> 3) * 256 + v] |= 1u << cfg->shuffle1[pos];
+    CKS(cudaMalloc(&s->d_enc_lut, 1024 * sizeof(uint32_t)));
+    CKS(cudaMemcpy(s->d_enc_lut, enc.data(), 1024 * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    bool up = true, down = true;
+    for (uint32_t i = 1; i < cfg->nlevels1; ++i) {
+      if (!(lv[i] > lv[i - 1])) up = false;
+      if (!(lv[i] < lv[i - 1])) down = false;
+    }
+    s->qmonotonic = up ? 1 : (down ? -1 : 0);
   }
   if (cfg->delay.geom_table) {
     CKS(cudaMalloc(&s->d_table, cfg->delay.geom_len * sizeof(double)));
@@ -500,10 +626,14 @@ fxc_status fxc_scan_close(fxc_scan* s) {
     cudaEventDestroy(pr.second);
   }
   cudaFree(s->d_partials);
+  cudaFree(s->d_big[0]);
+  cudaFree(s->d_big[1]);
   cudaFree(s->d_finfo);
   cudaFree(s->d_lut);
   cudaFree(s->d_levels);
   cudaFree(s->d_shuffle_out);
+  cudaFree(s->d_qlevels);
+  cudaFree(s->d_enc_lut);
   cudaFree(s->d_err);
   cudaFree(s->d_table);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -526,7 +656,8 @@ fxc_status fxc_sector_run_device(fxc_scan* s, const uint8_t* d_raw1, const uint8
   if (st != FXC_OK) return st;
   if (!d_acc) return fail(FXC_EINVAL, "d_acc is NULL");
   DeviceGuard g(s->eng->device);
-  return run_corr_device(s, d_raw1, d_raw2, nf, first_frame, d_acc, (cudaStream_t)stream);
+  return run_sector_device(s, d_raw1, d_raw2, nf, first_frame, d_acc, d_raw_out,
+                           (cudaStream_t)stream);
 }
 
 fxc_status fxc_scan_check(fxc_scan* s) {
@@ -589,6 +720,11 @@ fxc_status fxc_decode_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t* 
   DeviceGuard g(s->eng->device);
   st = stage_frame_info(s, first_frame, nf, (cudaStream_t)stream);
   if (st != FXC_OK) return st;
+  if (s->n > 8192) {
+    CK(launch_large_decode(large_params(s, d_raw1, d_raw2), 0, nf, d_x1, d_x2,
+                           s->eng->sm_count, (cudaStream_t)stream));
+    return FXC_OK;
+  }
   CorrParams p = corr_params(s, d_raw1, d_raw2, nf, first_frame);
   p.out_a = d_x1;
   p.out_b = d_x2;
@@ -606,6 +742,18 @@ fxc_status fxc_spectra_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t*
   DeviceGuard g(s->eng->device);
   st = stage_frame_info(s, first_frame, nf, (cudaStream_t)stream);
   if (st != FXC_OK) return st;
+  if (s->n > 8192) {
+    const LargeParams lp = large_params(s, d_raw1, d_raw2);
+    for (uint64_t f0 = 0; f0 < nf; f0 += s->big_frames) {
+      const uint64_t nb = std::min(s->big_frames, nf - f0);
+      CK(launch_large_fft(lp, f0, nb, s->d_big[0], s->d_big[1], s->eng->sm_count,
+                          (cudaStream_t)stream));
+      CK(launch_large_split(lp, s->d_big[1], f0, nb, reinterpret_cast<float2*>(d_s1),
+                            reinterpret_cast<float2*>(d_s2), s->eng->sm_count,
+                            (cudaStream_t)stream));
+    }
+    return FXC_OK;
+  }
   CorrParams p = corr_params(s, d_raw1, d_raw2, nf, first_frame);
   p.out_a = d_s1;
   p.out_b = d_s2;
@@ -637,12 +785,21 @@ fxc_status fxc_sector_submit(fxc_scan* s, const uint8_t* raw1, uint64_t n1, cons
     CK(cudaMemcpyAsync(sl->d_raw1, raw1, need1, cudaMemcpyHostToDevice, s->copy_stream));
     CK(cudaMemcpyAsync(sl->d_raw2, raw2, need2, cudaMemcpyHostToDevice, s->copy_stream));
   }
+  const bool raw = (s->cfg.products & FXC_PROD_RAW) != 0;
+  const uint64_t need_o = nf * s->bpfo;
+  if (raw) {
+    if ((st = grow(&sl->d_rawout, &sl->cap_out, need_o)) != FXC_OK) return st;
+    if ((st = grow_host(&sl->h_rawout, &sl->hcap_out, need_o)) != FXC_OK) return st;
+  }
   CK(cudaEventRecord(sl->ev_h2d, s->copy_stream));
   CK(cudaStreamWaitEvent(s->stream, sl->ev_h2d, 0));
-  st = run_corr_device(s, sl->d_raw1, sl->d_raw2, nf, first_frame, sl->d_acc, s->stream);
+  st = run_sector_device(s, sl->d_raw1, sl->d_raw2, nf, first_frame, sl->d_acc,
+                         raw ? sl->d_rawout : nullptr, s->stream);
   if (st != FXC_OK) return st;
   CK(cudaMemcpyAsync(sl->h_acc, sl->d_acc, sizeof(double) * 5 * s->h, cudaMemcpyDeviceToHost,
                      s->stream));
+  if (raw && need_o)
+    CK(cudaMemcpyAsync(sl->h_rawout, sl->d_rawout, need_o, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(sl->h_acc) + sizeof(double) * 5 * s->h, s->d_err,
                      4, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaEventRecord(sl->ev_done, s->stream));
@@ -682,6 +839,13 @@ fxc_status fxc_sector_wait(fxc_scan* s, uint64_t sector_id, int32_t timeout_ms,
     if (out->xcf) std::memcpy(out->xcf, sl->h_acc + 2 * h, sizeof(double) * 2 * h);
     if (out->phased) std::memcpy(out->phased, sl->h_acc + 4 * h, sizeof(double) * h);
     out->frames_failed = 0;
+    if (out->raw_out && (s->cfg.products & FXC_PROD_RAW)) {
+      const uint64_t need_o = sl->nf * s->bpfo;
+      if (out->raw_out_len < need_o)
+        return fail(FXC_EINVAL, "raw_out_len %llu < %llu bytes of phased frames",
+                    (unsigned long long)out->raw_out_len, (unsigned long long)need_o);
+      if (need_o) std::memcpy(out->raw_out, sl->h_rawout, need_o);
+    }
   }
   if (err) {
     cudaMemsetAsync(s->d_err, 0, 4, s->stream);

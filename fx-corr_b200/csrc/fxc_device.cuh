@@ -543,4 +543,32 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// ------------------------------------------------------ staging layout
+
+constexpr int kStages = 2;
+constexpr uint32_t kWaitPolls = 1u << 26;  // bounded mbarrier wait
+constexpr uint32_t kFiBytes = sizeof(FrameInfo);
+
+struct SmemLayout {
+  uint32_t off_a, off_b, off_stage, stage_stride, off_lut, off_lv, off_fi, off_bar, off_flag, total;
+};
+
+// Staging slot: [FPC FrameInfo][FPC frames of station 1][FPC frames of station 2]
+template <int N, int FPC>
+__host__ __device__ inline SmemLayout smem_layout(uint32_t raw_bytes) {
+  SmemLayout L;
+  const uint32_t cbytes = (uint32_t)(FPC * Geom<N>::CSTRIDE * sizeof(float2));
+  L.off_a = 0;
+  L.off_b = L.off_a + cbytes;
+  L.off_stage = L.off_b + cbytes;
+  L.stage_stride = (FPC * kFiBytes + raw_bytes + 127u) & ~127u;
+  L.off_lut = L.off_stage + kStages * L.stage_stride;
+  L.off_lv = L.off_lut + 2 * 1024 * 4;
+  L.off_fi = L.off_lv + 2 * 256 * 4;
+  L.off_bar = L.off_fi + FPC * kFiBytes;
+  L.off_flag = L.off_bar + kStages * 8;
+  L.total = L.off_flag + 16;
+  return L;
+}
+
 }  // namespace fxc

@@ -45,10 +45,11 @@ struct PhasedParams {
   int32_t out_lsb;       // negate odd output samples (both stations LSB)
   int32_t want_raw;
   float w1, w2;
-  double df_hz;
   const float* qlevels;  // levels1 as f32 (device)
   uint32_t nqlevels;
-  const uint8_t* shuffle_out;  // 32 entries (device)
+  int32_t qmonotonic;    // +1 / -1 strictly ascending / descending levels, else 0
+  const uint32_t* enc_lut;  // [4][256] byte LUTs of ant1's output shuffle (device)
+  const FrameInfo* finfo;
   double* partials;      // [grid][H] f64
   uint8_t* raw_out;      // nf * bpf_out
   uint32_t* err;
@@ -59,6 +60,27 @@ int corr_ctas_per_sm(uint32_t n);
 cudaError_t launch_corr(uint32_t n, int mode, const CorrParams& p, int grid, cudaStream_t s);
 cudaError_t launch_reduce(const double* part, int nblk, int h, double m11, double m22, double m12,
                           double* out, cudaStream_t s);
+// FFT lengths above 8192 (N = c * 8192): global-memory four-step path.
+struct LargeParams {
+  StationParams st[2];
+  const FrameInfo* finfo;  // records of every frame of the sector
+  int32_t n, c;
+  int32_t a1s, a1e, a2s, grid;
+  uint32_t products;
+};
+constexpr int kLargeGroups = 16;  // frame groups (partials) per sector
+int large_batch_frames(uint32_t n);
+cudaError_t launch_large_fft(const LargeParams& p, uint64_t f0, uint64_t nb, float2* buf0,
+                             float2* buf1, int sms, cudaStream_t s);
+cudaError_t launch_large_acc(const LargeParams& p, const float2* Y, uint64_t f0, uint64_t nb,
+                             int groups, int first_batch, double* part, cudaStream_t s);
+cudaError_t launch_large_decode(const LargeParams& p, uint64_t f0, uint64_t nb, float* x1,
+                                float* x2, int sms, cudaStream_t s);
+cudaError_t launch_large_split(const LargeParams& p, const float2* Y, uint64_t f0, uint64_t nb,
+                               float2* s1, float2* s2, int sms, cudaStream_t s);
+
+cudaError_t launch_phased(uint32_t n, const PhasedParams& p, int grid, cudaStream_t s);
+cudaError_t launch_reduce_phased(const double* part, int nblk, int h, double* out, cudaStream_t s);
 cudaError_t launch_frame_info(const DelayParams& p, uint64_t first, uint64_t nf, int n,
                               double df_hz, int a1s, int a2s, FrameInfo* out, cudaStream_t s);
 cudaError_t launch_delay_entries(const DelayParams& p, uint64_t first, uint64_t nf,

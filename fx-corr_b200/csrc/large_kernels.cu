@@ -1,0 +1,271 @@
+// large_kernels.cu — correlation path for FFT lengths above one CTA's shared
+// memory (N = C * M with M = 8192, C in {2, 4, 8}: N = 16384 .. 65536).
+//
+// The N-point complex FFT of z = x1 + i x2 runs as one decimation-in-frequency
+// radix-C step over the frame followed by C shared-memory FFTs of M points:
+//   y_q[m] = W_N^(m q) * sum_c z[m + M c] W_C^(c q),   Z[C k + q] = FFT_M(y_q)[k].
+// Kernels, per batch of frames held in device scratch:
+//   decode_global_kernel  decode + LSB flip + integer shift -> z   (src/utils.rs:126-376)
+//   dif_kernel<C>         the radix-C step with its twiddles    -> y
+//   cfft_kernel<M>        M-point Stockham FFT per row            -> Z (row q, column k)
+//   acc_global_kernel     two-for-one split, band alignment, fringe x ramp rotation and
+//                         ACF/XCF accumulation (src/main.rs:2491-2568) per bin, in f64,
+//                         into per-frame-group partials reduced by reduce_partials_kernel.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "fxc_device.cuh"
+#include "fxc_kernels.h"
+
+namespace fxc {
+
+constexpr int kLargeM = 8192;
+
+// One decoded, shifted sample of a station (0 outside [0, N)).
+__device__ __forceinline__ float sample_at(const uint8_t* __restrict__ frame, int bits, int kind,
+                                           const uint32_t* lut, const float* lv, int lsb, int m,
+                                           int n) {
+  if ((unsigned)m >= (unsigned)n) return 0.f;
+  const uint32_t bit = (uint32_t)m * (uint32_t)bits;
+  const uint32_t w = shuffle_word(reinterpret_cast<const uint32_t*>(frame)[bit >> 5], kind, lut);
+  const float v = lv[(w >> (bit & 31u)) & ((1u << bits) - 1u)];
+  return (lsb && (m & 1)) ? -v : v;
+}
+
+// z[f][n] = x1[n - s1] + i x2[n - s2] (levels scaled by the stations' exact
+// powers of two), or, with planar outputs, x1 / x2 unscaled.
+__global__ void decode_global_kernel(const LargeParams p, uint64_t f0, uint64_t nb, float2* z,
+                                     float* x1o, float* x2o) {
+  __shared__ uint32_t lut[2048];
+  __shared__ float lv[512];
+  for (int i = threadIdx.x; i < 512; i += blockDim.x)
+    lv[i] = p.st[i >> 8].levels[i & 255] * p.st[i >> 8].scale;
+  for (int s = 0; s < 2; ++s)
+    if (p.st[s].shkind == SH_GENERIC)
+      for (int i = threadIdx.x; i < 1024; i += blockDim.x) lut[s * 1024 + i] = p.st[s].shlut[i];
+  __syncthreads();
+  const int n = p.n;
+  const uint64_t total = nb * (uint64_t)n;
+  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t fl = idx / (uint64_t)n;
+    const int k = (int)(idx - fl * (uint64_t)n);
+    const uint64_t f = f0 + fl;
+    const FrameInfo& F = p.finfo[f];
+    const float a = sample_at(p.st[0].raw + f * p.st[0].bpf, p.st[0].bits, p.st[0].shkind, lut,
+                              lv, p.st[0].lsb, k - F.s1, n);
+    const float b = sample_at(p.st[1].raw + f * p.st[1].bpf, p.st[1].bits, p.st[1].shkind,
+                              lut + 1024, lv + 256, p.st[1].lsb, k - F.s2, n);
+    if (z) {
+      z[idx] = make_float2(a, b);
+    } else {
+      x1o[f * n + k] = a / p.st[0].scale;
+      x2o[f * n + k] = b / p.st[1].scale;
+    }
+  }
+}
+
+template <int C>
+__global__ void dif_kernel(const float2* __restrict__ z, float2* __restrict__ y, uint64_t nb) {
+  constexpr int M = kLargeM;
+  constexpr int N = C * M;
+  const uint64_t total = nb * (uint64_t)M;
+  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t f = idx / M;
+    const int m = (int)(idx - f * M);
+    const float2* zf = z + f * N;
+    float2 v[16];
+#pragma unroll
+    for (int c = 0; c < C; ++c) v[c] = zf[m + M * c];
+    if constexpr (C == 2) {
+      dft2<0>(v);
+    } else if constexpr (C == 4) {
+      dft4<0>(v);
+    } else {
+      dft8<0>(v);
+    }
+    float2* yf = y + f * N;
+#pragma unroll
+    for (int q = 0; q < C; ++q) {
+      float2 val = v[out_pos<C>(q)];
+      if (q > 0) {
+        float s, c;
+        sincospif(-2.0f * (float)((m * q) % N) / (float)N, &s, &c);
+        val = cmul(val, make_float2(c, s));
+      }
+      yf[q * M + m] = val;
+    }
+  }
+}
+
+// In-place M-point FFT of each row of y (rows of M complex values), natural order.
+template <int M>
+__global__ void __launch_bounds__(M / 16, 1) cfft_kernel(float2* __restrict__ y, uint64_t rows) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  constexpr int T1 = M / 16;
+  float2* bufA = reinterpret_cast<float2*>(smem);
+  float2* bufB = bufA + Geom<M>::CSTRIDE;
+  float* x1 = reinterpret_cast<float*>(bufB);
+  float* x2 = x1 + Geom<M>::FSTRIDE;
+  const int t = threadIdx.x;
+  Twiddles<M> tw;
+  tw.init(t);
+  for (uint64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    float2* row = y + r * M;
+    for (int i = t; i < M; i += T1) {
+      const float2 v = row[i];
+      x1[fpad(i)] = v.x;
+      x2[fpad(i)] = v.y;
+    }
+    __syncthreads();
+    first_pass<M>(x1, x2, 0, 0, bufA, t);
+    float2* Z = fft_rest<M>(bufA, bufB, t, tw);
+    __syncthreads();
+    for (int i = t; i < M; i += T1) row[i] = Z[cpad(i)];
+    __syncthreads();
+  }
+}
+
+// Per-bin split + accumulation.  Bin g = C*kk + q: q = blockIdx.y, kk from x,
+// so a warp reads consecutive columns of one row.  blockIdx.z = frame group.
+__global__ void acc_global_kernel(const LargeParams p, const float2* __restrict__ Y, uint64_t f0,
+                                  uint64_t nb, int first_batch, double* __restrict__ part) {
+  const int C = p.c, M = kLargeM, N = p.n, H = N / 2 + 1;
+  const int q = blockIdx.y;
+  const int kk = blockIdx.x * blockDim.x + threadIdx.x;
+  const int bin = C * kk + q;
+  if (kk >= M || bin > N / 2) return;
+  const int a1s = p.a1s, a1e = p.a1e, a2s = p.a2s, ov = a1e - a1s, sb = a2s - a1s;
+  const int a_gs = p.grid == 0 ? a1s : a2s;
+  const bool want_acf = (p.products & 1u) != 0, want_xcf = (p.products & 2u) != 0;
+  const bool ov_only = (p.products & 16u) != 0;
+  auto zi = [&](const float2* Zf, int k) {  // Z[k] of the natural-order spectrum
+    k &= (N - 1);
+    return Zf[(k % C) * M + k / C];
+  };
+  double a[4] = {0, 0, 0, 0};
+  const uint64_t groups = gridDim.z;
+  const uint64_t g0 = (blockIdx.z * nb) / groups, g1 = ((blockIdx.z + 1) * nb) / groups;
+  for (uint64_t fl = g0; fl < g1; ++fl) {
+    const float2* Zf = Y + fl * (uint64_t)N;
+    const FrameInfo& F = p.finfo[f0 + fl];
+    float sn, cs;
+    sincosf(fmaf((float)(bin - a_gs), F.dphi, F.phi0), &sn, &cs);
+    const float2 r = cmul(F.fr_mix, make_float2(cs, sn));
+    const float2 u = zi(Zf, bin), w = zi(Zf, N - bin);
+    if (p.grid == 0) {
+      const bool inov = bin >= a1s && bin < a1e;
+      const float2 p1 = make_float2(u.x + w.x, u.y - w.y);
+      if (want_acf && (!ov_only || inov)) a[0] += (double)cnorm2(p1);
+      if (inov) {
+        const int i2 = bin + sb;
+        const float2 c = zi(Zf, i2), d = zi(Zf, N - i2);
+        const float2 q2 = make_float2(c.y + d.y, d.x - c.x);
+        if (want_acf) a[1] += (double)cnorm2(q2);
+        if (want_xcf) {
+          const float2 x = cmul(cmulc(p1, q2), r);
+          a[2] += (double)x.x;
+          a[3] += (double)x.y;
+        }
+      }
+    } else {
+      const bool inov = bin >= a2s && bin < a2s + ov;
+      const float2 p2 = make_float2(u.y + w.y, w.x - u.x);
+      if (want_acf && (!ov_only || inov)) a[1] += (double)cnorm2(p2);
+      if (inov) {
+        const int i1 = bin - sb;
+        const float2 c = zi(Zf, i1), d = zi(Zf, N - i1);
+        const float2 q1 = make_float2(c.x + d.x, c.y - d.y);
+        if (want_acf) a[0] += (double)cnorm2(q1);
+        if (want_xcf) {
+          const float2 x = cmul(cmulc(q1, p2), r);
+          a[2] += (double)x.x;
+          a[3] += (double)x.y;
+        }
+      }
+    }
+  }
+  double* pg = part + (size_t)blockIdx.z * 4 * H;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    double* d = pg + (size_t)v * H + bin;
+    *d = (first_batch ? 0.0 : *d) + a[v];
+  }
+}
+
+// Spectra of both stations from the natural-order Z (stage entry point).
+__global__ void split_global_kernel(const LargeParams p, const float2* __restrict__ Y,
+                                    uint64_t f0, uint64_t nb, float2* s1, float2* s2) {
+  const int C = p.c, M = kLargeM, N = p.n, H = N / 2 + 1;
+  const uint64_t total = nb * (uint64_t)H;
+  const float u1 = 0.5f / p.st[0].scale, u2 = 0.5f / p.st[1].scale;
+  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t fl = idx / H;
+    const int k = (int)(idx - fl * H);
+    const float2* Zf = Y + fl * (uint64_t)N;
+    const int kn = (N - k) & (N - 1);
+    const float2 a = Zf[(k % C) * M + k / C], b = Zf[(kn % C) * M + kn / C];
+    s1[(f0 + fl) * H + k] = make_float2(u1 * (a.x + b.x), u1 * (a.y - b.y));
+    s2[(f0 + fl) * H + k] = make_float2(u2 * (a.y + b.y), -u2 * (a.x - b.x));
+  }
+}
+
+// ------------------------------------------------------------- launchers
+
+int large_batch_frames(uint32_t n) {
+  // two scratch buffers of batch * n complex f32 each, 64 MiB apiece
+  const uint64_t per = (uint64_t)n * sizeof(float2);
+  return (int)std::max<uint64_t>(1, (64ull << 20) / per);
+}
+
+static int grid_for(uint64_t work, int threads, int sms) {
+  const uint64_t g = (work + threads - 1) / threads;
+  return (int)(g < (uint64_t)sms * 8 ? (g ? g : 1) : (uint64_t)sms * 8);
+}
+
+cudaError_t launch_large_fft(const LargeParams& p, uint64_t f0, uint64_t nb, float2* buf0,
+                             float2* buf1, int sms, cudaStream_t s) {
+  // decode -> buf0, DIF -> buf1, row FFTs in place on buf1
+  decode_global_kernel<<<grid_for(nb * p.n, 256, sms), 256, 0, s>>>(p, f0, nb, buf0, nullptr,
+                                                                     nullptr);
+  const uint64_t work = nb * kLargeM;
+  switch (p.c) {
+    case 2: dif_kernel<2><<<grid_for(work, 256, sms), 256, 0, s>>>(buf0, buf1, nb); break;
+    case 4: dif_kernel<4><<<grid_for(work, 256, sms), 256, 0, s>>>(buf0, buf1, nb); break;
+    case 8: dif_kernel<8><<<grid_for(work, 256, sms), 256, 0, s>>>(buf0, buf1, nb); break;
+    default: return cudaErrorInvalidValue;
+  }
+  const uint32_t smem = 2 * Geom<kLargeM>::CSTRIDE * sizeof(float2);
+  auto kern = cfft_kernel<kLargeM>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const uint64_t rows = nb * (uint64_t)p.c;
+  kern<<<(unsigned)std::min<uint64_t>(rows, (uint64_t)sms), kLargeM / 16, smem, s>>>(buf1, rows);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_large_acc(const LargeParams& p, const float2* Y, uint64_t f0, uint64_t nb,
+                             int groups, int first_batch, double* part, cudaStream_t s) {
+  dim3 grid((kLargeM + 255) / 256, p.c, groups);
+  acc_global_kernel<<<grid, 256, 0, s>>>(p, Y, f0, nb, first_batch, part);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_large_decode(const LargeParams& p, uint64_t f0, uint64_t nb, float* x1,
+                                float* x2, int sms, cudaStream_t s) {
+  decode_global_kernel<<<grid_for(nb * p.n, 256, sms), 256, 0, s>>>(p, f0, nb, nullptr, x1, x2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_large_split(const LargeParams& p, const float2* Y, uint64_t f0, uint64_t nb,
+                               float2* s1, float2* s2, int sms, cudaStream_t s) {
+  split_global_kernel<<<grid_for(nb * (p.n / 2 + 1), 256, sms), 256, 0, s>>>(p, Y, f0, nb, s1,
+                                                                              s2);
+  return cudaGetLastError();
+}
+
+}  // namespace fxc

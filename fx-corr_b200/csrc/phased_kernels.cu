@@ -1,0 +1,323 @@
+// phased_kernels.cu — phased-array synthesis for sm_100a (yi-phasedarray,
+// src/main.rs:2222-2412).
+//
+// Per frame pair, after the same staging / decode / shift / shared two-for-one
+// FFT front end as the correlation kernel:
+//   1. S1, S2 from the shared spectrum, each rotated by its own fractional
+//      delay exp(-2 pi i k df frac_i) with the Nyquist imaginary part zeroed
+//      (apply_delay_and_rate_regular_bins, src/utils.rs:69-124);
+//   2. fringe phasors fr_lo1 / fr_lo2, band alignment onto the output grid
+//      and the weighted sum cb = w1 S1 + w2 S2 (src/main.rs:2264-2280);
+//   3. |cb|^2 accumulated per bin (f32 registers, f64 flushes);
+//   4. for the .raw product: cb[0].im = cb[N/2].im = 0, the inverse real FFT
+//      computed as the forward FFT of the Hermitian-extended conj(cb) scaled by
+//      1/N (src/utils.rs:60-66), odd samples negated when both inputs are LSB,
+//      nearest-level re-quantisation with ant1's levels and packing with ant1's
+//      shuffle (quantise_frame, src/utils.rs:378-410).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fxc_device.cuh"
+#include "fxc_kernels.h"
+
+namespace fxc {
+
+// Nearest level, first index wins ties (utils.rs:384-389).  For tables with
+// more than 16 entries that are strictly monotonic (flag set by the host) a
+// binary search finds the bracket and the exact f32 comparison runs over a
+// window of +-2 entries around it.
+__device__ __forceinline__ uint32_t nearest_level(float x, const float* __restrict__ ql, int n,
+                                                  int monotonic) {
+  int lo = 0, hi = n;
+  if (monotonic != 0 && n > 16) {
+    // ascending (monotonic > 0) or descending (< 0): find first index past x
+    int a = 0, b = n;
+    while (a < b) {
+      const int m = (a + b) >> 1;
+      const bool past = monotonic > 0 ? (ql[m] > x) : (ql[m] < x);
+      if (past) b = m;
+      else a = m + 1;
+    }
+    lo = max(0, a - 2);
+    hi = min(n, a + 2);
+  }
+  uint32_t best = (uint32_t)lo;
+  float min_err = 3.40282347e38f;
+  for (int i = lo; i < hi; ++i) {
+    const float err = fabsf(x - ql[i]);
+    if (err < min_err) {
+      min_err = err;
+      best = (uint32_t)i;
+    }
+  }
+  return best;
+}
+
+template <int N, int FPC>
+__global__ void __launch_bounds__(FPC * N / 16, (N >= 8192 ? 1 : 2))
+phased_kernel(const PhasedParams p) {
+  constexpr int T1 = N / 16;
+  constexpr int T = FPC * T1;
+  constexpr int H = N / 2 + 1;
+  constexpr int BPT = (N / 2) / T;
+  static_assert(BPT * T == N / 2 && BPT >= 2, "bins per thread");
+
+  extern __shared__ __align__(128) uint8_t smem[];
+  const SmemLayout L = smem_layout<N, FPC>(p.stage_bytes);
+  float2* bufA = reinterpret_cast<float2*>(smem + L.off_a);
+  float2* bufB = reinterpret_cast<float2*>(smem + L.off_b);
+  uint8_t* stage = smem + L.off_stage;
+  uint32_t* lut = reinterpret_cast<uint32_t*>(smem + L.off_lut);  // decode LUTs, then encode LUT
+  float* lv = reinterpret_cast<float*>(smem + L.off_lv);          // [0,512) decode levels
+  FrameInfo* finfo = reinterpret_cast<FrameInfo*>(smem + L.off_fi);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.off_bar);
+  int* flag = reinterpret_cast<int*>(smem + L.off_flag);
+  // quantiser tables live in the extra tail of the layout
+  float* ql = reinterpret_cast<float*>(smem + L.total);              // 256 levels
+  uint32_t* elut = reinterpret_cast<uint32_t*>(smem + L.total + 1024);  // [4][256] encode LUT
+
+  const int tid = threadIdx.x;
+  const int g = tid / T1;
+  const int t = tid % T1;
+
+  for (int i = tid; i < 512; i += T) lv[i] = p.st[i >> 8].levels[i & 255] * p.st[i >> 8].scale;
+  for (int s = 0; s < 2; ++s)
+    if (p.st[s].shkind == SH_GENERIC)
+      for (int i = tid; i < 1024; i += T) lut[s * 1024 + i] = p.st[s].shlut[i];
+  for (int i = tid; i < 256; i += T) ql[i] = i < (int)p.nqlevels ? p.qlevels[i] : 0.f;
+  for (int i = tid; i < 1024; i += T) elut[i] = p.enc_lut[i];
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    *flag = 0;
+    fence_proxy_async();
+  }
+  Twiddles<N> tw;
+  tw.init(t);
+
+  const uint64_t iters = (p.nf + FPC - 1) / FPC;
+  const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
+  const uint64_t it1 = ((blockIdx.x + 1) * iters) / gridDim.x;
+  const uint32_t bpf1 = p.st[0].bpf, bpf2 = p.st[1].bpf;
+  constexpr uint32_t kRaw1 = FPC * kFiBytes;
+
+  auto issue = [&](uint64_t it) {
+    const int slot = (int)((it - it0) % kStages);
+    const uint64_t f0 = it * FPC;
+    const uint64_t nvalid = (p.nf - f0) < (uint64_t)FPC ? (p.nf - f0) : (uint64_t)FPC;
+    const uint32_t bf = (uint32_t)(nvalid * kFiBytes);
+    const uint32_t b1 = (uint32_t)(nvalid * bpf1), b2 = (uint32_t)(nvalid * bpf2);
+    uint8_t* dst = stage + slot * L.stage_stride;
+    mbar_expect_tx(&bars[slot], bf + b1 + b2);
+    bulk_g2s(dst, p.finfo + f0, bf, &bars[slot]);
+    bulk_g2s(dst + kRaw1, p.st[0].raw + f0 * bpf1, b1, &bars[slot]);
+    bulk_g2s(dst + kRaw1 + FPC * bpf1, p.st[1].raw + f0 * bpf2, b2, &bars[slot]);
+  };
+  __syncthreads();
+  if (tid == 0)
+    for (uint64_t it = it0; it < it1 && it < it0 + kStages; ++it) issue(it);
+
+  float acc[BPT + 1];
+#pragma unroll
+  for (int i = 0; i <= BPT; ++i) acc[i] = 0.f;
+  const int a1s = p.a1s, a1e = p.a1e, a2s = p.a2s;
+  const int ov = a1e - a1s;
+  const int sb = a2s - a1s;
+  // undo the two-for-one factor 2 and the exact per-station level scaling
+  const float u1 = 0.5f / p.st[0].scale, u2 = 0.5f / p.st[1].scale;
+  bool first_flush = true;
+  uint32_t since_flush = 0;
+  double* part = p.partials + (size_t)blockIdx.x * H;
+  const uint32_t spw = 32u / p.bits_out;           // samples per packed word
+  const uint32_t wpf = (uint32_t)N / spw;          // words per output frame
+  const uint32_t qmask = (p.bits_out >= 32) ? 0xFFFFFFFFu : ((1u << p.bits_out) - 1u);
+
+  auto flush = [&]() {
+#pragma unroll
+    for (int i = 0; i <= BPT; ++i) {
+      if (i == BPT && tid != 0) continue;
+      const int bin = (i < BPT) ? (tid + T * i) : N / 2;
+      double* q = part + bin;
+      *q = (first_flush ? 0.0 : *q) + (double)acc[i];
+      acc[i] = 0.f;
+    }
+    first_flush = false;
+    since_flush = 0;
+  };
+
+  for (uint64_t it = it0; it < it1; ++it) {
+    const int slot = (int)((it - it0) % kStages);
+    const uint32_t parity = (uint32_t)(((it - it0) / kStages) & 1u);
+    const uint64_t frame_local = it * FPC + g;
+    const bool valid = frame_local < p.nf;
+
+    if (!mbar_wait(&bars[slot], parity, kWaitPolls)) {
+      atomicOr(flag, 1);
+      atomicOr(p.err, ERR_WAIT_TIMEOUT);
+    }
+    const uint8_t* st = stage + slot * L.stage_stride;
+    if (t == 0 && valid) finfo[g] = reinterpret_cast<const FrameInfo*>(st)[g];
+    float* x1 = reinterpret_cast<float*>(bufB) + g * 2 * Geom<N>::FSTRIDE;
+    float* x2 = x1 + Geom<N>::FSTRIDE;
+    {
+      float xs[16];
+      if (valid) {
+        decode16(reinterpret_cast<const uint32_t*>(st + kRaw1 + g * bpf1), p.st[0].bits,
+                 p.st[0].shkind, lut, lv, p.st[0].lsb, t, xs);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) xs[i] = 0.f;
+      }
+#pragma unroll
+      for (int i = 0; i < 16; ++i) x1[fpad(16 * t + i)] = xs[i];
+      if (valid) {
+        decode16(reinterpret_cast<const uint32_t*>(st + kRaw1 + FPC * bpf1 + g * bpf2),
+                 p.st[1].bits, p.st[1].shkind, lut + 1024, lv + 256, p.st[1].lsb, t, xs);
+      }
+#pragma unroll
+      for (int i = 0; i < 16; ++i) x2[fpad(16 * t + i)] = xs[i];
+    }
+    __syncthreads();
+    if (*flag) break;
+    if (tid == 0 && it + kStages < it1) {
+      fence_proxy_async();
+      issue(it + kStages);
+    }
+    const int s1 = valid ? finfo[g].s1 : 0;
+    const int s2 = valid ? finfo[g].s2 : 0;
+
+    float2* za = bufA + g * Geom<N>::CSTRIDE;
+    float2* zb = bufB + g * Geom<N>::CSTRIDE;
+    first_pass<N>(x1, x2, s1, s2, za, t);
+    float2* Z0 = fft_rest<N>(za, zb, t, tw);
+    const bool fin_b = Z0 != za;
+    __syncthreads();
+
+    // ---- per-bin synthesis over every valid frame of the iteration; the
+    // inverse-FFT input planes go to the buffer that does not hold Z
+#pragma unroll 1
+    for (int f = 0; f < FPC; ++f) {
+      if (it * FPC + f >= p.nf) break;
+      const float2* Z = (fin_b ? bufB : bufA) + f * Geom<N>::CSTRIDE;
+      float* y1 = reinterpret_cast<float*>(fin_b ? bufA : bufB) + f * 2 * Geom<N>::FSTRIDE;
+      float* y2 = y1 + Geom<N>::FSTRIDE;
+      const FrameInfo& F = finfo[f];
+      // spectrum of station s at its own bin k: unscaled, rotated by the
+      // station's fractional delay, Nyquist imaginary part zeroed, times fr_lo
+      auto station_bin = [&](int s, int k) -> float2 {
+        const float2 a = Z[cpad(k)], b = Z[cpad((N - k) & (N - 1))];
+        float2 v = s == 0 ? make_float2(u1 * (a.x + b.x), u1 * (a.y - b.y))
+                          : make_float2(u2 * (a.y + b.y), u2 * (b.x - a.x));
+        float sn, cs;
+        __sincosf((float)k * (s == 0 ? F.st1 : F.st2), &sn, &cs);
+        v = cmul(v, make_float2(cs, sn));
+        if (k == N / 2) v.y = 0.f;
+        return cmul(v, s == 0 ? F.fr_lo1 : F.fr_lo2);
+      };
+      auto bin_cb = [&](int k) -> float2 {
+        float2 a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
+        if (p.grid == 0) {
+          a1 = station_bin(0, k);
+          if (k >= a1s && k < a1e) a2 = station_bin(1, k + sb);
+        } else {
+          a2 = station_bin(1, k);
+          if (k >= a2s && k < a2s + ov) a1 = station_bin(0, k - sb);
+        }
+        return make_float2(a1.x * p.w1 + a2.x * p.w2, a1.y * p.w1 + a2.y * p.w2);
+      };
+      auto emit = [&](int k, float2 cb) {
+        // Hermitian extension of conj(cb) as planes for the forward FFT
+        if (k == 0 || k == N / 2) cb.y = 0.f;
+        y1[fpad(k)] = cb.x;
+        y2[fpad(k)] = -cb.y;
+        if (k != 0 && k != N / 2) {
+          y1[fpad(N - k)] = cb.x;
+          y2[fpad(N - k)] = cb.y;
+        }
+      };
+#pragma unroll
+      for (int i = 0; i < BPT; ++i) {
+        const int k = tid + T * i;
+        const float2 cb = bin_cb(k);
+        acc[i] += cnorm2(cb);
+        if (p.want_raw) emit(k, cb);
+      }
+      if (tid == 0) {
+        const float2 cb = bin_cb(N / 2);
+        acc[BPT] += cnorm2(cb);
+        if (p.want_raw) emit(N / 2, cb);
+      }
+    }
+    if (++since_flush >= p.flush_every) flush();
+
+    if (p.want_raw) {
+      __syncthreads();
+      // inverse real FFT of frame slot g: forward FFT of conj(C), real part / N
+      float* y1 = reinterpret_cast<float*>(fin_b ? bufA : bufB) + g * 2 * Geom<N>::FSTRIDE;
+      float* y2 = y1 + Geom<N>::FSTRIDE;
+      float2* qa = (fin_b ? bufB : bufA) + g * Geom<N>::CSTRIDE;  // free: Z consumed
+      float2* qb = (fin_b ? bufA : bufB) + g * Geom<N>::CSTRIDE;
+      first_pass<N>(y1, y2, 0, 0, qa, t);
+      float2* Y = fft_rest<N>(qa, qb, t, tw);
+      __syncthreads();
+      if (valid) {
+        const float inv_n = 1.0f / (float)N;
+        uint8_t* out = p.raw_out + frame_local * p.bpf_out;
+        for (uint32_t w = (uint32_t)t; w < wpf; w += T1) {
+          uint32_t word = 0;
+          for (uint32_t i = 0; i < spw; ++i) {
+            const uint32_t n = w * spw + i;
+            float x = Y[cpad((int)n)].x * inv_n;
+            if (p.out_lsb && (n & 1u)) x = -x;
+            word |= (nearest_level(x, ql, (int)p.nqlevels, p.qmonotonic) & qmask)
+                    << (i * p.bits_out);
+          }
+          const uint32_t sw = elut[word & 255u] | elut[256 + ((word >> 8) & 255u)] |
+                              elut[512 + ((word >> 16) & 255u)] | elut[768 + (word >> 24)];
+          reinterpret_cast<uint32_t*>(out)[w] = sw;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (since_flush > 0 || first_flush) flush();
+  if (tid == 0 && *flag) {
+    for (int s = 0; s < kStages; ++s) mbar_wait(&bars[s], 0, kWaitPolls);
+  }
+}
+
+// Fixed-order sum of the per-CTA phased partials into acc[4H, 5H).
+__global__ void reduce_phased_kernel(const double* __restrict__ part, int nblk, int h,
+                                     double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= h) return;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[(size_t)b * h + k];
+  out[4 * h + k] = s;
+}
+
+template <int N, int FPC>
+static cudaError_t launch_phased_one(const PhasedParams& p, int grid, cudaStream_t stream) {
+  const uint32_t smem = smem_layout<N, FPC>(p.stage_bytes).total + 1024 + 4096;
+  auto kern = phased_kernel<N, FPC>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, FPC * N / 16, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_phased(uint32_t n, const PhasedParams& p, int grid, cudaStream_t s) {
+  switch (n) {
+    case 1024: return launch_phased_one<1024, 4>(p, grid, s);
+    case 2048: return launch_phased_one<2048, 2>(p, grid, s);
+    case 4096: return launch_phased_one<4096, 1>(p, grid, s);
+    case 8192: return launch_phased_one<8192, 1>(p, grid, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_reduce_phased(const double* part, int nblk, int h, double* out, cudaStream_t s) {
+  reduce_phased_kernel<<<(h + 255) / 256, 256, 0, s>>>(part, nblk, h, out);
+  return cudaGetLastError();
+}
+
+}  // namespace fxc

@@ -330,11 +330,18 @@ class Scan:
         import torch
         h = self.cfg.h
         acc = torch.empty(5 * h, dtype=torch.float64, device="cuda")
-        self.run_device(d_raw1, d_raw2, nf, first_frame, acc, stream=stream)
+        raw = None
+        if self.cfg.products & PROD_RAW:
+            raw = torch.empty(max(1, nf * self.cfg.bpf(self.cfg.bits_out)), dtype=torch.uint8,
+                              device="cuda")
+        self.run_device(d_raw1, d_raw2, nf, first_frame, acc, d_raw_out=raw, stream=stream)
         self.check()
         a = acc.cpu().numpy()
-        return dict(acf11=a[:h], acf22=a[h:2 * h], xcf=a[2 * h:4 * h].view(np.complex128),
-                    phased=a[4 * h:])
+        out = dict(acf11=a[:h], acf22=a[h:2 * h], xcf=a[2 * h:4 * h].view(np.complex128),
+                   phased=a[4 * h:])
+        if raw is not None:
+            out["raw"] = raw.cpu().numpy()[: nf * self.cfg.bpf(self.cfg.bits_out)]
+        return out
 
     # -- host-buffer path (the reference-facing per-sector call)
     def submit(self, raw1, raw2, nf: int, first_frame: int = 0) -> int:
@@ -345,6 +352,8 @@ class Scan:
                                       nf, first_frame, C.byref(sid)))
         self._keep = getattr(self, "_keep", {})
         self._keep[sid.value] = (r1, r2)
+        self._nf = getattr(self, "_nf", {})
+        self._nf[sid.value] = nf
         return sid.value
 
     def wait(self, sector_id: int, timeout_ms: int = -1) -> dict:
@@ -356,12 +365,22 @@ class Scan:
         o.acf22 = a22.ctypes.data_as(C.POINTER(C.c_double))
         o.xcf = x.ctypes.data_as(C.POINTER(C.c_double))
         o.phased = ph.ctypes.data_as(C.POINTER(C.c_double))
+        raw = None
+        if self.cfg.products & PROD_RAW:
+            nf = getattr(self, "_nf", {}).get(sector_id, 0)
+            raw = np.zeros(max(1, nf * self.cfg.bpf(self.cfg.bits_out)), np.uint8)
+            o.raw_out = raw.ctypes.data_as(C.POINTER(C.c_uint8))
+            o.raw_out_len = raw.size
         try:
             check(lib().fxc_sector_wait(self.h, sector_id, timeout_ms, C.byref(o)))
         finally:
             getattr(self, "_keep", {}).pop(sector_id, None)
-        return dict(acf11=a11, acf22=a22, xcf=x.view(np.complex128), phased=ph,
-                    failed=o.frames_failed)
+        out = dict(acf11=a11, acf22=a22, xcf=x.view(np.complex128), phased=ph,
+                   failed=o.frames_failed)
+        if raw is not None:
+            out["raw"] = raw[: getattr(self, "_nf", {}).pop(sector_id, 0) *
+                             self.cfg.bpf(self.cfg.bits_out)]
+        return out
 
 
 # -------------------------------------------------------------- helpers

@@ -274,3 +274,69 @@ def test_parseval_full_sector(engine):
     # whole sector: E[x^2] = 5 for uniform codes over {+-1, +-3}; 1e9 samples
     assert math.isclose(one_sided / (n * nf * n), 5.0, rel_tol=2e-3)
     s.close()
+
+
+# ------------------------------------------------- FFT lengths above 8192
+
+@pytest.mark.parametrize("n", [16384, 32768, 65536])
+def test_large_decode_bit_exact(engine, n):
+    fs = 512e6
+    delay = dict(net_d1_base=-0.6 * n / fs, total_rate1_base=0.05, net_d2_base=7.0 / fs)
+    scan = make_scan(fft=n, fs=fs, bits1=2, bits2=4, shuffle="generic", lsb1=True, delay=delay,
+                     seed=n)
+    nf = 5
+    r1, r2 = random_raw(scan, nf, seed=n + 1)
+    s = engine.open_scan(to_fxc(scan))
+    x1, x2 = s.decode(dev(r1), dev(r2), nf, first_frame=2)
+    s.check()
+    x1, x2 = x1.cpu().numpy(), x2.cpu().numpy()
+    ents = oracle.c_delay_entries(scan, 2, nf)
+    b1, b2 = scan.bpf(2), scan.bpf(4)
+    for i in range(nf):
+        e1 = oracle.c_decode(r1[i * b1:(i + 1) * b1], n, 2, scan.shuffle1, scan.levels1, True)
+        e2 = oracle.c_decode(r2[i * b2:(i + 1) * b2], n, 4, scan.shuffle2, scan.levels2, False)
+        np.testing.assert_array_equal(x1[i], oracle.c_shift(e1, ents["int1"][i]))
+        np.testing.assert_array_equal(x2[i], oracle.c_shift(e2, ents["int2"][i]))
+    s.close()
+
+
+@pytest.mark.parametrize("n", [16384, 65536])
+def test_large_spectra_vs_fp64(engine, n):
+    scan = make_scan(fft=n, fs=512e6, bits1=2, bits2=8, shuffle="generic", lsb1=True,
+                     delay=DELAY)
+    nf = 3
+    r1, r2 = signal_raw(scan, nf, seed=n, rho=0.3, delay_samples=3.7)
+    s = engine.open_scan(to_fxc(scan))
+    s1, s2 = s.spectra(dev(r1), dev(r2), nf, first_frame=0)
+    s.check()
+    s1, s2 = s1.cpu().numpy(), s2.cpu().numpy()
+    ents = oracle.np_delay_entries(scan, 0, nf)
+    x1 = oracle.np_decode_frames(r1, nf, n, scan.bits1, scan.shuffle1, scan.levels1, True)
+    x2 = oracle.np_decode_frames(r2, nf, n, scan.bits2, scan.shuffle2, scan.levels2, False)
+    x1 = oracle.np_shift_frames(x1, np.array([e[0] for e in ents]))
+    x2 = oracle.np_shift_frames(x2, np.array([e[1] for e in ents]))
+    f1, f2 = np.fft.rfft(x1, axis=1), np.fft.rfft(x2, axis=1)
+    for a, b, name in ((s1, f1, "S1"), (s2, f2, "S2")):
+        err = np.abs(a - b).max() / np.sqrt(np.mean(np.abs(b) ** 2))
+        assert err < 5e-6, (name, err)
+    s.close()
+
+
+LARGE_CASES = [
+    dict(fft=16384, band=(256, 0, 7936, 256), grid=0, shuffle="generic", lsb1=True),
+    dict(fft=32768, band=(-64, 64, 16384, 0), grid=1, bits1=4, bits2=4),
+    dict(fft=65536, band=(0, 0, 32768, 0), grid=0, bits1=1, bits2=2,
+         products=oracle.PROD_ACF | oracle.PROD_ACF_OVERLAP_ONLY | oracle.PROD_XCF),
+]
+
+
+@pytest.mark.parametrize("kw", LARGE_CASES)
+@pytest.mark.parametrize("nf", [1, 37])
+def test_large_sector_vs_fp64(engine, kw, nf):
+    scan = make_scan(delay=DELAY, fs=512e6, **kw)
+    r1, r2 = signal_raw(scan, nf, seed=nf + kw["fft"], rho=0.2, delay_samples=6.4)
+    s = engine.open_scan(to_fxc(scan))
+    got = s.sector_device(dev(r1), dev(r2), nf, first_frame=3)
+    ref = oracle.fp64_sector_corr(scan, r1, r2, nf, first_frame=3)
+    assert_sector_close(got, ref, scan, f"gpu vs fp64 {kw} nf={nf}", nf=nf)
+    s.close()
