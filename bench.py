@@ -184,8 +184,8 @@ def measured_peaks():
 
 def profile_traffic_per_frame_pair():
     """DRAM bytes per frame pair of the correlation kernel from the committed
-    ncu summary (profiles/corr_kernel_n8192.md), or None."""
-    f = ROOT / "profiles" / "corr_kernel_n8192.md"
+    ncu summary (profiles/corr_kernel_n8192.txt), or None."""
+    f = ROOT / "profiles" / "corr_kernel_n8192.txt"
     if not f.exists():
         return None
     for ln in f.read_text().splitlines():
@@ -203,22 +203,24 @@ def flops_per_station_sample(n):
 
 # -------------------------------------------------------------- CPU legs
 
-def cpu_sample(cfg_o, raw1, raw2, target_s=8.0, max_frames=NF_SECTOR):
-    """Times the oracle port (all host threads) on a bounded sample and returns
-    (Gsample/s, frames, threads, seconds)."""
+def cpu_sample(cfg_o, get_sector, nsec, nfs, target_s=10.0):
+    """Times the oracle port (OpenMP, all host threads) sector by sector over
+    the scan until about target_s seconds of CPU work; returns (Gsample/s,
+    frames, threads, seconds)."""
     import oracle
 
     oracle.build()
     threads = os.cpu_count() or 1
-    nf = 256
-    t0 = time.perf_counter()
-    oracle.c_sector_corr(cfg_o, raw1, raw2, nf, 0, threads)
-    dt = time.perf_counter() - t0
-    nf = int(min(max_frames, max(256, nf * target_s / max(dt, 1e-3))))
-    t0 = time.perf_counter()
-    oracle.c_sector_corr(cfg_o, raw1, raw2, nf, 0, threads)
-    dt = time.perf_counter() - t0
-    return 2 * nf * N / dt / 1e9, nf, threads, dt
+    frames, spent = 0, 0.0
+    for i in range(nsec):
+        r1, r2 = get_sector(i)
+        t0 = time.perf_counter()
+        oracle.c_sector_corr(cfg_o, r1, r2, nfs, i * nfs, threads)
+        spent += time.perf_counter() - t0
+        frames += nfs
+        if spent >= target_s:
+            break
+    return 2 * frames * N / spent / 1e9, frames, threads, spent
 
 
 def to_oracle_scan(cfg):
@@ -442,11 +444,11 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         sys.path.insert(0, str(ROOT / "oracle"))
         cfg_o = to_oracle_scan(cfg)
-        r1 = sec1[0].cpu().numpy()
-        r2 = sec2[0].cpu().numpy()
-        v, nf_cpu, thr, dt = cpu_sample(cfg_o, r1, r2)
+        v, nf_cpu, thr, dt = cpu_sample(
+            cfg_o, lambda i: (sec1[i].cpu().numpy(), sec2[i].cpu().numpy()), SECTORS_, NFS)
         cpu = {"value": v, "unit": "Gsample/s", "cores": thr, "kind": "port",
-               "sample": f"{nf_cpu} frame pairs of sector 0 ({dt:.1f} s, OpenMP, all threads)"}
+               "sample": f"first {nf_cpu} frame pairs of the scan ({dt:.1f} s of CPU work, "
+                         f"C restatement, OpenMP over all host threads)"}
 
     if rank == 0:
         line = {
