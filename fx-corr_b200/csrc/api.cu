@@ -927,3 +927,26 @@ fxc_status fxc_normalize(uint32_t fft, uint64_t nf, double level_power, const do
 }
 
 }  // extern "C"
+
+// Internal helpers shared with noalloc.cu (no allocation, host only).
+namespace fxc {
+
+fxc_status internal_fail(fxc_status s, const char* msg) { return fail(s, "%s", msg); }
+
+fxc_status internal_prepare_tables(const fxc_scan_cfg* c, uint32_t* lut2048, float* lv512,
+                                   float scale[2], int kind[2]) {
+  const fxc_status st = validate_cfg(c);
+  if (st != FXC_OK) return st;
+  build_lut(c->shuffle1, lut2048);
+  build_lut(c->shuffle2, lut2048 + 1024);
+  for (int i = 0; i < 512; ++i) lv512[i] = 0.0f;
+  for (uint32_t i = 0; i < c->nlevels1; ++i) lv512[i] = (float)c->levels1[i];
+  for (uint32_t i = 0; i < c->nlevels2; ++i) lv512[256 + i] = (float)c->levels2[i];
+  scale[0] = level_scale(c->levels1, c->nlevels1);
+  scale[1] = level_scale(c->levels2, c->nlevels2);
+  kind[0] = shuffle_kind(c->shuffle1);
+  kind[1] = shuffle_kind(c->shuffle2);
+  return FXC_OK;
+}
+
+}  // namespace fxc

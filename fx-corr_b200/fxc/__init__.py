@@ -33,8 +33,9 @@ EXPORTS = [
     "fxc_sector_wait", "fxc_sector_run_device", "fxc_scan_check", "fxc_delay_entries_device",
     "fxc_decode_device", "fxc_spectra_device", "fxc_parse_shuffle", "fxc_band_alignment",
     "fxc_level_power", "fxc_normalize", "fxc_bytes_per_frame", "fxc_probe_fp32_peak",
-    "fxc_scan_set_profiling", "fxc_scan_profile",
+    "fxc_scan_set_profiling", "fxc_scan_profile", "fxc_sector_run_device_noalloc",
 ]
+NOALLOC_MAX_FRAMES = 32768
 
 
 class FxcError(RuntimeError):
@@ -136,6 +137,8 @@ def lib():
         "fxc_bytes_per_frame": ([C.c_uint32, C.c_uint32], C.c_uint64),
         "fxc_probe_fp32_peak": ([C.c_int32, f64p], st),
         "fxc_scan_set_profiling": ([vp, C.c_int32], st),
+        "fxc_sector_run_device_noalloc": ([C.POINTER(ScanCfgC), vp, vp, C.c_uint64, C.c_uint64,
+                                           vp, vp], st),
         "fxc_scan_profile": ([vp, f64p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_int32],
                              st),
     }
@@ -415,6 +418,16 @@ def normalize(fft, nf, level_power_, acc_real=None, acc_cplx=None):
                               None if ar is None else ar.ctypes.data_as(f64),
                               None if ac is None else ac.ctypes.data_as(f64), out.ctypes.data))
     return out.view(np.complex64)
+
+
+def sector_run_device_noalloc(cfg: ScanConfig, d_raw1, d_raw2, nf: int, first_frame: int,
+                              d_acc, stream=None):
+    """fxc_sector_run_device_noalloc: one sector on device inputs without any
+    device allocation (scratch is the library's fixed array), on the current
+    device; asynchronous on `stream`."""
+    c = cfg.to_c()
+    check(lib().fxc_sector_run_device_noalloc(C.byref(c), _ptr(d_raw1), _ptr(d_raw2), nf,
+                                              first_frame, _ptr(d_acc), _stream(stream)))
 
 
 def probe_fp32_peak(device: int = 0) -> float:

@@ -176,6 +176,32 @@ FXC_API fxc_status fxc_scan_set_profiling(fxc_scan* s, int32_t enable);
 FXC_API fxc_status fxc_scan_profile(fxc_scan* s, double* kernel_ms, uint64_t* kernel_launches,
                                     uint64_t* all_launches, int32_t reset);
 
+/* ---- allocation-free correlation call ----------------------------------
+ * No counterpart in the reference (its CPU path allocates per sector); this
+ * entry point exists for callers that cannot allocate device memory where
+ * they correlate: a real-time streaming loop that must not pay the implicit
+ * device synchronisation of cudaMalloc/cudaFree, or a host application whose
+ * memory manager owns all device memory.
+ *
+ * Same result as opening a scan with `cfg` and calling fxc_sector_run_device
+ * (ACF/XCF products), without an engine or scan and without allocating: the
+ * kernels' scratch is a fixed FXC_NOALLOC_SCRATCH_MIB MiB array that every
+ * GPU loading the library holds until the process exits.  Limits: fft_len
+ * <= 8192, nf <= FXC_NOALLOC_MAX_FRAMES per call (add the results of several
+ * calls for a longer sector), geometric table <= FXC_NOALLOC_MAX_GEOM entries;
+ * larger requests fail with FXC_EINVAL / FXC_EUNSUPPORTED.  Runs on the
+ * current device, enqueued on `stream`.  The first call on each device looks
+ * up the array's device address, so make that first call before any stream
+ * capture.  All calls share the array: calls whose work overlaps on one GPU
+ * (other streams or host threads) race and must be serialised by the caller. */
+#define FXC_NOALLOC_MAX_FRAMES 32768
+#define FXC_NOALLOC_MAX_GEOM 4096
+#define FXC_NOALLOC_SCRATCH_MIB 24
+FXC_API fxc_status fxc_sector_run_device_noalloc(const fxc_scan_cfg* cfg, const uint8_t* d_raw1,
+                                                 const uint8_t* d_raw2, uint64_t nf,
+                                                 uint64_t first_frame, double* d_acc,
+                                                 void* stream);
+
 /* Stage entry points, for parity tests of the individual steps. */
 /* Per-frame delay model on the device (src/main.rs:184-241). */
 FXC_API fxc_status fxc_delay_entries_device(fxc_scan* s, uint64_t first_frame, uint64_t nf,
