@@ -129,38 +129,21 @@ corr_kernel(const CorrParams p) {
       atomicOr(flag, 1);
       atomicOr(p.err, ERR_WAIT_TIMEOUT);
     }
-    const uint8_t* st = stage + slot * L.stage_stride;
+    uint8_t* st = stage + slot * L.stage_stride;
+    uint32_t* w1 = reinterpret_cast<uint32_t*>(st + kRaw1);
+    uint32_t* w2 = reinterpret_cast<uint32_t*>(st + kRaw1 + FPC * bpf1);
+    // non-identity 32-bit shuffles are applied once, in place, to the staged words
+    preshuffle_slot(w1, FPC * bpf1 / 4, p.st[0].shkind, lut, w2, FPC * bpf2 / 4, p.st[1].shkind,
+                    lut + 1024, tid, T);
     if (t == 0 && valid) finfo[g] = reinterpret_cast<const FrameInfo*>(st)[g];
-    // ---- decode both stations of frame slot g into the planes (aliasing B)
-    float* x1 = reinterpret_cast<float*>(bufB) + g * 2 * Geom<N>::FSTRIDE;
-    float* x2 = x1 + Geom<N>::FSTRIDE;
-    {
-      float xs[16];
-      if (valid) {
-        decode16(reinterpret_cast<const uint32_t*>(st + kRaw1 + g * bpf1), p.st[0].bits,
-                 p.st[0].shkind, lut, lv, p.st[0].lsb, t, xs);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 16; ++i) xs[i] = 0.f;
-      }
-#pragma unroll
-      for (int i = 0; i < 16; ++i) x1[fpad(16 * t + i)] = xs[i];
-      if (valid) {
-        decode16(reinterpret_cast<const uint32_t*>(st + kRaw1 + FPC * bpf1 + g * bpf2),
-                 p.st[1].bits, p.st[1].shkind, lut + 1024, lv + 256, p.st[1].lsb, t, xs);
-      }
-#pragma unroll
-      for (int i = 0; i < 16; ++i) x2[fpad(16 * t + i)] = xs[i];
-    }
     __syncthreads();
     if (*flag) break;
-    // staging slot consumed: refill it with iteration it + kStages
-    if (tid == 0 && it + kStages < it1) {
-      fence_proxy_async();
-      issue(it + kStages);
-    }
     const int s1 = valid ? finfo[g].s1 : 0;
     const int s2 = valid ? finfo[g].s2 : 0;
+    const PackedStation pa{w1 + g * (bpf1 / 4), lv, (uint32_t)p.st[0].bits,
+                           (1u << p.st[0].bits) - 1u, p.st[0].lsb ? 1 : 0, s1};
+    const PackedStation pb{w2 + g * (bpf2 / 4), lv + 256, (uint32_t)p.st[1].bits,
+                           (1u << p.st[1].bits) - 1u, p.st[1].lsb ? 1 : 0, s2};
 
     if constexpr (MODE == MODE_DECODE) {
       if (valid) {
@@ -169,18 +152,28 @@ corr_kernel(const CorrParams p) {
         const float u1 = 1.0f / p.st[0].scale, u2 = 1.0f / p.st[1].scale;  // exact
         for (int n = t; n < N; n += T1) {
           const int m1 = n - s1, m2 = n - s2;
-          o1[n] = ((unsigned)m1 < (unsigned)N) ? x1[fpad(m1)] * u1 : 0.f;
-          o2[n] = ((unsigned)m2 < (unsigned)N) ? x2[fpad(m2)] * u2 : 0.f;
+          o1[n] = ((unsigned)m1 < (unsigned)N) ? packed_sample(pa, m1) * u1 : 0.f;
+          o2[n] = ((unsigned)m2 < (unsigned)N) ? packed_sample(pb, m2) * u2 : 0.f;
         }
       }
       __syncthreads();
+      if (tid == 0 && it + kStages < it1) {
+        fence_proxy_async();
+        issue(it + kStages);
+      }
       continue;
     }
 
     float2* za = bufA + g * Geom<N>::CSTRIDE;
     float2* zb = bufB + g * Geom<N>::CSTRIDE;
-    first_pass<N>(x1, x2, s1, s2, za, t);
+    first_pass_packed<N>(pa, pb, za, t);
     float2* Z0 = fft_rest<N>(za, zb, t, tw);
+    // fft_rest opened with a barrier after the fused first pass: the staging
+    // slot is consumed, refill it with iteration it + kStages
+    if (tid == 0 && it + kStages < it1) {
+      fence_proxy_async();
+      issue(it + kStages);
+    }
     // the final buffer sits at the same offset for every frame slot
     const bool fin_b = Z0 != za;
     __syncthreads();
@@ -191,7 +184,7 @@ corr_kernel(const CorrParams p) {
         float2* o2 = reinterpret_cast<float2*>(p.out_b) + frame_local * H;
         const float u1 = 0.5f / p.st[0].scale, u2 = 0.5f / p.st[1].scale;  // exact
         for (int k = t; k < H; k += T1) {
-          const float2 a = Z0[cpad(k)], b = Z0[cpad((N - k) & (N - 1))];
+          const float2 a = Z0[k], b = Z0[(N - k) & (N - 1)];
           o1[k] = make_float2(u1 * (a.x + b.x), u1 * (a.y - b.y));
           o2[k] = make_float2(u2 * (a.y + b.y), -u2 * (a.x - b.x));
         }
@@ -216,14 +209,14 @@ corr_kernel(const CorrParams p) {
       __sincosf((float)T * F.dphi, &sn, &cs);
       const float2 rstep = make_float2(cs, sn);
       auto bin_acc = [&](int bin, float2 r, float* a) {
-        const float2 u = Z[cpad(bin)], w = Z[cpad((N - bin) & (N - 1))];
+        const float2 u = Z[bin], w = Z[(N - bin) & (N - 1)];
         if (p.grid == 0) {
           const bool inov = bin >= a1s && bin < a1e;
           const float2 p1 = make_float2(u.x + w.x, u.y - w.y);  // 2*S1[bin]
           if (want_acf && (!ov_only || inov)) a[0] += cnorm2(p1);
           if (inov) {
             const int i2 = bin + sb;
-            const float2 c = Z[cpad(i2)], d = Z[cpad((N - i2) & (N - 1))];
+            const float2 c = Z[i2], d = Z[(N - i2) & (N - 1)];
             const float2 q2 = make_float2(c.y + d.y, d.x - c.x);  // 2*S2[i2]
             if (want_acf) a[1] += cnorm2(q2);
             if (want_xcf) {
@@ -238,7 +231,7 @@ corr_kernel(const CorrParams p) {
           if (want_acf && (!ov_only || inov)) a[1] += cnorm2(p2);
           if (inov) {
             const int i1 = bin - sb;
-            const float2 c = Z[cpad(i1)], d = Z[cpad((N - i1) & (N - 1))];
+            const float2 c = Z[i1], d = Z[(N - i1) & (N - 1)];
             const float2 q1 = make_float2(c.x + d.x, c.y - d.y);  // 2*S1[i1]
             if (want_acf) a[0] += cnorm2(q1);
             if (want_xcf) {

@@ -222,8 +222,11 @@ struct Twiddles {
 };
 
 // One Stockham pass (radix R, stride NS) over padded complex buffers: every
-// thread handles 16/R work items j = t + T1*w.
-template <int N, int R, int NS>
+// thread handles 16/R work items j = t + T1*w.  The last pass of a transform
+// (OUT_PAD = false) stores an unpadded natural-order spectrum: its stores are
+// consecutive runs, and unpadded consecutive runs of any alignment (the
+// Z[N-k], Z[k+sb] reads of the consumers) are free of bank conflicts.
+template <int N, int R, int NS, bool OUT_PAD = true>
 __device__ __forceinline__ void stockham_pass(const float2* __restrict__ in, float2* __restrict__ out,
                                               int t, float2 w) {
   constexpr int T1 = N / 16;
@@ -309,9 +312,15 @@ __device__ __forceinline__ void stockham_pass(const float2* __restrict__ in, flo
   for (int wi = 0; wi < WI; ++wi) {
     const int j = t + T1 * wi;
     const int k = j & (NS - 1);
-    float2* dst = out + cpad((j - k) * R + k);
+    if constexpr (OUT_PAD) {
+      float2* dst = out + cpad((j - k) * R + k);
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst[r * SS] = v[wi * R + out_pos<R>(r)];
+      for (int r = 0; r < R; ++r) dst[r * SS] = v[wi * R + out_pos<R>(r)];
+    } else {
+      float2* dst = out + (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) dst[r * NS] = v[wi * R + out_pos<R>(r)];
+    }
   }
 }
 
@@ -321,13 +330,91 @@ template <int N>
 __device__ __forceinline__ void first_pass(const float* __restrict__ x1, const float* __restrict__ x2,
                                            int s1, int s2, float2* __restrict__ out, int t) {
   constexpr int T1 = N / 16;
+  static_assert(T1 % 32 == 0, "plane stride");
+  // fpad(t + r*T1) = fpad(t) + r*(T1 + T1/32) since T1 is a multiple of 32
+  constexpr int PS = T1 + T1 / 32;
   float2 v[16];
+  // the shift is uniform per frame: unshifted stations take the unchecked path
+  if (s1 == 0) {
+    const float* p = x1 + fpad(t);
 #pragma unroll
-  for (int r = 0; r < 16; ++r) {
-    const int n = t + r * T1;
-    const int m1 = n - s1, m2 = n - s2;
-    v[r].x = ((unsigned)m1 < (unsigned)N) ? x1[fpad(m1)] : 0.0f;
-    v[r].y = ((unsigned)m2 < (unsigned)N) ? x2[fpad(m2)] : 0.0f;
+    for (int r = 0; r < 16; ++r) v[r].x = p[r * PS];
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m = t + r * T1 - s1;
+      v[r].x = ((unsigned)m < (unsigned)N) ? x1[fpad(m)] : 0.0f;
+    }
+  }
+  if (s2 == 0) {
+    const float* p = x2 + fpad(t);
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r].y = p[r * PS];
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m = t + r * T1 - s2;
+      v[r].y = ((unsigned)m < (unsigned)N) ? x2[fpad(m)] : 0.0f;
+    }
+  }
+  dft16(v);
+  float2* dst = out + 17 * t;  // cpad(16 t + r) = 17 t + r
+#pragma unroll
+  for (int r = 0; r < 16; ++r) dst[r] = v[out_pos<16>(r)];
+}
+
+// One station of a frame as staged packed words (already shuffled into the
+// decoder's bit order), decoded on the fly by first_pass_packed.
+struct PackedStation {
+  const uint32_t* words;  // the frame's words in shared memory
+  const float* lv;        // levels (scaled) in shared memory
+  uint32_t bits, mask;
+  int lsb;                // negate odd samples (LSB -> USB, src/utils.rs:196-197)
+  int shift;              // integer shift of this frame, clamped to [-N, N]
+};
+
+// Sample m of the frame (0 <= m < N): b-bit code taken LSB-first from the
+// packed words (src/utils.rs:215-376), mapped to its level, odd samples negated
+// for LSB input.
+__device__ __forceinline__ float packed_sample(const PackedStation& p, int m) {
+  const uint32_t bit = (uint32_t)m * p.bits;
+  const uint32_t w = p.words[bit >> 5];
+  const float v = p.lv[(w >> (bit & 31u)) & p.mask];
+  return __int_as_float(__float_as_int(v) ^ (int)((uint32_t)(m & p.lsb) << 31));
+}
+
+// First pass fused with the decode: z[n] = x1[n - s1] + i x2[n - s2] read
+// straight from the packed words with the integer shift and zero fill
+// (src/utils.rs:126-145).  Lanes take consecutive n, so each word load is a
+// broadcast; a station with zero shift takes the unchecked path.
+template <int N>
+__device__ __forceinline__ void first_pass_packed(const PackedStation& a, const PackedStation& b,
+                                                  float2* __restrict__ out, int t) {
+  constexpr int T1 = N / 16;
+  float2 v[16];
+  if (a.shift == 0) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r].x = packed_sample(a, t + r * T1);
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m = t + r * T1 - a.shift;
+      const bool in = (unsigned)m < (unsigned)N;
+      const float x = packed_sample(a, in ? m : 0);
+      v[r].x = in ? x : 0.0f;
+    }
+  }
+  if (b.shift == 0) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r].y = packed_sample(b, t + r * T1);
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m = t + r * T1 - b.shift;
+      const bool in = (unsigned)m < (unsigned)N;
+      const float x = packed_sample(b, in ? m : 0);
+      v[r].y = in ? x : 0.0f;
+    }
   }
   dft16(v);
   float2* dst = out + 17 * t;  // cpad(16 t + r) = 17 t + r
@@ -343,20 +430,22 @@ __device__ __forceinline__ float2* fft_rest(float2* a, float2* b, int t, const T
   constexpr int RL = Geom<N>::RL;
   float2* in = a;
   float2* out = b;
-  if constexpr (P16 >= 2) {
+  // the returned spectrum is unpadded: Z[k] at index k
+  static_assert(P16 >= 2, "at least two radix-16 passes");
+  {
     __syncthreads();
-    stockham_pass<N, 16, 16>(in, out, t, tw.w[1]);
+    stockham_pass<N, 16, 16, (P16 >= 3 || RL > 1)>(in, out, t, tw.w[1]);
     float2* x = in; in = out; out = x;
   }
   if constexpr (P16 >= 3) {
     __syncthreads();
-    stockham_pass<N, 16, 256>(in, out, t, tw.w[2]);
+    stockham_pass<N, 16, 256, (RL > 1)>(in, out, t, tw.w[2]);
     float2* x = in; in = out; out = x;
   }
   if constexpr (RL > 1) {
     constexpr int NS = 1 << (4 * P16);
     __syncthreads();
-    stockham_pass<N, RL, NS>(in, out, t, tw.w[P16]);
+    stockham_pass<N, RL, NS, false>(in, out, t, tw.w[P16]);
     float2* x = in; in = out; out = x;
   }
   return in;
@@ -462,7 +551,7 @@ __device__ __forceinline__ void frame_info(const DelayParams& p, uint64_t frame_
 }
 
 // ----------------------------------------------------------------- decode
-// utils.rs:215-376 for the 16 samples [16q, 16q+16) of one frame.
+// 32-bit word shuffle of the decoder (src/utils.rs:159-171).
 
 __device__ __forceinline__ uint32_t shuffle_word(uint32_t w, int kind, const uint32_t* lut) {
   if (kind == SH_PAIRSWAP) return ((w & 0xAAAAAAAAu) >> 1) | ((w & 0x55555555u) << 1);
@@ -472,37 +561,16 @@ __device__ __forceinline__ uint32_t shuffle_word(uint32_t w, int kind, const uin
   return w;
 }
 
-__device__ __forceinline__ void decode16(const uint32_t* __restrict__ words, int bits, int kind,
-                                         const uint32_t* lut, const float* __restrict__ lv, int lsb,
-                                         int q, float (&x)[16]) {
-  if (bits == 2) {
-    const uint32_t w = shuffle_word(words[q], kind, lut);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) x[i] = lv[(w >> (2 * i)) & 3u];
-  } else if (bits == 1) {
-    const uint32_t w = shuffle_word(words[q >> 1], kind, lut) >> ((q & 1) * 16);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) x[i] = lv[(w >> i) & 1u];
-  } else if (bits == 4) {
-    const uint32_t w0 = shuffle_word(words[2 * q], kind, lut);
-    const uint32_t w1 = shuffle_word(words[2 * q + 1], kind, lut);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      x[i] = lv[(w0 >> (4 * i)) & 15u];
-      x[8 + i] = lv[(w1 >> (4 * i)) & 15u];
-    }
-  } else {
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const uint32_t w = shuffle_word(words[4 * q + b], kind, lut);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) x[4 * b + i] = lv[(w >> (8 * i)) & 255u];
-    }
-  }
-  if (lsb) {
-#pragma unroll
-    for (int i = 1; i < 16; i += 2) x[i] = -x[i];
-  }
+// Applies the stations' 32-bit shuffles (src/utils.rs:159-171) in place to the
+// staged words of a slot: [FPC frames of station 1][FPC frames of station 2].
+__device__ __forceinline__ void preshuffle_slot(uint32_t* w1, uint32_t n1, int kind1,
+                                                const uint32_t* lut1, uint32_t* w2, uint32_t n2,
+                                                int kind2, const uint32_t* lut2, int tid,
+                                                int nthreads) {
+  if (kind1 != SH_IDENTITY)
+    for (uint32_t i = tid; i < n1; i += nthreads) w1[i] = shuffle_word(w1[i], kind1, lut1);
+  if (kind2 != SH_IDENTITY)
+    for (uint32_t i = tid; i < n2; i += nthreads) w2[i] = shuffle_word(w2[i], kind2, lut2);
 }
 
 // Bounded mbarrier helpers (cp.async.bulk staging).

@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(M / 16, 1) cfft_kernel(float2* __restrict__ y,
     first_pass<M>(x1, x2, 0, 0, bufA, t);
     float2* Z = fft_rest<M>(bufA, bufB, t, tw);
     __syncthreads();
-    for (int i = t; i < M; i += T1) row[i] = Z[cpad(i)];
+    for (int i = t; i < M; i += T1) row[i] = Z[i];
     __syncthreads();
   }
 }

@@ -154,41 +154,29 @@ phased_kernel(const PhasedParams p) {
       atomicOr(flag, 1);
       atomicOr(p.err, ERR_WAIT_TIMEOUT);
     }
-    const uint8_t* st = stage + slot * L.stage_stride;
+    uint8_t* st = stage + slot * L.stage_stride;
+    uint32_t* w1 = reinterpret_cast<uint32_t*>(st + kRaw1);
+    uint32_t* w2 = reinterpret_cast<uint32_t*>(st + kRaw1 + FPC * bpf1);
+    preshuffle_slot(w1, FPC * bpf1 / 4, p.st[0].shkind, lut, w2, FPC * bpf2 / 4, p.st[1].shkind,
+                    lut + 1024, tid, T);
     if (t == 0 && valid) finfo[g] = reinterpret_cast<const FrameInfo*>(st)[g];
-    float* x1 = reinterpret_cast<float*>(bufB) + g * 2 * Geom<N>::FSTRIDE;
-    float* x2 = x1 + Geom<N>::FSTRIDE;
-    {
-      float xs[16];
-      if (valid) {
-        decode16(reinterpret_cast<const uint32_t*>(st + kRaw1 + g * bpf1), p.st[0].bits,
-                 p.st[0].shkind, lut, lv, p.st[0].lsb, t, xs);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 16; ++i) xs[i] = 0.f;
-      }
-#pragma unroll
-      for (int i = 0; i < 16; ++i) x1[fpad(16 * t + i)] = xs[i];
-      if (valid) {
-        decode16(reinterpret_cast<const uint32_t*>(st + kRaw1 + FPC * bpf1 + g * bpf2),
-                 p.st[1].bits, p.st[1].shkind, lut + 1024, lv + 256, p.st[1].lsb, t, xs);
-      }
-#pragma unroll
-      for (int i = 0; i < 16; ++i) x2[fpad(16 * t + i)] = xs[i];
-    }
     __syncthreads();
     if (*flag) break;
+    const int s1 = valid ? finfo[g].s1 : 0;
+    const int s2 = valid ? finfo[g].s2 : 0;
+    const PackedStation pa{w1 + g * (bpf1 / 4), lv, (uint32_t)p.st[0].bits,
+                           (1u << p.st[0].bits) - 1u, p.st[0].lsb ? 1 : 0, s1};
+    const PackedStation pb{w2 + g * (bpf2 / 4), lv + 256, (uint32_t)p.st[1].bits,
+                           (1u << p.st[1].bits) - 1u, p.st[1].lsb ? 1 : 0, s2};
+
+    float2* za = bufA + g * Geom<N>::CSTRIDE;
+    float2* zb = bufB + g * Geom<N>::CSTRIDE;
+    first_pass_packed<N>(pa, pb, za, t);
+    float2* Z0 = fft_rest<N>(za, zb, t, tw);
     if (tid == 0 && it + kStages < it1) {
       fence_proxy_async();
       issue(it + kStages);
     }
-    const int s1 = valid ? finfo[g].s1 : 0;
-    const int s2 = valid ? finfo[g].s2 : 0;
-
-    float2* za = bufA + g * Geom<N>::CSTRIDE;
-    float2* zb = bufB + g * Geom<N>::CSTRIDE;
-    first_pass<N>(x1, x2, s1, s2, za, t);
-    float2* Z0 = fft_rest<N>(za, zb, t, tw);
     const bool fin_b = Z0 != za;
     __syncthreads();
 
@@ -204,7 +192,7 @@ phased_kernel(const PhasedParams p) {
       // spectrum of station s at its own bin k: unscaled, rotated by the
       // station's fractional delay, Nyquist imaginary part zeroed, times fr_lo
       auto station_bin = [&](int s, int k) -> float2 {
-        const float2 a = Z[cpad(k)], b = Z[cpad((N - k) & (N - 1))];
+        const float2 a = Z[k], b = Z[(N - k) & (N - 1)];
         float2 v = s == 0 ? make_float2(u1 * (a.x + b.x), u1 * (a.y - b.y))
                           : make_float2(u2 * (a.y + b.y), u2 * (b.x - a.x));
         float sn, cs;
@@ -266,7 +254,7 @@ phased_kernel(const PhasedParams p) {
           uint32_t word = 0;
           for (uint32_t i = 0; i < spw; ++i) {
             const uint32_t n = w * spw + i;
-            float x = Y[cpad((int)n)].x * inv_n;
+            float x = Y[n].x * inv_n;
             if (p.out_lsb && (n & 1u)) x = -x;
             word |= (nearest_level(x, ql, (int)p.nqlevels, p.qmonotonic) & qmask)
                     << (i * p.bits_out);
