@@ -198,6 +198,9 @@ struct Geom {
 
 // Per-thread twiddle bases (frame invariant): pass p (1 <= p < P16) uses
 // exp(-2 pi i (t mod 16^p) / 16^(p+1)); the trailing pass uses exp(-2 pi i t / N).
+// A shared-memory table of the powers would trade the 14 complex products of
+// a power chain for 15 8-byte shared loads, and the shared-memory pipe, not
+// the FMA pipe, is the tighter resource of these kernels.
 template <int N>
 struct Twiddles {
   float2 w[Geom<N>::NPASS];
@@ -383,6 +386,51 @@ __device__ __forceinline__ float packed_sample(const PackedStation& p, int m) {
   return __int_as_float(__float_as_int(v) ^ (int)((uint32_t)(m & p.lsb) << 31));
 }
 
+// The 16 first-pass inputs of one station, x[t + r*T1 - shift] for r < 16,
+// decoded from the packed words.  Since T1 is a multiple of the samples per
+// word, the bit position and the odd/even sign of a thread's 16 samples are
+// constant and the word offsets step by a compile-time stride.
+template <int N, int BITS, bool IMAG>
+__device__ __forceinline__ void station_inputs(const PackedStation& p, float2 (&v)[16], int t) {
+  constexpr int T1 = N / 16;
+  constexpr int SPW = 32 / BITS;                 // samples per word
+  constexpr int LOG2_SPW = BITS == 1 ? 5 : (BITS == 2 ? 4 : (BITS == 4 ? 3 : 2));
+  constexpr int WSTEP = T1 / SPW;                // word stride between r and r+1
+  constexpr uint32_t MASK = (1u << BITS) - 1u;
+  static_assert(T1 % SPW == 0, "frame stride is a whole number of words");
+  const int m0 = t - p.shift;
+  const uint32_t bitpos = (uint32_t)(m0 & (SPW - 1)) * BITS;
+  const uint32_t sign = (uint32_t)(m0 & p.lsb) << 31;  // odd samples of LSB input are negated
+  const int w0 = m0 >> LOG2_SPW;                 // floor division (m0 may be negative)
+  if (p.shift == 0) {
+    const uint32_t* w = p.words + w0;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const float x = __uint_as_float(__float_as_uint(p.lv[(w[r * WSTEP] >> bitpos) & MASK]) ^ sign);
+      if (IMAG) v[r].y = x; else v[r].x = x;
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m = m0 + r * T1;
+      const bool in = (unsigned)m < (unsigned)N;
+      const uint32_t w = p.words[in ? w0 + r * WSTEP : 0];
+      const float x = __uint_as_float(__float_as_uint(p.lv[(w >> bitpos) & MASK]) ^ sign);
+      if (IMAG) v[r].y = in ? x : 0.0f; else v[r].x = in ? x : 0.0f;
+    }
+  }
+}
+
+template <int N, bool IMAG>
+__device__ __forceinline__ void station_inputs_any(const PackedStation& p, float2 (&v)[16], int t) {
+  switch (p.bits) {
+    case 1: station_inputs<N, 1, IMAG>(p, v, t); break;
+    case 2: station_inputs<N, 2, IMAG>(p, v, t); break;
+    case 4: station_inputs<N, 4, IMAG>(p, v, t); break;
+    default: station_inputs<N, 8, IMAG>(p, v, t); break;
+  }
+}
+
 // First pass fused with the decode: z[n] = x1[n - s1] + i x2[n - s2] read
 // straight from the packed words with the integer shift and zero fill
 // (src/utils.rs:126-145).  Lanes take consecutive n, so each word load is a
@@ -390,32 +438,9 @@ __device__ __forceinline__ float packed_sample(const PackedStation& p, int m) {
 template <int N>
 __device__ __forceinline__ void first_pass_packed(const PackedStation& a, const PackedStation& b,
                                                   float2* __restrict__ out, int t) {
-  constexpr int T1 = N / 16;
   float2 v[16];
-  if (a.shift == 0) {
-#pragma unroll
-    for (int r = 0; r < 16; ++r) v[r].x = packed_sample(a, t + r * T1);
-  } else {
-#pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const int m = t + r * T1 - a.shift;
-      const bool in = (unsigned)m < (unsigned)N;
-      const float x = packed_sample(a, in ? m : 0);
-      v[r].x = in ? x : 0.0f;
-    }
-  }
-  if (b.shift == 0) {
-#pragma unroll
-    for (int r = 0; r < 16; ++r) v[r].y = packed_sample(b, t + r * T1);
-  } else {
-#pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const int m = t + r * T1 - b.shift;
-      const bool in = (unsigned)m < (unsigned)N;
-      const float x = packed_sample(b, in ? m : 0);
-      v[r].y = in ? x : 0.0f;
-    }
-  }
+  station_inputs_any<N, false>(a, v, t);
+  station_inputs_any<N, true>(b, v, t);
   dft16(v);
   float2* dst = out + 17 * t;  // cpad(16 t + r) = 17 t + r
 #pragma unroll
@@ -423,26 +448,31 @@ __device__ __forceinline__ void first_pass_packed(const PackedStation& a, const 
 }
 
 // Runs passes 2..NPASS; `a` holds the first pass output, returns the buffer
-// with the natural-order spectrum Z[0..N).
-template <int N>
+// with the natural-order spectrum Z[0..N).  With NO_TRAIL the trailing radix-2
+// pass (RL == 2) is left to the consumer: the returned buffer then holds its
+// input Y unpadded, and Z[k] = Y[k] + W_N^k Y[k + N/2],
+// Z[k + N/2] = Y[k] - W_N^k Y[k + N/2] for k < N/2.
+template <int N, bool NO_TRAIL = false>
 __device__ __forceinline__ float2* fft_rest(float2* a, float2* b, int t, const Twiddles<N>& tw) {
   constexpr int P16 = Geom<N>::P16;
   constexpr int RL = Geom<N>::RL;
+  static_assert(!NO_TRAIL || RL == 2, "only a trailing radix-2 pass is left out");
+  constexpr bool TRAIL = RL > 1 && !NO_TRAIL;
   float2* in = a;
   float2* out = b;
-  // the returned spectrum is unpadded: Z[k] at index k
+  // the returned buffer is unpadded
   static_assert(P16 >= 2, "at least two radix-16 passes");
   {
     __syncthreads();
-    stockham_pass<N, 16, 16, (P16 >= 3 || RL > 1)>(in, out, t, tw.w[1]);
+    stockham_pass<N, 16, 16, (P16 >= 3 || TRAIL)>(in, out, t, tw.w[1]);
     float2* x = in; in = out; out = x;
   }
   if constexpr (P16 >= 3) {
     __syncthreads();
-    stockham_pass<N, 16, 256, (RL > 1)>(in, out, t, tw.w[2]);
+    stockham_pass<N, 16, 256, TRAIL>(in, out, t, tw.w[2]);
     float2* x = in; in = out; out = x;
   }
-  if constexpr (RL > 1) {
+  if constexpr (TRAIL) {
     constexpr int NS = 1 << (4 * P16);
     __syncthreads();
     stockham_pass<N, RL, NS, false>(in, out, t, tw.w[P16]);
