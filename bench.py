@@ -430,7 +430,7 @@ def main():
         "peak": fp32_peak, "unit": "TFLOP/s",
         "frac": flops_launch / (launch_ms * 1e-3) / 1e12 / fp32_peak,
         "traffic": None if tpf is None else tpf * NFS,
-        "kernel": "corr_kernel<8192,1,0>", "launch_ms": launch_ms,
+        "kernel": "corr_fold_kernel (FFT 8192)", "launch_ms": launch_ms,
         "algorithmic_flops_per_launch": flops_launch,
         "peak_source": "live FMA probe of this GPU (fxc_probe_fp32_peak)",
         "hbm": {"achieved": bytes_launch / (launch_ms * 1e-3) / 1e9, "peak": hbm_peak,

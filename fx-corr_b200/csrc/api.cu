@@ -189,6 +189,7 @@ void station_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2, Sta
     st[k].lsb = k ? s->cfg.lsb2 : s->cfg.lsb1;
     st[k].shkind = s->shkind[k];
     st[k].scale = s->scale[k];
+    std::memcpy(st[k].perm, k ? s->cfg.shuffle2 : s->cfg.shuffle1, 32);
   }
 }
 

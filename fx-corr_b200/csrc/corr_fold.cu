@@ -1,0 +1,394 @@
+// corr_fold.cu — the FFT-8192 correlation kernel (the full-rate path).
+//
+// Same contract as corr_kernel<8192, 1, MODE_CORR> (src/main.rs:2491-2568
+// per frame pair, partials reduced by reduce_partials_kernel), arranged to
+// spend as few shared-memory wavefronts and barriers per frame pair as the
+// data flow allows:
+//   * decode straight from the staged .raw words: each thread's 16 samples of
+//     a station sit at one bit position of 16 words (the frame stride N/16 is
+//     a whole number of words), so a sample costs a word load, a rotate and a
+//     masked merge into a byte offset of the level table.  A shuffle that
+//     splits a 2-bit sample's bits takes two rotates; 1- and 2-bit shuffles
+//     never rewrite the staged words.  The LSB flip (odd samples negated,
+//     src/utils.rs:196-197) is a per-thread constant because N/16 is even: it
+//     selects a negated copy of the level table;
+//   * the station whose bin grid the products are indexed on (the primary:
+//     station 1 for grid 0, station 2 for grid 1) is the real part of the
+//     shared complex FFT, so the accumulation is free of grid selects;
+//   * the trailing radix-2 pass is folded into the accumulation: a thread
+//     reads Y[j], Y[j + N/2], Y[N/2 - j], Y[N - j] of the last radix-16 pass
+//     and forms Z at j, N/2 - j, N/2 + j, N - j, i.e. both stations' spectra
+//     at the bin pair (j, N/2 - j); the secondary spectrum goes through the
+//     free ping-pong buffer to the thread that owns the band-shifted bin;
+//   * four barriers per frame pair: after the first pass, after each
+//     radix-16 pass, and between the two halves of the accumulation.  The
+//     frame record is double-buffered so no barrier closes an iteration.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fxc_device.cuh"
+#include "fxc_kernels.h"
+
+namespace fxc {
+namespace {
+
+constexpr int kN = 8192;
+constexpr int kT = kN / 16;          // threads per CTA, one frame pair per iteration
+constexpr int kH = kN / 2 + 1;
+constexpr int kUnits = kN / 4 / kT;  // bin pairs per thread
+static_assert(kUnits == 4, "the twiddle switch below covers W_16^0..3");
+constexpr int kSlots = 2 * kUnits + 1;  // accumulator rows (bin N/4 by thread 0)
+
+// Shared memory: level tables first, at a fixed address, so that the decode's
+// table loads take an immediate base.
+//   [0, 4096)      levels: primary, primary negated, secondary, secondary negated (256 f32 each)
+//   [4096, 4352)   rotate amounts: [2 stations][32 sample slots] u32
+//   [4352, 4448)   frame records, double-buffered
+//   [4448, 4464)   mbarriers; [4464, 4480) error flag
+//   [4608, 12800)  byte LUTs of 4- and 8-bit generic shuffles
+//   then the two ping-pong buffers and the staging slots
+struct FoldLayout {
+  uint32_t off_a, off_b, off_stage, stage_stride, total;
+};
+constexpr uint32_t kOffPos = 4096, kOffFi = 4352, kOffBar = 4448, kOffFlag = 4464, kOffLut = 4608;
+constexpr uint32_t kOffA = kOffLut + 8192;
+
+__host__ __device__ inline FoldLayout fold_layout(uint32_t raw_bytes) {
+  FoldLayout L;
+  L.off_a = kOffA;
+  L.off_b = L.off_a + Geom<kN>::CSTRIDE * (uint32_t)sizeof(float2);
+  L.off_stage = L.off_b + Geom<kN>::CSTRIDE * (uint32_t)sizeof(float2);
+  L.stage_stride = (kFiBytes + raw_bytes + 127u) & ~127u;
+  L.total = L.off_stage + kStages * L.stage_stride;
+  return L;
+}
+static_assert(kOffA % 128 == 0 && kOffFi % 16 == 0 && kOffBar % 8 == 0, "alignment");
+
+// 16 inputs of one station: x[t + r N/16 - shift] (zero outside the frame),
+// r < 16, as a byte offset of the level table: rotate the word so that the
+// sample's bits land at byte-offset bits 2.., mask, merge the table base
+// (which also selects the negated copy for odd samples of an LSB station).
+template <int BITS, bool IMAG, bool SPLIT>
+__device__ __forceinline__ void fold_inputs(const uint32_t* __restrict__ words, const uint8_t* lvbase,
+                                            int shift, uint32_t rots, uint32_t tbase,
+                                            float2 (&v)[16], int t) {
+  constexpr int T1 = kN / 16;
+  constexpr int SPW = 32 / BITS;
+  constexpr int LOG2_SPW = BITS == 1 ? 5 : (BITS == 2 ? 4 : (BITS == 4 ? 3 : 2));
+  constexpr int WSTEP = T1 / SPW;
+  constexpr uint32_t OMASK = ((1u << BITS) - 1u) << 2;
+  static_assert(T1 % SPW == 0, "frame stride is a whole number of words");
+  const int m0 = t - shift;
+  const int w0 = m0 >> LOG2_SPW;  // floor division
+  const uint32_t r0 = rots & 31u, r1 = (rots >> 8) & 31u;
+  auto level = [&](uint32_t w) -> float {
+    uint32_t off;
+    if constexpr (SPLIT) {
+      off = (__funnelshift_r(w, w, r0) & 4u) | tbase;
+      off |= __funnelshift_r(w, w, r1) & 8u;
+    } else {
+      off = (__funnelshift_r(w, w, r0) & OMASK) | tbase;
+    }
+    return *reinterpret_cast<const float*>(lvbase + off);
+  };
+  if (shift == 0) {
+    const uint32_t* w = words + w0;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const float x = level(w[r * WSTEP]);
+      if (IMAG) v[r].y = x; else v[r].x = x;
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m = m0 + r * T1;
+      const bool in = (unsigned)m < (unsigned)kN;
+      const float x = level(words[in ? w0 + r * WSTEP : 0]);
+      if (IMAG) v[r].y = in ? x : 0.0f; else v[r].x = in ? x : 0.0f;
+    }
+  }
+}
+
+template <bool IMAG>
+__device__ __forceinline__ void fold_station(int bits, bool split, const uint32_t* words,
+                                             const uint8_t* lvbase, int shift, uint32_t rots,
+                                             uint32_t tbase, float2 (&v)[16], int t) {
+  switch (bits) {
+    case 1: fold_inputs<1, IMAG, false>(words, lvbase, shift, rots, tbase, v, t); break;
+    case 2:
+      if (split) fold_inputs<2, IMAG, true>(words, lvbase, shift, rots, tbase, v, t);
+      else fold_inputs<2, IMAG, false>(words, lvbase, shift, rots, tbase, v, t);
+      break;
+    case 4: fold_inputs<4, IMAG, false>(words, lvbase, shift, rots, tbase, v, t); break;
+    default: fold_inputs<8, IMAG, false>(words, lvbase, shift, rots, tbase, v, t); break;
+  }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const FoldLayout L = fold_layout(p.stage_bytes);
+  float* lv = reinterpret_cast<float*>(smem);
+  uint32_t* pos = reinterpret_cast<uint32_t*>(smem + kOffPos);
+  FrameInfo* finfo = reinterpret_cast<FrameInfo*>(smem + kOffFi);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
+  int* flag = reinterpret_cast<int*>(smem + kOffFlag);
+  uint32_t* lut = reinterpret_cast<uint32_t*>(smem + kOffLut);
+  float2* bufA = reinterpret_cast<float2*>(smem + L.off_a);
+  float2* bufB = reinterpret_cast<float2*>(smem + L.off_b);
+  uint8_t* stage = smem + L.off_stage;
+  const int tid = threadIdx.x;
+
+  // primary station (real part of the FFT, products indexed on its bins) first
+  const bool g0 = p.grid == 0;
+  const StationParams& sp = p.st[g0 ? 0 : 1];
+  const StationParams& ss = p.st[g0 ? 1 : 0];
+  const int bitsP = sp.bits, bitsS = ss.bits;
+  // 4- and 8-bit stations with a non-identity shuffle are rewritten in place
+  // (byte LUTs); 1- and 2-bit stations are decoded from the raw words
+  const bool preP = bitsP > 2 && sp.shkind != SH_IDENTITY;
+  const bool preS = bitsS > 2 && ss.shkind != SH_IDENTITY;
+
+  // ---- constant tables
+  for (int i = tid; i < 1024; i += kT) {
+    const StationParams& q = (i < 512) ? sp : ss;
+    const float x = q.levels[i & 255] * q.scale;
+    lv[i] = (i & 256) ? -x : x;
+  }
+  for (int i = tid; i < 64; i += kT) {
+    // rotate amounts of sample slot c: bit j of the sample is word bit p_j
+    const int k = i >> 5, c = i & 31;
+    const StationParams& q = k ? ss : sp;
+    const int b = q.bits;
+    const bool natural = (k ? preS : preP) || q.shkind == SH_IDENTITY;
+    uint32_t r = 0;
+    if (c * b < 32) {
+      const int p0 = natural ? c * b : q.perm[c * b];
+      const int p1 = b >= 2 ? (natural ? c * b + 1 : q.perm[c * b + 1]) : 0;
+      r = (uint32_t)((p0 - 2) & 31) | ((uint32_t)((p1 - 3) & 31) << 8);
+    }
+    pos[i] = r;
+  }
+  for (int k = 0; k < 2; ++k) {
+    const StationParams& q = k ? ss : sp;
+    if ((k ? preS : preP) && q.shkind == SH_GENERIC)
+      for (int i = tid; i < 1024; i += kT) lut[k * 1024 + i] = q.shlut[i];
+  }
+  // a 2-bit shuffle keeps every sample's two bits adjacent and in order, or not
+  auto split2 = [](const StationParams& q) {
+    if (q.bits != 2 || q.shkind == SH_IDENTITY) return false;
+    for (int c = 0; c < 16; ++c)
+      if (q.perm[2 * c + 1] != q.perm[2 * c] + 1 || (q.perm[2 * c] & 1)) return true;
+    return false;
+  };
+  const bool splitP = split2(sp), splitS = split2(ss);
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    *flag = 0;
+    fence_proxy_async();
+  }
+  Twiddles<kN> tw;
+  tw.init(tid);
+
+  const uint64_t iters = p.nf;
+  const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
+  const uint64_t it1 = ((blockIdx.x + 1) * iters) / gridDim.x;
+  const uint32_t bpfP = sp.bpf, bpfS = ss.bpf;
+  const uint8_t* rawP = sp.raw;
+  const uint8_t* rawS = ss.raw;
+
+  // slot: [FrameInfo][primary frame][secondary frame]
+  auto issue = [&](uint64_t it) {
+    const int slot = (int)((it - it0) % kStages);
+    uint8_t* dst = stage + slot * L.stage_stride;
+    mbar_expect_tx(&bars[slot], kFiBytes + bpfP + bpfS);
+    bulk_g2s(dst, p.finfo + it, kFiBytes, &bars[slot]);
+    bulk_g2s(dst + kFiBytes, rawP + it * bpfP, bpfP, &bars[slot]);
+    bulk_g2s(dst + kFiBytes + bpfP, rawS + it * bpfS, bpfS, &bars[slot]);
+  };
+  __syncthreads();
+  if (tid == 0)
+    for (uint64_t it = it0; it < it1 && it < it0 + kStages; ++it) issue(it);
+
+  // acc[2i]: bin tid + T i, acc[2i+1]: bin N/2 - tid - T i, acc[2 kUnits]: bin N/4 (tid 0).
+  // Columns: primary ACF, secondary ACF (at the primary bin), XCF re, im.
+  float acc[kSlots][4];
+#pragma unroll
+  for (int i = 0; i < kSlots; ++i)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[i][v] = 0.f;
+  const int a1s = p.a1s, a1e = p.a1e, a2s = p.a2s;
+  const int ov = a1e - a1s;
+  const int sb = a2s - a1s;
+  const int ovs = g0 ? a1s : a2s;   // overlap on the primary grid: [ovs, ovs + ov)
+  const int qoff = g0 ? sb : -sb;   // secondary bin = primary bin + qoff
+  const bool want_acf = (p.products & 1u) != 0;
+  const bool want_xcf = (p.products & 2u) != 0;
+  const bool ov_only = (p.products & 16u) != 0;
+  const float xconj = g0 ? 1.0f : -1.0f;  // XCF = S1 conj(S2): conj(P conj(S)) for grid 1
+  const int lsbP = sp.lsb ? 1 : 0, lsbS = ss.lsb ? 1 : 0;
+  bool first_flush = true;
+  uint32_t since_flush = 0;
+  double* part = p.partials + (size_t)blockIdx.x * 4 * kH;
+  const int colP = g0 ? 0 : 1, colS = g0 ? 1 : 0;  // output columns of the two ACFs
+
+  auto flush = [&]() {
+#pragma unroll
+    for (int i = 0; i < kSlots; ++i) {
+      if (i == kSlots - 1 && tid != 0) continue;
+      const int j = tid + kT * (i >> 1);
+      const int bin = (i == kSlots - 1) ? kN / 4 : ((i & 1) ? kN / 2 - j : j);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int col = v == 0 ? colP : (v == 1 ? colS : v);
+        double* q = part + (size_t)col * kH + bin;
+        *q = (first_flush ? 0.0 : *q) + (double)acc[i][v];
+        acc[i][v] = 0.f;
+      }
+    }
+    first_flush = false;
+    since_flush = 0;
+  };
+
+  for (uint64_t it = it0; it < it1; ++it) {
+    const int slot = (int)((it - it0) % kStages);
+    const uint32_t parity = (uint32_t)(((it - it0) / kStages) & 1u);
+    const int fb = (int)((it - it0) & 1u);
+    if (!mbar_wait(&bars[slot], parity, kWaitPolls)) {
+      atomicOr(flag, 1);
+      atomicOr(p.err, ERR_WAIT_TIMEOUT);
+    }
+    uint8_t* st = stage + slot * L.stage_stride;
+    uint32_t* wP = reinterpret_cast<uint32_t*>(st + kFiBytes);
+    uint32_t* wS = reinterpret_cast<uint32_t*>(st + kFiBytes + bpfP);
+    const FrameInfo* fs = reinterpret_cast<const FrameInfo*>(st);
+    const int sP = g0 ? fs->s1 : fs->s2;
+    const int sS = g0 ? fs->s2 : fs->s1;
+    if (tid == 0) finfo[fb] = *fs;
+    if (preP || preS) {  // CTA-uniform
+      preshuffle_slot(wP, bpfP / 4, preP ? sp.shkind : SH_IDENTITY, lut, wS, bpfS / 4,
+                      preS ? ss.shkind : SH_IDENTITY, lut + 1024, tid, kT);
+      __syncthreads();
+    }
+
+    // ---- decode + first radix-16 pass into bufA
+    {
+      float2 v[16];
+      const int mP = tid - sP, mS = tid - sS;
+      const int cP = mP & ((32 / bitsP) - 1), cS = mS & ((32 / bitsS) - 1);
+      const uint32_t tbP = (uint32_t)((mP & lsbP) << 10);
+      const uint32_t tbS = 2048u + (uint32_t)((mS & lsbS) << 10);
+      fold_station<false>(bitsP, splitP, wP, smem, sP, pos[cP], tbP, v, tid);
+      fold_station<true>(bitsS, splitS, wS, smem, sS, pos[32 + cS], tbS, v, tid);
+      dft16(v);
+      float2* dst = bufA + 17 * tid;  // cpad(16 t + r) = 17 t + r
+#pragma unroll
+      for (int r = 0; r < 16; ++r) dst[r] = v[out_pos<16>(r)];
+    }
+    const float2* Y = fft_rest<kN, true>(bufA, bufB, tid, tw);
+    // fft_rest opened with a barrier after the first pass: the staging slot
+    // is consumed, refill it with iteration it + kStages
+    if (tid == 0 && it + kStages < it1) {
+      fence_proxy_async();
+      issue(it + kStages);
+    }
+    float2* Q = (Y == bufA) ? bufB : bufA;  // free buffer: secondary spectrum by bin
+    __syncthreads();
+    if (*flag) break;  // no thread writes the flag before the next barrier
+
+    // ---- trailing radix-2 pass + two-for-one split (x2) at the bin pairs
+    const FrameInfo& F = finfo[fb];
+    float sn, cs;
+    const int a_gs = ovs;
+    const float2 mix = F.fr_mix;
+    __sincosf(fmaf((float)(tid - a_gs), F.dphi, F.phi0), &sn, &cs);
+    float2 rup = cmul(mix, make_float2(cs, sn));
+    __sincosf(fmaf((float)(kN / 2 - tid - a_gs), F.dphi, F.phi0), &sn, &cs);
+    float2 rdn = cmul(mix, make_float2(cs, sn));
+    __sincosf((float)kT * F.dphi, &sn, &cs);
+    const float2 rstep = make_float2(cs, sn);
+    float2 rq = make_float2(0.f, 0.f);
+    if (tid == 0) {
+      __sincosf(fmaf((float)(kN / 4 - a_gs), F.dphi, F.phi0), &sn, &cs);
+      rq = cmul(mix, make_float2(cs, sn));
+    }
+
+    float2 prim[2 * kUnits];
+#pragma unroll
+    for (int i = 0; i < kUnits; ++i) {
+      const int j = tid + kT * i;
+      float2 wj;  // W_N^j = W_N^tid W_16^i
+      switch (i) {  // compile-time after unrolling
+        case 0: wj = tw.w[Geom<kN>::P16]; break;
+        case 1: wj = mul_w16<1>(tw.w[Geom<kN>::P16]); break;
+        case 2: wj = mul_w16<2>(tw.w[Geom<kN>::P16]); break;
+        default: wj = mul_w16<3>(tw.w[Geom<kN>::P16]); break;
+      }
+      const float2 a = Y[j], b = Y[j + kN / 2], c = Y[kN / 2 - j], d = Y[(kN - j) & (kN - 1)];
+      const float2 wb = cmul(wj, b), wd = cmulc(d, wj);  // W^j b, conj(W^j) d
+      const float2 zj = cadd(a, wb), zjh = csub(a, wb);  // Z[j], Z[j + N/2]
+      const float2 zmn = cadd(c, wd);                    // Z[N - j]
+      // Z[N/2 - j]; for j = 0 that is Z[N/2] = Y[0] - Y[N/2]
+      const float2 zm = j == 0 ? zjh : csub(c, wd);
+      // primary = real part: P[k] = (Z[k] + conj Z[N-k]), S[k] = -i (Z[k] - conj Z[N-k])
+      prim[2 * i] = make_float2(zj.x + zmn.x, zj.y - zmn.y);
+      Q[j] = make_float2(zj.y + zmn.y, zmn.x - zj.x);
+      prim[2 * i + 1] = make_float2(zm.x + zjh.x, zm.y - zjh.y);
+      Q[kN / 2 - j] = make_float2(zm.y + zjh.y, zjh.x - zm.x);
+    }
+    float2 prim_q = make_float2(0.f, 0.f);
+    if (tid == 0) {  // bin N/4: Z[N/4] = Y[N/4] - i Y[3N/4], Z[3N/4] = Y[N/4] + i Y[3N/4]
+      const float2 a = Y[kN / 4], b = Y[3 * kN / 4];
+      const float2 zq = make_float2(a.x + b.y, a.y - b.x), zq3 = make_float2(a.x - b.y, a.y + b.x);
+      prim_q = make_float2(zq.x + zq3.x, zq.y - zq3.y);
+      Q[kN / 4] = make_float2(zq.y + zq3.y, zq3.x - zq.x);
+    }
+    __syncthreads();
+
+    // ---- accumulation (constant indices into acc[][]: a runtime index
+    // would move it to local memory)
+    auto bin_acc = [&](int bin, float2 pv, float2 r, float* a) {
+      const bool inov = (unsigned)(bin - ovs) < (unsigned)ov;
+      const float2 q = Q[inov ? bin + qoff : bin];
+      if (want_acf && (!ov_only || inov)) a[0] = fmaf(pv.x, pv.x, fmaf(pv.y, pv.y, a[0]));
+      if (inov) {
+        if (want_acf) a[1] = fmaf(q.x, q.x, fmaf(q.y, q.y, a[1]));
+        if (want_xcf) {
+          float2 x = cmulc(pv, q);
+          x.y *= xconj;
+          a[2] = fmaf(x.x, r.x, fmaf(-x.y, r.y, a[2]));
+          a[3] = fmaf(x.x, r.y, fmaf(x.y, r.x, a[3]));
+        }
+      }
+    };
+#pragma unroll
+    for (int i = 0; i < kUnits; ++i) {
+      const int j = tid + kT * i;
+      bin_acc(j, prim[2 * i], rup, acc[2 * i]);
+      bin_acc(kN / 2 - j, prim[2 * i + 1], rdn, acc[2 * i + 1]);
+      rup = cmul(rup, rstep);
+      rdn = cmulc(rdn, rstep);
+    }
+    if (tid == 0) bin_acc(kN / 4, prim_q, rq, acc[kSlots - 1]);
+    if (++since_flush >= p.flush_every) flush();
+  }
+  if (since_flush > 0 || first_flush) flush();
+  // never leave a bulk copy in flight into a finished CTA's shared memory
+  if (tid == 0 && *flag) {
+    for (int s = 0; s < kStages; ++s) mbar_wait(&bars[s], 0, kWaitPolls);
+  }
+}
+
+uint32_t fold_smem_bytes(uint32_t stage_bytes) { return fold_layout(stage_bytes).total; }
+
+cudaError_t launch_corr_fold(const CorrParams& p, int grid, cudaStream_t stream) {
+  const uint32_t smem = fold_smem_bytes(p.stage_bytes);
+  cudaError_t e = cudaFuncSetAttribute(corr_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  corr_fold_kernel<<<grid, kT, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace fxc

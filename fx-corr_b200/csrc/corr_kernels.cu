@@ -35,19 +35,6 @@ corr_kernel(const CorrParams p) {
   constexpr int H = N / 2 + 1;
   constexpr int BPT = (N / 2) / T;
   static_assert(BPT * T == N / 2 && BPT >= 2, "bins per thread");
-  // N = 8192: the trailing radix-2 pass is folded into the accumulation
-  // (accumulate_fused below); thread tid then owns bins tid + T i and
-  // N/2 - tid - T i (i < BPT/2), tid 0 also bin N/4.
-  constexpr bool kFoldTrail = MODE == MODE_CORR && Geom<N>::RL == 2 && FPC == 1;
-  auto acc_bin = [&](int i, int tid_) -> int {
-    if (i == BPT) return kFoldTrail ? N / 4 : N / 2;
-    if constexpr (kFoldTrail) {
-      const int j = tid_ + T * (i >> 1);
-      return (i & 1) ? N / 2 - j : j;
-    } else {
-      return tid_ + T * i;
-    }
-  };
 
   extern __shared__ __align__(128) uint8_t smem[];
   const SmemLayout L = smem_layout<N, FPC>(p.stage_bytes);
@@ -119,8 +106,8 @@ corr_kernel(const CorrParams p) {
   auto flush = [&]() {
 #pragma unroll
     for (int i = 0; i <= BPT; ++i) {
+      const int bin = (i < BPT) ? (tid + T * i) : N / 2;
       if (i == BPT && tid != 0) continue;
-      const int bin = acc_bin(i, tid);
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
         double* q = part + (size_t)v * H + bin;
@@ -180,7 +167,7 @@ corr_kernel(const CorrParams p) {
     float2* za = bufA + g * Geom<N>::CSTRIDE;
     float2* zb = bufB + g * Geom<N>::CSTRIDE;
     first_pass_packed<N>(pa, pb, za, t);
-    float2* Z0 = fft_rest<N, kFoldTrail>(za, zb, t, tw);
+    float2* Z0 = fft_rest<N>(za, zb, t, tw);
     // fft_rest opened with a barrier after the fused first pass: the staging
     // slot is consumed, refill it with iteration it + kStages
     if (tid == 0 && it + kStages < it1) {
@@ -202,100 +189,6 @@ corr_kernel(const CorrParams p) {
           o2[k] = make_float2(u2 * (a.y + b.y), -u2 * (a.x - b.x));
         }
       }
-      __syncthreads();
-      continue;
-    }
-
-    if constexpr (kFoldTrail) {
-      // ---- MODE_CORR, N = 8192: trailing radix-2 pass + accumulation.  With
-      // one frame pair per iteration, `valid` holds for the whole CTA.
-      {
-        const float2* Y = fin_b ? bufB : bufA;
-        float2* Q = fin_b ? bufA : bufB;  // the free buffer: secondary spectrum by bin
-        const FrameInfo& F = finfo[0];
-        const bool g0 = p.grid == 0;
-        const int ovs = g0 ? a1s : a2s;  // overlap of the primary grid: [ovs, ovs + ov)
-        float sn, cs;
-        __sincosf(fmaf((float)(tid - a_gs), F.dphi, F.phi0), &sn, &cs);
-        float2 rup = cmul(F.fr_mix, make_float2(cs, sn));
-        __sincosf(fmaf((float)(N / 2 - tid - a_gs), F.dphi, F.phi0), &sn, &cs);
-        float2 rdn = cmul(F.fr_mix, make_float2(cs, sn));
-        __sincosf((float)T * F.dphi, &sn, &cs);
-        const float2 rstep = make_float2(cs, sn);
-        // two-for-one (x2): S1 from (Z[k], Z[N-k]) = (u, w), S2 likewise
-        auto split = [](float2 u, float2 w, float2& s1, float2& s2) {
-          s1 = make_float2(u.x + w.x, u.y - w.y);
-          s2 = make_float2(u.y + w.y, w.x - u.x);
-        };
-        float2 prim[BPT];  // primary spectrum (x2) of the owned bins, slot order of acc
-#pragma unroll
-        for (int i = 0; i < BPT / 2; ++i) {
-          const int j = tid + T * i;
-          float2 wj;
-          switch (i) {  // W_N^j = W_N^tid W_16^i, compile-time after unrolling
-            case 0: wj = tw.w[Geom<N>::P16]; break;
-            case 1: wj = mul_w16<1>(tw.w[Geom<N>::P16]); break;
-            case 2: wj = mul_w16<2>(tw.w[Geom<N>::P16]); break;
-            default: wj = mul_w16<3>(tw.w[Geom<N>::P16]); break;
-          }
-          const float2 a = Y[j], b = Y[j + N / 2], c = Y[N / 2 - j], d = Y[(N - j) & (N - 1)];
-          const float2 wb = cmul(wj, b), wd = cmulc(d, wj);  // W^j b, conj(W^j) d
-          const float2 zj = cadd(a, wb), zjh = csub(a, wb);  // Z[j], Z[j + N/2]
-          const float2 zm = csub(c, wd), zmn = cadd(c, wd);  // Z[N/2 - j], Z[N - j]
-          float2 s1, s2;
-          split(zj, zmn, s1, s2);  // bin j
-          prim[2 * i] = g0 ? s1 : s2;
-          Q[j] = g0 ? s2 : s1;
-          // bin N/2 - j (j = 0: bin N/2, Z[N/2] = Y[0] - Y[N/2] on both sides)
-          split(j == 0 ? zjh : zm, zjh, s1, s2);
-          prim[2 * i + 1] = g0 ? s1 : s2;
-          Q[N / 2 - j] = g0 ? s2 : s1;
-        }
-        float2 prim_q;  // bin N/4 (tid 0): Z[N/4] = Y[N/4] - i Y[3N/4], Z[3N/4] = Y[N/4] + i Y[3N/4]
-        if (tid == 0) {
-          const float2 a = Y[N / 4], b = Y[3 * N / 4];
-          const float2 zq = make_float2(a.x + b.y, a.y - b.x), zq3 = make_float2(a.x - b.y, a.y + b.x);
-          float2 s1, s2;
-          split(zq, zq3, s1, s2);
-          prim_q = g0 ? s1 : s2;
-          Q[N / 4] = g0 ? s2 : s1;
-        }
-        __syncthreads();
-        const int qoff = g0 ? sb : -sb;  // secondary bin = primary bin + qoff
-        // (constant indices into a[]: a runtime index would move acc[][] to local memory)
-        auto bin_acc = [&](int bin, float2 pv, float2 r, float* a) {
-          const bool inov = bin >= ovs && bin < ovs + ov;
-          if (want_acf && (!ov_only || inov)) {
-            const float e = cnorm2(pv);
-            if (g0) a[0] += e; else a[1] += e;
-          }
-          if (inov) {
-            const float2 q = Q[bin + qoff];
-            if (want_acf) {
-              const float e = cnorm2(q);
-              if (g0) a[1] += e; else a[0] += e;
-            }
-            if (want_xcf) {
-              const float2 x = cmul(g0 ? cmulc(pv, q) : cmulc(q, pv), r);
-              a[2] += x.x;
-              a[3] += x.y;
-            }
-          }
-        };
-#pragma unroll
-        for (int i = 0; i < BPT / 2; ++i) {
-          const int j = tid + T * i;
-          bin_acc(j, prim[2 * i], rup, acc[2 * i]);
-          bin_acc(N / 2 - j, prim[2 * i + 1], rdn, acc[2 * i + 1]);
-          rup = cmul(rup, rstep);
-          rdn = cmulc(rdn, rstep);
-        }
-        if (tid == 0) {
-          __sincosf(fmaf((float)(N / 4 - a_gs), F.dphi, F.phi0), &sn, &cs);
-          bin_acc(N / 4, prim_q, cmul(F.fr_mix, make_float2(cs, sn)), acc[BPT]);
-        }
-      }
-      if (++since_flush >= p.flush_every) flush();
       __syncthreads();
       continue;
     }
@@ -440,7 +333,10 @@ static cudaError_t launch_mode(uint32_t n, const CorrParams& p, int grid, cudaSt
     case 1024: return launch_one<1024, 4, MODE>(p, grid, s);
     case 2048: return launch_one<2048, 2, MODE>(p, grid, s);
     case 4096: return launch_one<4096, 1, MODE>(p, grid, s);
-    case 8192: return launch_one<8192, 1, MODE>(p, grid, s);
+    case 8192:
+      // the FFT-8192 correlation has a kernel of its own (corr_fold.cu)
+      if constexpr (MODE == MODE_CORR) return launch_corr_fold(p, grid, s);
+      else return launch_one<8192, 1, MODE>(p, grid, s);
     default: return cudaErrorInvalidValue;
   }
 }

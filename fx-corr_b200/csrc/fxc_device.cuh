@@ -44,6 +44,7 @@ struct StationParams {
   int32_t shkind;          // 0 identity, 1 pair swap, 2 generic
   float scale;             // power of two equalising the two stations' RMS level
                            // inside the shared complex FFT (exact to undo)
+  uint8_t perm[32];        // the 32-bit shuffle: decoder bit o is word bit perm[o]
 };
 
 enum { SH_IDENTITY = 0, SH_PAIRSWAP = 1, SH_GENERIC = 2 };

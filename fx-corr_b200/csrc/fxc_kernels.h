@@ -58,6 +58,9 @@ struct PhasedParams {
 int corr_frames_per_cta_iter(uint32_t n);
 int corr_ctas_per_sm(uint32_t n);
 cudaError_t launch_corr(uint32_t n, int mode, const CorrParams& p, int grid, cudaStream_t s);
+// FFT-8192 correlation (MODE_CORR), one frame pair per CTA iteration (corr_fold.cu)
+cudaError_t launch_corr_fold(const CorrParams& p, int grid, cudaStream_t s);
+uint32_t fold_smem_bytes(uint32_t stage_bytes);
 cudaError_t launch_reduce(const double* part, int nblk, int h, double m11, double m22, double m12,
                           double* out, cudaStream_t s);
 // FFT lengths above 8192 (N = c * 8192): global-memory four-step path.

@@ -172,6 +172,7 @@ extern "C" fxc_status fxc_sector_run_device_noalloc(const fxc_scan_cfg* cfg,
     p.st[k].lsb = k ? cfg->lsb2 : cfg->lsb1;
     p.st[k].shkind = kind[k];
     p.st[k].scale = scale[k];
+    std::memcpy(p.st[k].perm, k ? cfg->shuffle2 : cfg->shuffle1, 32);
   }
   p.dl = dl;
   p.nf = nf;

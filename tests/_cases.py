@@ -33,6 +33,9 @@ def make_scan(fft=1024, fs=32e6, bits1=2, bits2=2, shuffle="identity", lsb1=Fals
             return list(range(32))
         if kind == "pairswap":
             return [i ^ 1 for i in range(32)]
+        if kind == "sample2":  # whole 2-bit samples reordered, bits kept in order
+            order = np.random.Generator(np.random.PCG64(s)).permutation(16)
+            return [2 * int(order[i >> 1]) + (i & 1) for i in range(32)]
         return oracle.random_shuffle(s)
 
     return oracle.Scan(

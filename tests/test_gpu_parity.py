@@ -156,6 +156,17 @@ SECTOR_CASES = [
     dict(fft=2048, products=oracle.PROD_XCF, band=(0, 0, 1024, 0)),
     dict(fft=4096, products=oracle.PROD_ACF | oracle.PROD_ACF_OVERLAP_ONLY,
          band=(-9, 9, 2048, 0), grid=1),
+    # FFT 8192 (its own kernel): every decode variant, both grids, LSB on
+    # either station, product subsets
+    dict(fft=8192, shuffle="pairswap", lsb2=True, band=(-40, 40, 4096, 0), grid=1),
+    dict(fft=8192, bits1=4, bits2=2, shuffle="generic", lsb1=True, lsb2=True,
+         band=(64, 0, 4032, 64), grid=1),
+    dict(fft=8192, bits1=8, bits2=4, shuffle="generic", band=(0, 0, 4096, 0),
+         products=oracle.PROD_ACF | oracle.PROD_ACF_OVERLAP_ONLY | oracle.PROD_XCF),
+    dict(fft=8192, shuffle="sample2", lsb1=True, band=(16, 0, 4080, 16), grid=1,
+         products=oracle.PROD_XCF),
+    dict(fft=8192, bits1=1, bits2=1, shuffle="generic", lsb2=True, band=(-3, 3, 4096, 0),
+         products=oracle.PROD_ACF),
 ]
 
 
