@@ -41,7 +41,7 @@ constexpr int kSlots = 2 * kUnits + 1;  // accumulator rows (bin N/4 by thread 0
 
 // Shared memory: level tables first, at a fixed address, so that the decode's
 // table loads take an immediate base.
-//   [0, 4096)      levels: primary, primary negated, secondary, secondary negated (256 f32 each)
+//   [0, 4096)      levels: primary at 0, secondary at 2048 (2^b f32 each, then their negations)
 //   [4096, 4352)   rotate amounts: [2 stations][32 sample slots] u32
 //   [4352, 4448)   frame records, double-buffered
 //   [4448, 4464)   mbarriers; [4464, 4480) error flag
@@ -98,6 +98,22 @@ __device__ __forceinline__ void fold_inputs(const uint32_t* __restrict__ words, 
       const float x = level(w[r * WSTEP]);
       if (IMAG) v[r].y = x; else v[r].x = x;
     }
+  } else if ((unsigned)(shift + (T1 - 1)) < (unsigned)(2 * T1 - 1)) {
+    // |shift| < N/16: only r = 0 and r = 15 can fall outside the frame
+    const uint32_t* w = words + w0;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      float x;
+      if (r == 0 || r == 15) {
+        const int m = m0 + r * T1;
+        const bool in = (unsigned)m < (unsigned)kN;
+        x = level(words[in ? w0 + r * WSTEP : 0]);
+        x = in ? x : 0.0f;
+      } else {
+        x = level(w[r * WSTEP]);
+      }
+      if (IMAG) v[r].y = x; else v[r].x = x;
+    }
   } else {
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
@@ -152,9 +168,12 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
 
   // ---- constant tables
   for (int i = tid; i < 1024; i += kT) {
+    // per station: 2^b levels, then their negations (the two sign groups of a
+    // warp's table loads fall in different banks)
     const StationParams& q = (i < 512) ? sp : ss;
-    const float x = q.levels[i & 255] * q.scale;
-    lv[i] = (i & 256) ? -x : x;
+    const int n = 1 << q.bits, c = i & 511;
+    const float x = c < 2 * n ? q.levels[c & (n - 1)] * q.scale : 0.0f;
+    lv[i] = c >= n ? -x : x;
   }
   for (int i = tid; i < 64; i += kT) {
     // rotate amounts of sample slot c: bit j of the sample is word bit p_j
@@ -277,8 +296,8 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
       float2 v[16];
       const int mP = tid - sP, mS = tid - sS;
       const int cP = mP & ((32 / bitsP) - 1), cS = mS & ((32 / bitsS) - 1);
-      const uint32_t tbP = (uint32_t)((mP & lsbP) << 10);
-      const uint32_t tbS = 2048u + (uint32_t)((mS & lsbS) << 10);
+      const uint32_t tbP = (uint32_t)((mP & lsbP) << (bitsP + 2));
+      const uint32_t tbS = 2048u + (uint32_t)((mS & lsbS) << (bitsS + 2));
       fold_station<false>(bitsP, splitP, wP, smem, sP, pos[cP], tbP, v, tid);
       fold_station<true>(bitsS, splitS, wS, smem, sS, pos[32 + cS], tbS, v, tid);
       dft16(v);

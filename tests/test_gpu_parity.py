@@ -202,6 +202,29 @@ def test_sector_vs_fp64(engine, kw, nf):
     s.close()
 
 
+@pytest.mark.parametrize("d1", [-2.3e-6, 5.1e-6, 1.7e-5])
+def test_sector_large_shift(engine, d1):
+    """Integer shifts beyond N/16 (and beyond N: an all-zero station frame)."""
+    delay = dict(DELAY, net_d1_base=d1)
+    scan = make_scan(fft=8192, fs=512e6, delay=delay, shuffle="generic", lsb1=True,
+                     band=(128, 0, 3968, 128))
+    nf = 9
+    r1, r2 = signal_raw(scan, nf, seed=5, rho=0.2, delay_samples=6.4)
+    s = engine.open_scan(to_fxc(scan))
+    got = s.sector_device(dev(r1), dev(r2), nf, first_frame=3)
+    ref = oracle.fp64_sector_corr(scan, r1, r2, nf, first_frame=3)
+    if not np.any(ref["acf11"]):  # shift >= N: station 1 frames are all zero
+        # only rounding leakage of the shared complex FFT remains
+        scale = float(ref["acf22"].max())
+        assert float(np.abs(got["acf11"]).max()) < 1e-10 * scale
+        assert float(np.abs(got["xcf"]).max()) < 1e-6 * scale
+        rel, ph, ab = spectral_errors(got["acf22"], ref["acf22"])
+        assert rel < 1e-5, rel
+    else:
+        assert_sector_close(got, ref, scan, f"large shift {d1}", nf=nf, ref_acf=ref)
+    s.close()
+
+
 def test_sector_empty_and_deterministic(engine):
     scan = make_scan(fft=4096, fs=512e6, delay=DELAY, band=(40, 0, 2008, 40))
     s = engine.open_scan(to_fxc(scan))
