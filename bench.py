@@ -184,8 +184,8 @@ def measured_peaks():
 
 def profile_traffic_per_frame_pair():
     """DRAM bytes per frame pair of the correlation kernel from the committed
-    ncu summary (profiles/corr_kernel_n8192.txt), or None."""
-    f = ROOT / "profiles" / "corr_kernel_n8192.txt"
+    ncu summary (profiles/corr_fold_kernel_n8192.txt), or None."""
+    f = ROOT / "profiles" / "corr_fold_kernel_n8192.txt"
     if not f.exists():
         return None
     for ln in f.read_text().splitlines():
