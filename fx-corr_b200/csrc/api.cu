@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "fxc.h"
+#include "fxc_internal.h"
 #include "fxc_kernels.h"
 
 using namespace fxc;
@@ -64,6 +65,7 @@ struct fxc_engine {
   uint64_t in_use = 0;
   std::mutex mu;
   std::vector<fxc_scan*> scans;  // open scans, closed by fxc_engine_destroy
+  std::vector<fxc_server*> servers;  // live servers, destroyed first by fxc_engine_destroy
 };
 
 struct SectorSlot {
@@ -90,6 +92,10 @@ struct fxc_scan {
   int shkind[2] = {0, 0};
   float scale[2] = {1.0f, 1.0f};  // exact powers of two (see level_scale)
   double* d_table = nullptr;
+  uint64_t table_cap = 0;        // doubles
+  bool table_bound = false;      // the bound configuration has a geometric table
+  uint8_t* h_tab = nullptr;      // pinned staging of the uploaded tables
+  uint64_t h_tab_cap = 0;
   uint32_t* d_lut = nullptr;     // [2][1024]
   float* d_levels = nullptr;     // [2][256]
   uint8_t* d_shuffle_out = nullptr;
@@ -98,6 +104,9 @@ struct fxc_scan {
   int qmonotonic = 0;
   double* d_partials = nullptr;
   uint64_t partials_elems = 0;
+  uint64_t partials_cap = 0;     // elements allocated
+  uint64_t big_cap = 0;          // float2 elements allocated per batch buffer
+  uint32_t acc_cap = 0;          // H the sector slots' d_acc / h_acc hold
   FrameInfo* d_finfo = nullptr;  // per-frame delay records of the sector in flight
   uint64_t finfo_cap = 0;
   float2* d_big[2] = {nullptr, nullptr};  // FFT lengths > 8192: batch scratch
@@ -157,8 +166,8 @@ DelayParams delay_params(const fxc_scan* s) {
   p.frame_dt = c.frame_dt;
   p.fs = c.fs;
   p.time_offset_s = c.time_offset_s;
-  p.table = s->d_table;
-  p.table_len = s->d_table ? c.geom_len : 0;
+  p.table = s->table_bound ? s->d_table : nullptr;
+  p.table_len = s->table_bound ? c.geom_len : 0;
   p.coarse = c.coarse_delay_s;
   p.user_samples = c.delay_user_samples;
   p.extra_rate = c.extra_delay_rate_sps;
@@ -286,17 +295,6 @@ fxc_status validate_cfg(const fxc_scan_cfg* c) {
   if (c->products & ~31u) return fail(FXC_EINVAL, "unknown product flags");
   if ((c->products & (FXC_PROD_PHASED | FXC_PROD_RAW)) && !(c->w1 == c->w1 && c->w2 == c->w2))
     return fail(FXC_EINVAL, "phased weights must be numbers");
-  return FXC_OK;
-}
-
-fxc_status grow(uint8_t** p, uint64_t* cap, uint64_t need) {
-  if (*cap >= need) return FXC_OK;
-  if (*p) cudaFree(*p);
-  *p = nullptr;
-  *cap = 0;
-  const uint64_t want = std::max<uint64_t>(need, 16);
-  CK(cudaMalloc(p, want));
-  *cap = want;
   return FXC_OK;
 }
 
@@ -439,7 +437,164 @@ fxc_status run_corr_stage(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uin
   return FXC_OK;
 }
 
+// Reserves `delta` more bytes of the engine's HBM budget for scan s.
+fxc_status reserve(fxc_scan* s, uint64_t delta) {
+  if (!delta) return FXC_OK;
+  std::lock_guard<std::mutex> lk(s->eng->mu);
+  if (s->eng->in_use + delta > s->eng->budget)
+    return fail(FXC_EBUSY, "HBM budget exhausted (%llu + %llu > %llu bytes)",
+                (unsigned long long)s->eng->in_use, (unsigned long long)delta,
+                (unsigned long long)s->eng->budget);
+  s->eng->in_use += delta;
+  s->hbm_bytes += delta;
+  return FXC_OK;
+}
+
+// Device buffer of at least `need` bytes, growth charged to the budget.
+fxc_status grow_charged(fxc_scan* s, uint8_t** p, uint64_t* cap, uint64_t need) {
+  if (*cap >= need) return FXC_OK;
+  const uint64_t want = std::max<uint64_t>(need, 16);
+  fxc_status st = reserve(s, want - *cap);
+  if (st != FXC_OK) return st;
+  const uint64_t old = *cap;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  const cudaError_t e = cudaMalloc(p, want);
+  if (e != cudaSuccess) {
+    std::lock_guard<std::mutex> lk(s->eng->mu);
+    s->eng->in_use -= std::min(s->eng->in_use, want);
+    s->hbm_bytes -= std::min(s->hbm_bytes, want);
+    (void)old;
+    return fail(e == cudaErrorMemoryAllocation ? FXC_ENOMEM : FXC_ECUDA, "cudaMalloc: %s",
+                cudaGetErrorString(e));
+  }
+  *cap = want;
+  return FXC_OK;
+}
+
 }  // namespace
+
+namespace fxc {
+
+// Binds scan s to cfg: derived sizes, buffers grown (and charged to the HBM
+// budget) where the new configuration needs more, tables uploaded on the
+// scan's compute stream from pinned staging.  Rebinding an idle scan to
+// another configuration is the serving loop's way of reusing the device
+// state of a finished job; nothing is freed until the scan closes.
+fxc_status scan_bind(fxc_scan* s, const fxc_scan_cfg* cfg) {
+  fxc_status st = validate_cfg(cfg);
+  if (st != FXC_OK) return st;
+  for (const auto& sl : s->slots)
+    if (sl.busy) return fail(FXC_EBUSY, "scan has sectors in flight");
+  fxc_engine* e = s->eng;
+  DeviceGuard g(e->device);
+  const uint32_t n = cfg->fft_len, h = n / 2 + 1;
+  const uint64_t maxg = n > 8192 ? (uint64_t)kLargeGroups
+                                 : (uint64_t)e->sm_count * (uint64_t)corr_ctas_per_sm(n);
+  const uint64_t pel = maxg * 4 * h;
+  const uint64_t bigf = n > 8192 ? (uint64_t)large_batch_frames(n) : 0;
+  const uint64_t bige = bigf * (uint64_t)n;
+  const uint64_t tlen = cfg->delay.geom_table ? cfg->delay.geom_len : 0;
+  // the previous configuration's work must be done before buffers are reused
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaStreamSynchronize(s->copy_stream));
+  if (pel > s->partials_cap) {
+    uint8_t* p = reinterpret_cast<uint8_t*>(s->d_partials);
+    uint64_t cap = s->partials_cap * 8;
+    if ((st = grow_charged(s, &p, &cap, pel * 8)) != FXC_OK) return st;
+    s->d_partials = reinterpret_cast<double*>(p);
+    s->partials_cap = cap / 8;
+  }
+  if (bige > s->big_cap) {
+    for (int b = 0; b < 2; ++b) {
+      uint8_t* p = reinterpret_cast<uint8_t*>(s->d_big[b]);
+      uint64_t cap = s->big_cap * sizeof(float2);
+      if ((st = grow_charged(s, &p, &cap, bige * sizeof(float2))) != FXC_OK) return st;
+      s->d_big[b] = reinterpret_cast<float2*>(p);
+    }
+    s->big_cap = bige;
+  }
+  if (tlen > s->table_cap) {
+    uint8_t* p = reinterpret_cast<uint8_t*>(s->d_table);
+    uint64_t cap = s->table_cap * 8;
+    if ((st = grow_charged(s, &p, &cap, tlen * 8)) != FXC_OK) return st;
+    s->d_table = reinterpret_cast<double*>(p);
+    s->table_cap = cap / 8;
+  }
+  if (h > s->acc_cap) {
+    for (auto& sl : s->slots) {
+      uint8_t* p = reinterpret_cast<uint8_t*>(sl.d_acc);
+      uint64_t cap = (uint64_t)s->acc_cap * 5 * 8;
+      if ((st = grow_charged(s, &p, &cap, (uint64_t)h * 5 * 8)) != FXC_OK) return st;
+      sl.d_acc = reinterpret_cast<double*>(p);
+      if (sl.h_acc) cudaFreeHost(sl.h_acc);
+      sl.h_acc = nullptr;
+      CK(cudaMallocHost(&sl.h_acc, sizeof(double) * 5 * h + 16));
+    }
+    s->acc_cap = h;
+  }
+  // tables into pinned staging, then one async upload each
+  constexpr uint64_t kLut = 0, kLv = 8192, kSh = kLv + 2048, kQl = kSh + 32, kEnc = kQl + 1024,
+                     kTab = kEnc + 4096;
+  if ((st = grow_host(&s->h_tab, &s->h_tab_cap, kTab + tlen * 8)) != FXC_OK) return st;
+  uint32_t* lut = reinterpret_cast<uint32_t*>(s->h_tab + kLut);
+  float* lv = reinterpret_cast<float*>(s->h_tab + kLv);
+  float* ql = reinterpret_cast<float*>(s->h_tab + kQl);
+  uint32_t* enc = reinterpret_cast<uint32_t*>(s->h_tab + kEnc);
+  build_lut(cfg->shuffle1, lut);
+  build_lut(cfg->shuffle2, lut + 1024);
+  for (int i = 0; i < 512; ++i) lv[i] = 0.0f;
+  for (uint32_t i = 0; i < cfg->nlevels1; ++i) lv[i] = (float)cfg->levels1[i];
+  for (uint32_t i = 0; i < cfg->nlevels2; ++i) lv[256 + i] = (float)cfg->levels2[i];
+  std::memcpy(s->h_tab + kSh, cfg->shuffle1, 32);
+  // phased re-quantiser: ant1's levels as f32 (quantise_frame compares
+  // |x - lv as f32|) and the encode LUT of ant1's shuffle: packed bit pos
+  // goes to bit shuffle1[pos] (utils.rs:395)
+  std::memcpy(ql, lv, 256 * sizeof(float));
+  std::memset(enc, 0, 1024 * sizeof(uint32_t));
+  for (int pos = 0; pos < 32; ++pos)
+    for (int v = 0; v < 256; ++v)
+      if ((v >> (pos & 7)) & 1) enc[(pos >> 3) * 256 + v] |= 1u << cfg->shuffle1[pos];
+  bool up = true, down = true;
+  for (uint32_t i = 1; i < cfg->nlevels1; ++i) {
+    if (!(lv[i] > lv[i - 1])) up = false;
+    if (!(lv[i] < lv[i - 1])) down = false;
+  }
+  if (tlen) std::memcpy(s->h_tab + kTab, cfg->delay.geom_table, tlen * 8);
+  CK(cudaMemcpyAsync(s->d_lut, lut, 8192, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->d_levels, lv, 2048, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->d_shuffle_out, s->h_tab + kSh, 32, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->d_qlevels, ql, 1024, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->d_enc_lut, enc, 4096, cudaMemcpyHostToDevice, s->stream));
+  if (tlen)
+    CK(cudaMemcpyAsync(s->d_table, s->h_tab + kTab, tlen * 8, cudaMemcpyHostToDevice, s->stream));
+  // the copy stream's first transfer of a sector must not overtake the uploads
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, s->stream));
+  CK(cudaStreamWaitEvent(s->copy_stream, ev, 0));
+  cudaEventDestroy(ev);
+
+  s->cfg = *cfg;
+  s->cfg.delay.geom_table = nullptr;  // the host pointer is not kept
+  s->table_bound = tlen != 0;
+  s->qmonotonic = up ? 1 : (down ? -1 : 0);
+  s->n = n;
+  s->h = h;
+  s->bpf1 = (uint32_t)fxc_bytes_per_frame(n, cfg->bits1);
+  s->bpf2 = (uint32_t)fxc_bytes_per_frame(n, cfg->bits2);
+  s->bpfo = (uint32_t)fxc_bytes_per_frame(n, cfg->bits_out);
+  s->shkind[0] = shuffle_kind(cfg->shuffle1);
+  s->shkind[1] = shuffle_kind(cfg->shuffle2);
+  s->scale[0] = level_scale(cfg->levels1, cfg->nlevels1);
+  s->scale[1] = level_scale(cfg->levels2, cfg->nlevels2);
+  s->partials_elems = pel;
+  s->big_frames = bigf;
+  return FXC_OK;
+}
+
+}  // namespace fxc
 
 // ======================================================================= ABI
 
@@ -490,6 +645,12 @@ fxc_status fxc_engine_create(const fxc_device_opts* opts, fxc_engine** out) {
 
 fxc_status fxc_engine_destroy(fxc_engine* e) {
   if (!e) return FXC_OK;
+  std::vector<fxc_server*> live;
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    live = e->servers;
+  }
+  for (fxc_server* sv : live) fxc_server_destroy(sv);
   std::vector<fxc_scan*> open;
   {
     std::lock_guard<std::mutex> lk(e->mu);
@@ -508,34 +669,6 @@ fxc_status fxc_scan_open(fxc_engine* e, const fxc_scan_cfg* cfg, fxc_scan** out)
   DeviceGuard g(e->device);
   auto* s = new fxc_scan();
   s->eng = e;
-  s->cfg = *cfg;
-  s->n = cfg->fft_len;
-  s->h = s->n / 2 + 1;
-  s->bpf1 = (uint32_t)fxc_bytes_per_frame(s->n, cfg->bits1);
-  s->bpf2 = (uint32_t)fxc_bytes_per_frame(s->n, cfg->bits2);
-  s->bpfo = (uint32_t)fxc_bytes_per_frame(s->n, cfg->bits_out);
-  s->shkind[0] = shuffle_kind(cfg->shuffle1);
-  s->shkind[1] = shuffle_kind(cfg->shuffle2);
-  s->scale[0] = level_scale(cfg->levels1, cfg->nlevels1);
-  s->scale[1] = level_scale(cfg->levels2, cfg->nlevels2);
-  const uint64_t maxg = s->n > 8192 ? (uint64_t)kLargeGroups
-                                    : (uint64_t)e->sm_count * (uint64_t)corr_ctas_per_sm(s->n);
-  s->partials_elems = maxg * 4 * s->h;
-  s->big_frames = s->n > 8192 ? (uint64_t)large_batch_frames(s->n) : 0;
-  const uint64_t need = s->partials_elems * 8 + 2 * 1024 * 4 + 2 * 256 * 4 + 64 +
-                        (cfg->delay.geom_table ? cfg->delay.geom_len * 8 : 0) +
-                        2 * s->big_frames * (uint64_t)s->n * sizeof(float2);
-  {
-    std::lock_guard<std::mutex> lk(e->mu);
-    if (e->in_use + need > e->budget) {
-      delete s;
-      return fail(FXC_EBUSY, "HBM budget exhausted (%llu + %llu > %llu bytes)",
-                  (unsigned long long)e->in_use, (unsigned long long)need,
-                  (unsigned long long)e->budget);
-    }
-    e->in_use += need;
-  }
-  s->hbm_bytes = need;
   auto cleanup = [&](fxc_status r) {
     fxc_scan_close(s);
     return r;
@@ -549,60 +682,31 @@ fxc_status fxc_scan_open(fxc_engine* e, const fxc_scan_cfg* cfg, fxc_scan** out)
   } while (0)
   CKS(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   CKS(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
-  CKS(cudaMalloc(&s->d_partials, s->partials_elems * sizeof(double)));
-  for (int b = 0; b < 2 && s->big_frames; ++b)
-    CKS(cudaMalloc(&s->d_big[b], s->big_frames * (uint64_t)s->n * sizeof(float2)));
   CKS(cudaMalloc(&s->d_lut, 2 * 1024 * sizeof(uint32_t)));
   CKS(cudaMalloc(&s->d_levels, 2 * 256 * sizeof(float)));
   CKS(cudaMalloc(&s->d_shuffle_out, 32));
+  CKS(cudaMalloc(&s->d_qlevels, 256 * sizeof(float)));
+  CKS(cudaMalloc(&s->d_enc_lut, 1024 * sizeof(uint32_t)));
   CKS(cudaMalloc(&s->d_err, 16));
   CKS(cudaMemset(s->d_err, 0, 16));
-  {
-    std::vector<uint32_t> lut(2048);
-    build_lut(cfg->shuffle1, lut.data());
-    build_lut(cfg->shuffle2, lut.data() + 1024);
-    CKS(cudaMemcpy(s->d_lut, lut.data(), lut.size() * 4, cudaMemcpyHostToDevice));
-    std::vector<float> lv(512, 0.0f);
-    for (uint32_t i = 0; i < cfg->nlevels1; ++i) lv[i] = (float)cfg->levels1[i];
-    for (uint32_t i = 0; i < cfg->nlevels2; ++i) lv[256 + i] = (float)cfg->levels2[i];
-    CKS(cudaMemcpy(s->d_levels, lv.data(), lv.size() * 4, cudaMemcpyHostToDevice));
-    CKS(cudaMemcpy(s->d_shuffle_out, cfg->shuffle1, 32, cudaMemcpyHostToDevice));
-    // phased re-quantiser: ant1's levels as f32 (quantise_frame compares
-    // |x - lv as f32|) and the encode LUT of ant1's shuffle: packed bit pos
-    // goes to bit shuffle1[pos] (utils.rs:395)
-    CKS(cudaMalloc(&s->d_qlevels, 256 * sizeof(float)));
-    CKS(cudaMemcpy(s->d_qlevels, lv.data(), 256 * sizeof(float), cudaMemcpyHostToDevice));
-    std::vector<uint32_t> enc(1024, 0u);
-    for (int pos = 0; pos < 32; ++pos)
-      for (int v = 0; v < 256; ++v)
-        if ((v >> (pos & 7)) & 1) enc[(pos >> 3) * 256 + v] |= 1u << cfg->shuffle1[pos];
-    CKS(cudaMalloc(&s->d_enc_lut, 1024 * sizeof(uint32_t)));
-    CKS(cudaMemcpy(s->d_enc_lut, enc.data(), 1024 * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    bool up = true, down = true;
-    for (uint32_t i = 1; i < cfg->nlevels1; ++i) {
-      if (!(lv[i] > lv[i - 1])) up = false;
-      if (!(lv[i] < lv[i - 1])) down = false;
-    }
-    s->qmonotonic = up ? 1 : (down ? -1 : 0);
-  }
-  if (cfg->delay.geom_table) {
-    CKS(cudaMalloc(&s->d_table, cfg->delay.geom_len * sizeof(double)));
-    CKS(cudaMemcpy(s->d_table, cfg->delay.geom_table, cfg->delay.geom_len * sizeof(double),
-                   cudaMemcpyHostToDevice));
-  }
-  s->cfg.delay.geom_table = nullptr;  // the host pointer is not kept
   s->slots.resize((size_t)e->max_inflight);
   for (auto& sl : s->slots) {
     CKS(cudaEventCreateWithFlags(&sl.ev_h2d, cudaEventDisableTiming));
     CKS(cudaEventCreateWithFlags(&sl.ev_done, cudaEventDisableTiming));
-    CKS(cudaMalloc(&sl.d_acc, sizeof(double) * 5 * s->h));
-    CKS(cudaMallocHost(&sl.h_acc, sizeof(double) * 5 * s->h + 16));
   }
 #undef CKS
   {
     std::lock_guard<std::mutex> lk(e->mu);
     e->scans.push_back(s);
   }
+  st = scan_bind(s, cfg);
+  if (st != FXC_OK) {
+    const std::string msg = g_err;
+    fxc_scan_close(s);
+    g_err = msg;
+    return st;
+  }
+  CK(cudaStreamSynchronize(s->stream));
   *out = s;
   return FXC_OK;
 }
@@ -637,6 +741,7 @@ fxc_status fxc_scan_close(fxc_scan* s) {
   cudaFree(s->d_enc_lut);
   cudaFree(s->d_err);
   cudaFree(s->d_table);
+  cudaFreeHost(s->h_tab);
   if (s->stream) cudaStreamDestroy(s->stream);
   if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
   {
@@ -780,8 +885,8 @@ fxc_status fxc_sector_submit(fxc_scan* s, const uint8_t* raw1, uint64_t n1, cons
                        s->slots.size());
   DeviceGuard g(s->eng->device);
   fxc_status st;
-  if ((st = grow(&sl->d_raw1, &sl->cap1, need1)) != FXC_OK) return st;
-  if ((st = grow(&sl->d_raw2, &sl->cap2, need2)) != FXC_OK) return st;
+  if ((st = grow_charged(s, &sl->d_raw1, &sl->cap1, need1)) != FXC_OK) return st;
+  if ((st = grow_charged(s, &sl->d_raw2, &sl->cap2, need2)) != FXC_OK) return st;
   if (nf) {
     CK(cudaMemcpyAsync(sl->d_raw1, raw1, need1, cudaMemcpyHostToDevice, s->copy_stream));
     CK(cudaMemcpyAsync(sl->d_raw2, raw2, need2, cudaMemcpyHostToDevice, s->copy_stream));
@@ -789,7 +894,7 @@ fxc_status fxc_sector_submit(fxc_scan* s, const uint8_t* raw1, uint64_t n1, cons
   const bool raw = (s->cfg.products & FXC_PROD_RAW) != 0;
   const uint64_t need_o = nf * s->bpfo;
   if (raw) {
-    if ((st = grow(&sl->d_rawout, &sl->cap_out, need_o)) != FXC_OK) return st;
+    if ((st = grow_charged(s, &sl->d_rawout, &sl->cap_out, need_o)) != FXC_OK) return st;
     if ((st = grow_host(&sl->h_rawout, &sl->hcap_out, need_o)) != FXC_OK) return st;
   }
   CK(cudaEventRecord(sl->ev_h2d, s->copy_stream));
@@ -933,6 +1038,13 @@ fxc_status fxc_normalize(uint32_t fft, uint64_t nf, double level_power, const do
 namespace fxc {
 
 fxc_status internal_fail(fxc_status s, const char* msg) { return fail(s, "%s", msg); }
+
+void engine_track_server(fxc_engine* e, fxc_server* sv, bool add) {
+  std::lock_guard<std::mutex> lk(e->mu);
+  auto& v = e->servers;
+  if (add) v.push_back(sv);
+  else v.erase(std::remove(v.begin(), v.end(), sv), v.end());
+}
 
 fxc_status internal_prepare_tables(const fxc_scan_cfg* c, uint32_t* lut2048, float* lv512,
                                    float scale[2], int kind[2]) {

@@ -25,13 +25,8 @@
 #include <mutex>
 
 #include "fxc.h"
+#include "fxc_internal.h"
 #include "fxc_kernels.h"
-
-namespace fxc {
-fxc_status internal_fail(fxc_status s, const char* msg);
-fxc_status internal_prepare_tables(const fxc_scan_cfg* c, uint32_t* lut2048, float* lv512,
-                                   float scale[2], int kind[2]);
-}  // namespace fxc
 
 using namespace fxc;
 

@@ -34,6 +34,7 @@ EXPORTS = [
     "fxc_decode_device", "fxc_spectra_device", "fxc_parse_shuffle", "fxc_band_alignment",
     "fxc_level_power", "fxc_normalize", "fxc_bytes_per_frame", "fxc_probe_fp32_peak",
     "fxc_scan_set_profiling", "fxc_scan_profile", "fxc_sector_run_device_noalloc",
+    "fxc_server_create", "fxc_server_submit", "fxc_server_wait", "fxc_server_destroy",
 ]
 NOALLOC_MAX_FRAMES = 32768
 
@@ -91,6 +92,21 @@ class DeviceOpts(C.Structure):
                 ("hbm_budget_bytes", C.c_uint64)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("slots", C.c_int32)]
+
+
+class JobC(C.Structure):
+    _fields_ = [("cfg", C.c_void_p), ("raw1", C.c_void_p), ("raw2", C.c_void_p),
+                ("nf", C.c_uint64), ("first_frame", C.c_uint64), ("sector_frames", C.c_uint64),
+                ("out", C.c_void_p), ("raw_out", C.c_void_p)]
+
+
+class JobStats(C.Structure):
+    _fields_ = [("status", C.c_int32), ("sectors", C.c_uint32), ("t_submit_ns", C.c_uint64),
+                ("t_start_ns", C.c_uint64), ("t_done_ns", C.c_uint64)]
+
+
 class SectorOut(C.Structure):
     _fields_ = [("acf11", C.POINTER(C.c_double)), ("acf22", C.POINTER(C.c_double)),
                 ("xcf", C.POINTER(C.c_double)), ("phased", C.POINTER(C.c_double)),
@@ -141,6 +157,10 @@ def lib():
                                            vp, vp], st),
         "fxc_scan_profile": ([vp, f64p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_int32],
                              st),
+        "fxc_server_create": ([vp, C.POINTER(ServerOpts), C.POINTER(vp)], st),
+        "fxc_server_submit": ([vp, C.POINTER(JobC), C.POINTER(C.c_uint64)], st),
+        "fxc_server_wait": ([vp, C.c_uint64, C.c_int32, C.POINTER(JobStats)], st),
+        "fxc_server_destroy": ([vp], st),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -246,6 +266,7 @@ class Engine:
         self.h = h
         self.device = device
         self._scans = weakref.WeakSet()
+        self._servers = weakref.WeakSet()
 
     def open_scan(self, cfg: ScanConfig) -> "Scan":
         s = Scan(self, cfg)
@@ -254,9 +275,11 @@ class Engine:
 
     def close(self):
         if self.h:
-            # the library closes every scan still open on this engine
+            # the library destroys the engine's servers and closes its scans
             for s in list(self._scans):
                 s.h = None
+            for sv in list(self._servers):
+                sv.h = None
             lib().fxc_engine_destroy(self.h)
             self.h = None
 
@@ -384,6 +407,69 @@ class Scan:
             out["raw"] = raw[: getattr(self, "_nf", {}).pop(sector_id, 0) *
                              self.cfg.bpf(self.cfg.bits_out)]
         return out
+
+
+class Server:
+    """The serving loop (fxc_server_*): jobs of one scan configuration each,
+    admitted into ``slots`` concurrent device contexts as they free up."""
+
+    def __init__(self, eng: Engine, slots: int = 4):
+        self.eng = eng
+        h = C.c_void_p()
+        check(lib().fxc_server_create(eng.h, C.byref(ServerOpts(slots)), C.byref(h)))
+        self.h = h
+        self._jobs = {}
+        eng._servers.add(self)
+
+    def submit(self, cfg: ScanConfig, raw1, raw2, nf: int, first_frame: int = 0,
+               sector_frames: int = 0) -> int:
+        """Queue a job; raw1/raw2 are host arrays (page-locked torch tensors
+        or numpy arrays) that must stay alive until wait()."""
+        c = cfg.to_c()
+        sf = sector_frames or max(nf, 1)
+        nsec = (nf + sf - 1) // sf if nf else 1
+        out = np.zeros((nsec, 5 * cfg.h))
+        raw = None
+        if cfg.products & PROD_RAW:
+            raw = np.zeros(max(1, nf * cfg.bpf(cfg.bits_out)), np.uint8)
+        j = JobC(C.addressof(c), _ptr(raw1), _ptr(raw2), nf, first_frame, sector_frames,
+                 out.ctypes.data, None if raw is None else raw.ctypes.data)
+        jid = C.c_uint64()
+        check(lib().fxc_server_submit(self.h, C.byref(j), C.byref(jid)))
+        self._jobs[jid.value] = (cfg, raw1, raw2, out, raw)
+        return jid.value
+
+    def wait(self, job_id: int, timeout_ms: int = -1):
+        """(list of per-dump result dicts, stats dict) of a finished job."""
+        st = JobStats()
+        try:
+            check(lib().fxc_server_wait(self.h, job_id, timeout_ms, C.byref(st)))
+        except FxcError as e:
+            if e.status != ETIMEDOUT:
+                self._jobs.pop(job_id, None)
+            raise
+        cfg, _, _, out, raw = self._jobs.pop(job_id)
+        h = cfg.h
+        dumps = [dict(acf11=o[:h], acf22=o[h:2 * h], xcf=o[2 * h:4 * h].view(np.complex128),
+                      phased=o[4 * h:]) for o in out]
+        stats = dict(status=st.status, sectors=st.sectors, t_submit_ns=st.t_submit_ns,
+                     t_start_ns=st.t_start_ns, t_done_ns=st.t_done_ns,
+                     latency_s=(st.t_done_ns - st.t_submit_ns) * 1e-9)
+        if raw is not None:
+            stats["raw"] = raw
+        return dumps, stats
+
+    def close(self):
+        if self.h and self.eng.h:
+            lib().fxc_server_destroy(self.h)
+        self.h = None
+        self._jobs.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # -------------------------------------------------------------- helpers

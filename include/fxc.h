@@ -202,6 +202,53 @@ FXC_API fxc_status fxc_sector_run_device_noalloc(const fxc_scan_cfg* cfg, const 
                                                  uint64_t first_frame, double* d_acc,
                                                  void* stream);
 
+/* ---- serving loop -------------------------------------------------------
+ * No reference counterpart: the reference correlates one scan per process
+ * (the run_once sector loop, src/main.rs:2173-2591).  A server admits jobs
+ * (one scan's frames from host memory, dumped every sector_frames frames)
+ * into `slots` concurrent device contexts; a job that arrives while others
+ * run starts as soon as a slot is free and the engine's HBM budget admits
+ * its buffers, and the jobs' copies and kernels overlap on the device.  The
+ * device state of a finished job (partials, frame records, staging buffers,
+ * tables) is reused by the next job of its slot.  Each job's products are
+ * those of fxc_sector_submit/wait over the same sectors, bit for bit, alone
+ * or in any mix. */
+typedef struct fxc_server fxc_server;
+
+typedef struct fxc_server_opts {
+  int32_t slots;             /* jobs on the device at once (0 = 4) */
+} fxc_server_opts;
+
+typedef struct fxc_job {
+  const fxc_scan_cfg* cfg;   /* copied at submit, geometric table included */
+  const uint8_t* raw1;       /* nf * bytes_per_frame(bits1) bytes; page-locked memory
+                                lets the copies overlap other jobs' work */
+  const uint8_t* raw2;       /* nf * bytes_per_frame(bits2) bytes */
+  uint64_t nf;               /* frames in the job */
+  uint64_t first_frame;      /* scan frame index of raw1[0] (delay-model time) */
+  uint64_t sector_frames;    /* frames per dump; 0 = one dump for the whole job */
+  double* out;               /* per dump: acf11[H] | acf22[H] | xcf[2H] | phased[H] */
+  uint8_t* raw_out;          /* FXC_PROD_RAW: nf * bytes_per_frame(bits_out) bytes */
+} fxc_job;
+
+typedef struct fxc_job_stats {
+  int32_t status;            /* the job's fxc_status */
+  uint32_t sectors;          /* dumps written */
+  uint64_t t_submit_ns;      /* steady clock: submitted, started on a slot, done */
+  uint64_t t_start_ns;
+  uint64_t t_done_ns;
+} fxc_job_stats;
+
+FXC_API fxc_status fxc_server_create(fxc_engine* e, const fxc_server_opts* opts, fxc_server** out);
+/* Queues a job; the caller's buffers stay untouched until fxc_server_wait
+ * returns for the id. */
+FXC_API fxc_status fxc_server_submit(fxc_server* sv, const fxc_job* job, uint64_t* job_id);
+/* Waits for a job (timeout_ms < 0: no limit) and forgets it. */
+FXC_API fxc_status fxc_server_wait(fxc_server* sv, uint64_t job_id, int32_t timeout_ms,
+                                   fxc_job_stats* stats);
+/* Finishes the queued jobs, then releases the slots. */
+FXC_API fxc_status fxc_server_destroy(fxc_server* sv);
+
 /* Stage entry points, for parity tests of the individual steps. */
 /* Per-frame delay model on the device (src/main.rs:184-241). */
 FXC_API fxc_status fxc_delay_entries_device(fxc_scan* s, uint64_t first_frame, uint64_t nf,
