@@ -291,6 +291,139 @@ def run_reference(args, rank, world):
 
 # ------------------------------------------------------------------ main
 
+def serve_jobs(n_jobs, load, seed=5150):
+    """Seeded Poisson stream of correlation jobs: 0.1-5 s chunks at 256-1024
+    Msps, 2-bit, FFT 1024-16384, random station delays and rates, dumps every
+    second; arrivals at `load` x real time (data seconds offered per second)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    mean_dur = 2.55
+    t = 0.0
+    jobs = []
+    for k in range(n_jobs):
+        t += float(rng.exponential(mean_dur / load))
+        dur = float(rng.uniform(0.1, 5.0))
+        fs = float(rng.choice([256e6, 512e6, 1024e6]))
+        fft = int(rng.choice([1024, 2048, 4096, 8192, 16384]))
+        nf = max(1, int(round(dur * fs / fft)))
+        delay = dict(frame_dt=fft / fs, fs=fs, net_d1_base=float(rng.uniform(-2e-6, 2e-6)),
+                     total_rate1_base=float(rng.uniform(-1e-6, 1e-6)),
+                     net_d2_base=float(rng.uniform(-2e-6, 2e-6)), lo1_hz=8.4e9, lo2_hz=8.4e9)
+        jobs.append(dict(arrival=t, dur=dur, fs=fs, fft=fft, nf=nf,
+                         sector_frames=max(1, int(round(fs / fft))), delay=delay, seed=k))
+    return jobs
+
+
+def serve_leg(fxc, torch, eng, n_jobs=20, load=2.0, slots=4):
+    """Served (fxc_server, continuous batching) vs plain (one job at a time:
+    scan open, per-sector submit/wait, scan close) on the same job stream,
+    at the offered load and saturated (all jobs queued at once)."""
+    import threading
+
+    jobs = serve_jobs(n_jobs, load)
+    cfgs = []
+    for j in jobs:
+        c = fxc.ScanConfig(fft=j["fft"], fs=j["fs"], bits1=2, bits2=2,
+                           levels1=[-3.0, -1.0, 1.0, 3.0], levels2=[-3.0, -1.0, 1.0, 3.0],
+                           shuffle1=shuffle_internal(101), shuffle2=shuffle_internal(102),
+                           products=fxc.PROD_ACF | fxc.PROD_XCF, delay=j["delay"])
+        cfgs.append(c)
+    need = max(j["nf"] * j["fft"] * 2 // 8 for j in jobs)
+    pool = []
+    for st in range(2):
+        g = torch.Generator(device="cuda").manual_seed(77 + st)
+        d = torch.randint(0, 256, (need,), dtype=torch.uint8, device="cuda", generator=g)
+        hbuf = torch.empty(need, dtype=torch.uint8, pin_memory=True)
+        hbuf.copy_(d)
+        pool.append(hbuf)
+        del d
+    torch.cuda.synchronize()
+    p1, p2 = pool[0].numpy(), pool[1].numpy()
+    samples = [2 * j["nf"] * j["fft"] for j in jobs]
+
+    def plain_job(j, c):
+        s = eng.open_scan(c)
+        b = c.bpf(2)
+        sf, ids = j["sector_frames"], []
+        for f0 in range(0, j["nf"], sf):
+            n = min(sf, j["nf"] - f0)
+            if len(ids) == 3:
+                s.wait(ids.pop(0))
+            ids.append(s.submit(p1[f0 * b:(f0 + n) * b], p2[f0 * b:(f0 + n) * b], n, f0))
+        while ids:
+            s.wait(ids.pop(0))
+        s.close()
+
+    def run_plain(paced):
+        lat = []
+        t0 = time.perf_counter()
+        for j, c in zip(jobs, cfgs):
+            arr = t0 + (j["arrival"] if paced else 0.0)
+            now = time.perf_counter()
+            if now < arr:
+                time.sleep(arr - now)
+            plain_job(j, c)
+            lat.append(time.perf_counter() - arr)
+        return lat, time.perf_counter() - t0
+
+    sv = fxc.Server(eng, slots=slots)  # long-lived: slots keep their device state
+
+    def run_served(paced):
+        ids = [None] * len(jobs)
+        t0 = time.perf_counter()
+
+        def submitter():
+            for k, (j, c) in enumerate(zip(jobs, cfgs)):
+                if paced:
+                    dt = t0 + j["arrival"] - time.perf_counter()
+                    if dt > 0:
+                        time.sleep(dt)
+                b = c.bpf(2) * j["nf"]
+                ids[k] = sv.submit(c, p1[:b], p2[:b], j["nf"], 0, j["sector_frames"])
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        st = [sv.wait(i)[1] for i in ids]
+        wall = time.perf_counter() - t0
+        for x in st:
+            if x["status"] != 0:
+                raise RuntimeError(f"served job failed: {x}")
+        return [x["latency_s"] for x in st], wall
+
+    # warm both paths (module load; the server's slots grow to the job mix)
+    plain_job(jobs[0], cfgs[0])
+    run_served(False)
+    run_served(False)
+    # saturated: every job queued at once, median of three runs each
+    p_sat_wall = statistics.median(run_plain(False)[1] for _ in range(3))
+    s_sat_wall = statistics.median(run_served(False)[1] for _ in range(3))
+    s_lat, s_wall = run_served(True)
+    p_lat, p_wall = run_plain(True)
+    sv.close()
+    tot = float(sum(samples))
+
+    def pct(v, q):
+        return float(np.percentile(np.asarray(v) * 1e3, q))
+
+    return {
+        "jobs": len(jobs), "slots": slots, "offered_load_x_realtime": load,
+        "job_mix": "Poisson arrivals; 0.1-5 s at 256/512/1024 Msps, 2-bit, FFT 1024-16384, "
+                   "random delays/rates, 1-s dumps, pinned host buffers",
+        "data_s_per_job_mean": float(np.mean([j["dur"] for j in jobs])),
+        "served": {"p50_ms": pct(s_lat, 50), "p99_ms": pct(s_lat, 99),
+                   "gsample_s": tot / s_wall / 1e9,
+                   "saturated_jobs_per_s": len(jobs) / s_sat_wall,
+                   "saturated_gsample_s": tot / s_sat_wall / 1e9},
+        "plain": {"p50_ms": pct(p_lat, 50), "p99_ms": pct(p_lat, 99),
+                  "gsample_s": tot / p_wall / 1e9,
+                  "saturated_jobs_per_s": len(jobs) / p_sat_wall,
+                  "saturated_gsample_s": tot / p_sat_wall / 1e9},
+        "saturated_job_throughput_ratio": p_sat_wall / s_sat_wall,
+        "saturated_runs": "median of 3 per path",
+        "path": "fxc_server_submit/fxc_server_wait vs fxc_scan_open + fxc_sector_submit/wait",
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -300,6 +433,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-vs-plain leg")
+    ap.add_argument("--serve-jobs", type=int, default=20)
     ap.add_argument("--sectors", type=int, default=SECTORS,
                     help="sectors per step (profiling cases only; the workload is 10)")
     ap.add_argument("--frames-per-sector", type=int, default=NF_SECTOR,
@@ -418,6 +553,11 @@ def main():
                "path": "fxc_sector_submit/fxc_sector_wait, pinned host buffers"}
     clk = clocks.stop()
 
+    # ---- serving: continuous batching vs one job at a time (rank 0 of N=1)
+    serve = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        serve = serve_leg(fxc, torch, eng, n_jobs=args.serve_jobs)
+
     # ---- roofline of the dominant kernel (correlation kernel, one sector per launch)
     launch_ms = kern_ms / max(1, kern_launches)
     flops_launch = flops_per_station_sample(N) * 2 * NFS * N
@@ -465,6 +605,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "serving": serve,
             "gpu_launches": all_launches,
             "clocks": clk,
             "realtime_factor": value / (2 * FS / 1e9),
