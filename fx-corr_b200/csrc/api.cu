@@ -963,6 +963,18 @@ fxc_status fxc_sector_wait(fxc_scan* s, uint64_t sector_id, int32_t timeout_ms,
 
 // ---------------------------------------------------------------- helpers
 
+fxc_status fxc_host_alloc(uint64_t bytes, void** out) {
+  if (!out) return fail(FXC_EINVAL, "out is NULL");
+  *out = nullptr;
+  CK(cudaMallocHost(out, std::max<uint64_t>(bytes, 16)));
+  return FXC_OK;
+}
+
+fxc_status fxc_host_free(void* p) {
+  if (p) CK(cudaFreeHost(p));
+  return FXC_OK;
+}
+
 uint64_t fxc_bytes_per_frame(uint32_t fft, uint32_t bits) {
   return ((uint64_t)fft * bits + 7) / 8;
 }

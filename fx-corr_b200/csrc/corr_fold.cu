@@ -297,7 +297,9 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
       const int mP = tid - sP, mS = tid - sS;
       const int cP = mP & ((32 / bitsP) - 1), cS = mS & ((32 / bitsS) - 1);
       const uint32_t tbP = (uint32_t)((mP & lsbP) << (bitsP + 2));
-      const uint32_t tbS = 2048u + (uint32_t)((mS & lsbS) << (bitsS + 2));
+      // the secondary station enters odd frames negated (see sgn below)
+      const uint32_t tbS = 2048u + (uint32_t)((((uint32_t)mS & (uint32_t)lsbS) ^ (uint32_t)(it & 1u))
+                                              << (bitsS + 2));
       fold_station<false>(bitsP, splitP, wP, smem, sP, pos[cP], tbP, v, tid);
       fold_station<true>(bitsS, splitS, wS, smem, sS, pos[32 + cS], tbS, v, tid);
       dft16(v);
@@ -333,6 +335,13 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
       rq = cmul(mix, make_float2(cs, sn));
     }
 
+    // Rounding in the shared complex FFT leaks a fixed fraction (~1e-6) of
+    // each station's spectrum into the other's; summed over frames that
+    // would bias the cross-spectrum by ~1e-6 of the auto-spectra, i.e. by
+    // 1e-6/rho of a weakly correlated XCF.  Negating the secondary station's
+    // input on odd frames (undone exactly here) alternates the sign of that
+    // leak, so it cancels in the sum instead of accumulating.
+    const float sgn = (it & 1u) ? -1.0f : 1.0f;
     float2 prim[2 * kUnits];
 #pragma unroll
     for (int i = 0; i < kUnits; ++i) {
@@ -352,16 +361,16 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
       const float2 zm = j == 0 ? zjh : csub(c, wd);
       // primary = real part: P[k] = (Z[k] + conj Z[N-k]), S[k] = -i (Z[k] - conj Z[N-k])
       prim[2 * i] = make_float2(zj.x + zmn.x, zj.y - zmn.y);
-      Q[j] = make_float2(zj.y + zmn.y, zmn.x - zj.x);
+      Q[j] = make_float2(sgn * (zj.y + zmn.y), sgn * (zmn.x - zj.x));
       prim[2 * i + 1] = make_float2(zm.x + zjh.x, zm.y - zjh.y);
-      Q[kN / 2 - j] = make_float2(zm.y + zjh.y, zjh.x - zm.x);
+      Q[kN / 2 - j] = make_float2(sgn * (zm.y + zjh.y), sgn * (zjh.x - zm.x));
     }
     float2 prim_q = make_float2(0.f, 0.f);
     if (tid == 0) {  // bin N/4: Z[N/4] = Y[N/4] - i Y[3N/4], Z[3N/4] = Y[N/4] + i Y[3N/4]
       const float2 a = Y[kN / 4], b = Y[3 * kN / 4];
       const float2 zq = make_float2(a.x + b.y, a.y - b.x), zq3 = make_float2(a.x - b.y, a.y + b.x);
       prim_q = make_float2(zq.x + zq3.x, zq.y - zq3.y);
-      Q[kN / 4] = make_float2(zq.y + zq3.y, zq3.x - zq.x);
+      Q[kN / 4] = make_float2(sgn * (zq.y + zq3.y), sgn * (zq3.x - zq.x));
     }
     __syncthreads();
 

@@ -142,8 +142,12 @@ corr_kernel(const CorrParams p) {
     const int s2 = valid ? finfo[g].s2 : 0;
     const PackedStation pa{w1 + g * (bpf1 / 4), lv, (uint32_t)p.st[0].bits,
                            (1u << p.st[0].bits) - 1u, p.st[0].lsb ? 1 : 0, s1};
+    // MODE_CORR: station 2 enters odd frames negated, undone in the
+    // accumulation, so that the shared FFT's cross-station rounding leak
+    // alternates in sign and cancels over frames instead of biasing the XCF
     const PackedStation pb{w2 + g * (bpf2 / 4), lv + 256, (uint32_t)p.st[1].bits,
-                           (1u << p.st[1].bits) - 1u, p.st[1].lsb ? 1 : 0, s2};
+                           (1u << p.st[1].bits) - 1u, p.st[1].lsb ? 1 : 0, s2,
+                           MODE == MODE_CORR ? (uint32_t)(frame_local & 1u) : 0u};
 
     if constexpr (MODE == MODE_DECODE) {
       if (valid) {
@@ -208,6 +212,7 @@ corr_kernel(const CorrParams p) {
       const float2 rot_half = cmul(F.fr_mix, make_float2(cs, sn));
       __sincosf((float)T * F.dphi, &sn, &cs);
       const float2 rstep = make_float2(cs, sn);
+      const float sg = ((it * FPC + f) & 1u) ? -1.0f : 1.0f;  // station 2 sign of this frame
       auto bin_acc = [&](int bin, float2 r, float* a) {
         const float2 u = Z[bin], w = Z[(N - bin) & (N - 1)];
         if (p.grid == 0) {
@@ -217,7 +222,7 @@ corr_kernel(const CorrParams p) {
           if (inov) {
             const int i2 = bin + sb;
             const float2 c = Z[i2], d = Z[(N - i2) & (N - 1)];
-            const float2 q2 = make_float2(c.y + d.y, d.x - c.x);  // 2*S2[i2]
+            const float2 q2 = make_float2(sg * (c.y + d.y), sg * (d.x - c.x));  // 2*S2[i2]
             if (want_acf) a[1] += cnorm2(q2);
             if (want_xcf) {
               const float2 x = cmul(cmulc(p1, q2), r);
@@ -227,7 +232,7 @@ corr_kernel(const CorrParams p) {
           }
         } else {
           const bool inov = bin >= a2s && bin < a2s + ov;
-          const float2 p2 = make_float2(u.y + w.y, w.x - u.x);  // 2*S2[bin]
+          const float2 p2 = make_float2(sg * (u.y + w.y), sg * (w.x - u.x));  // 2*S2[bin]
           if (want_acf && (!ov_only || inov)) a[1] += cnorm2(p2);
           if (inov) {
             const int i1 = bin - sb;

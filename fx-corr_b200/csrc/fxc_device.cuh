@@ -375,6 +375,7 @@ struct PackedStation {
   uint32_t bits, mask;
   int lsb;                // negate odd samples (LSB -> USB, src/utils.rs:196-197)
   int shift;              // integer shift of this frame, clamped to [-N, N]
+  uint32_t flip = 0;      // 1: negate the whole frame (first_pass_packed only)
 };
 
 // Sample m of the frame (0 <= m < N): b-bit code taken LSB-first from the
@@ -401,7 +402,8 @@ __device__ __forceinline__ void station_inputs(const PackedStation& p, float2 (&
   static_assert(T1 % SPW == 0, "frame stride is a whole number of words");
   const int m0 = t - p.shift;
   const uint32_t bitpos = (uint32_t)(m0 & (SPW - 1)) * BITS;
-  const uint32_t sign = (uint32_t)(m0 & p.lsb) << 31;  // odd samples of LSB input are negated
+  // odd samples of LSB input are negated; `flip` negates the frame
+  const uint32_t sign = ((uint32_t)(m0 & p.lsb) ^ p.flip) << 31;
   const int w0 = m0 >> LOG2_SPW;                 // floor division (m0 may be negative)
   if (p.shift == 0) {
     const uint32_t* w = p.words + w0;

@@ -59,7 +59,10 @@ __global__ void decode_global_kernel(const LargeParams p, uint64_t f0, uint64_t 
     const float b = sample_at(p.st[1].raw + f * p.st[1].bpf, p.st[1].bits, p.st[1].shkind,
                               lut + 1024, lv + 256, p.st[1].lsb, k - F.s2, n);
     if (z) {
-      z[idx] = make_float2(a, b);
+      // station 2 enters odd frames negated (undone after the FFT), so the
+      // shared FFT's cross-station rounding leak alternates in sign and
+      // cancels over frames instead of biasing the cross-spectrum
+      z[idx] = make_float2(a, (f & 1u) ? -b : b);
     } else {
       x1o[f * n + k] = a / p.st[0].scale;
       x2o[f * n + k] = b / p.st[1].scale;
@@ -155,6 +158,7 @@ __global__ void acc_global_kernel(const LargeParams p, const float2* __restrict_
     float sn, cs;
     sincosf(fmaf((float)(bin - a_gs), F.dphi, F.phi0), &sn, &cs);
     const float2 r = cmul(F.fr_mix, make_float2(cs, sn));
+    const float sg = ((f0 + fl) & 1u) ? -1.0f : 1.0f;  // station 2 sign of this frame
     const float2 u = zi(Zf, bin), w = zi(Zf, N - bin);
     if (p.grid == 0) {
       const bool inov = bin >= a1s && bin < a1e;
@@ -163,7 +167,7 @@ __global__ void acc_global_kernel(const LargeParams p, const float2* __restrict_
       if (inov) {
         const int i2 = bin + sb;
         const float2 c = zi(Zf, i2), d = zi(Zf, N - i2);
-        const float2 q2 = make_float2(c.y + d.y, d.x - c.x);
+        const float2 q2 = make_float2(sg * (c.y + d.y), sg * (d.x - c.x));
         if (want_acf) a[1] += (double)cnorm2(q2);
         if (want_xcf) {
           const float2 x = cmul(cmulc(p1, q2), r);
@@ -173,7 +177,7 @@ __global__ void acc_global_kernel(const LargeParams p, const float2* __restrict_
       }
     } else {
       const bool inov = bin >= a2s && bin < a2s + ov;
-      const float2 p2 = make_float2(u.y + w.y, w.x - u.x);
+      const float2 p2 = make_float2(sg * (u.y + w.y), sg * (w.x - u.x));
       if (want_acf && (!ov_only || inov)) a[1] += (double)cnorm2(p2);
       if (inov) {
         const int i1 = bin - sb;
@@ -210,7 +214,8 @@ __global__ void split_global_kernel(const LargeParams p, const float2* __restric
     const int kn = (N - k) & (N - 1);
     const float2 a = Zf[(k % C) * M + k / C], b = Zf[(kn % C) * M + kn / C];
     s1[(f0 + fl) * H + k] = make_float2(u1 * (a.x + b.x), u1 * (a.y - b.y));
-    s2[(f0 + fl) * H + k] = make_float2(u2 * (a.y + b.y), -u2 * (a.x - b.x));
+    const float v2 = ((f0 + fl) & 1u) ? -u2 : u2;  // undo the odd-frame negation
+    s2[(f0 + fl) * H + k] = make_float2(v2 * (a.y + b.y), -v2 * (a.x - b.x));
   }
 }
 

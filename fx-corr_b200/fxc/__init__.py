@@ -35,6 +35,7 @@ EXPORTS = [
     "fxc_level_power", "fxc_normalize", "fxc_bytes_per_frame", "fxc_probe_fp32_peak",
     "fxc_scan_set_profiling", "fxc_scan_profile", "fxc_sector_run_device_noalloc",
     "fxc_server_create", "fxc_server_submit", "fxc_server_wait", "fxc_server_destroy",
+    "fxc_host_alloc", "fxc_host_free",
 ]
 NOALLOC_MAX_FRAMES = 32768
 
@@ -161,6 +162,8 @@ def lib():
         "fxc_server_submit": ([vp, C.POINTER(JobC), C.POINTER(C.c_uint64)], st),
         "fxc_server_wait": ([vp, C.c_uint64, C.c_int32, C.POINTER(JobStats)], st),
         "fxc_server_destroy": ([vp], st),
+        "fxc_host_alloc": ([C.c_uint64, C.POINTER(vp)], st),
+        "fxc_host_free": ([vp], st),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

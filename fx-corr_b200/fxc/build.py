@@ -74,5 +74,40 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+CLI_DIR = PKG.parent / "cli"
+BIN_DIR = PKG.parent / "bin"
+CLI_TOOLS = ("yi-corr", "yi-acf", "yi-xcf", "yi-phasedarray")
+
+
+def build_cli(force: bool = False, verbose: bool = False) -> Path:
+    """The yi-* tools: one C++ binary (mode from argv[0]) linked against
+    libfxc.so by rpath, plus the three other names as symlinks."""
+    build(force=force, verbose=verbose)
+    BIN_DIR.mkdir(exist_ok=True)
+    out = BIN_DIR / CLI_TOOLS[0]
+    srcs = sorted(CLI_DIR.glob("*.cpp"))
+    deps = srcs + sorted(CLI_DIR.glob("*.h")) + [INCLUDE / "fxc.h", LIB]
+    if force or _stale(out, deps):
+        tmp = out.with_name(out.name + f".tmp{os.getpid()}")
+        cxx = os.environ.get("CXX") or shutil.which("g++") or "g++"
+        cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", str(INCLUDE), "-I", str(CLI_DIR),
+               *map(str, srcs), "-o", str(tmp), "-L", str(LIB_DIR), "-lfxc",
+               "-Wl,-rpath,$ORIGIN/../fxc/lib", "-lpthread"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"g++ failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+        os.replace(tmp, out)
+    for name in CLI_TOOLS[1:]:
+        link = BIN_DIR / name
+        if not link.is_symlink():
+            if link.exists():
+                link.unlink()
+            link.symlink_to(CLI_TOOLS[0])
+    return out
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
+    print(build_cli(force="--force" in sys.argv, verbose=True))

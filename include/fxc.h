@@ -249,6 +249,12 @@ FXC_API fxc_status fxc_server_wait(fxc_server* sv, uint64_t job_id, int32_t time
 /* Finishes the queued jobs, then releases the slots. */
 FXC_API fxc_status fxc_server_destroy(fxc_server* sv);
 
+/* Page-locked host memory for sector buffers (no reference counterpart: the
+ * reference reads into pageable Vec<u8>, src/main.rs:2133-2147); copies from
+ * it overlap device work. */
+FXC_API fxc_status fxc_host_alloc(uint64_t bytes, void** out);
+FXC_API fxc_status fxc_host_free(void* p);
+
 /* Stage entry points, for parity tests of the individual steps. */
 /* Per-frame delay model on the device (src/main.rs:184-241). */
 FXC_API fxc_status fxc_delay_entries_device(fxc_scan* s, uint64_t first_frame, uint64_t nf,

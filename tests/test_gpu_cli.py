@@ -1,0 +1,191 @@
+"""The yi-* command line end to end on the GPU: XML schedule + .raw files in,
+.cor (and phased .raw) out.  The spectra a tool writes must be the ones the
+library computes for the configuration the reference's run_once derives
+(bit for bit), and within tolerance of the FP64 oracle after the .cor
+normalisation; the XCF phase slope recovers the synthetic lag."""
+from __future__ import annotations
+
+import math
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from _cases import spectral_errors, to_fxc, xcf_floor
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parents[1]
+BIN = ROOT / "fx-corr_b200" / "bin"
+FS, FFT, OBS_HZ = 32e6, 1024, 8.4e9
+CLOCK2_S, CLOCK2_RATE = 1.5e-6, 1e-12
+LAG = 123.4
+EPOCH, TAG = "2024/043 15:52:00", "2024043155200"
+IDENT = ",".join(str(31 - i) for i in range(32))
+
+
+def write_case(d: Path, seconds=1.1, seed=2024):
+    """Schedule (zero-length baseline, so the geometric terms vanish) and two
+    .raw files: 2-bit +-1/+-3, common component at rho=0.05 delayed by LAG
+    samples plus the 1.5 us clock offset at station 2."""
+    xml = f"""<?xml version="1.0"?>
+<schedule>
+  <station key="A"><name>YAMAGU32</name><pos-x>-3502544.587</pos-x><pos-y>3950966.235</pos-y>
+    <pos-z>3566381.192</pos-z><terminal>t1</terminal></station>
+  <station key="B"><name>YAMAGU34</name><pos-x>-3502544.587</pos-x><pos-y>3950966.235</pos-y>
+    <pos-z>3566381.192</pos-z><terminal>t2</terminal></station>
+  <clock key="A"><delay>0</delay><rate>0</rate></clock>
+  <clock key="B"><delay>{CLOCK2_S}</delay><rate>{CLOCK2_RATE}</rate></clock>
+  <terminal name="t1"><speed>{int(FS)}</speed><bit>2</bit><level>-3,-1,+1,+3</level></terminal>
+  <terminal name="t2"><speed>{int(FS)}</speed><bit>2</bit><level>-3,-1,+1,+3</level></terminal>
+  <shuffle key="A">{IDENT}</shuffle>
+  <shuffle key="B">{IDENT}</shuffle>
+  <source name="SRC"><ra>12h00m00.0s</ra><dec>+30d00m00.0s</dec></source>
+  <stream><label>cli</label><frequency>{int(OBS_HZ)}</frequency><fft>{FFT}</fft></stream>
+  <process><epoch>{EPOCH}</epoch><length>1</length><object>SRC</object>
+    <stations>AB</stations></process>
+</schedule>
+"""
+    (d / "sched.xml").write_text(xml)
+    raw = d / "raw"
+    raw.mkdir()
+    n = int(seconds * FS)
+    n -= n % FFT
+    x1, x2 = oracle.synth_station_pair(n, seed, rho=0.05, delay_samples=LAG + CLOCK2_S * FS)
+    lv = oracle.default_levels(2)
+    ident = list(range(32))
+    (raw / f"YAMAGU32_{TAG}.raw").write_bytes(oracle.encode_station(x1, 2, lv, ident, False).tobytes())
+    (raw / f"YAMAGU34_{TAG}.raw").write_bytes(oracle.encode_station(x2, 2, lv, ident, False).tobytes())
+    return d / "sched.xml", raw
+
+
+def run_tool(name, *args, cwd=None):
+    r = subprocess.run([str(BIN / name), *map(str, args)], cwd=cwd, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, (r.returncode, r.stdout[-2000:], r.stderr[-2000:])
+    return r
+
+
+def read_cor(path: Path, fft: int):
+    b = path.read_bytes()
+    assert b[:4] == bytes([0x83, 0xF9, 0xA2, 0x3E])
+    assert int.from_bytes(b[4:8], "little") == 0x01030000
+    nsec = int.from_bytes(b[28:32], "little", signed=True)
+    rec = 128 + fft // 2 * 8
+    assert len(b) == 256 + nsec * rec
+    spec = [np.frombuffer(b[256 + k * rec + 128:256 + (k + 1) * rec], np.float32)
+            .reshape(-1, 2) for k in range(nsec)]
+    return nsec, [s[:, 0] + 1j * s[:, 1] for s in spec]
+
+
+def derived_scan(total_f, bits_out=2, products=oracle.PROD_ACF | oracle.PROD_XCF):
+    """The configuration run_once derives for write_case's schedule
+    (src/main.rs:1063-1673): zero geometry, station 2 read 48 samples later,
+    clock rate as the only delay rate."""
+    seek2 = round(CLOCK2_S * FS)
+    d_seek = seek2 / FS
+    frame_dt = FFT / FS
+    n_table = max(math.ceil(total_f * frame_dt), 1) + 1
+    delay = dict(time_offset_s=0.0, clock2_delay_s=CLOCK2_S, clock2_rate_sps=CLOCK2_RATE,
+                 d_seek=d_seek, net_d1_base=(0.0 + 0.0 + 0.0 / FS) + CLOCK2_S - d_seek,
+                 total_rate1_base=(0.0 + 0.0 + 0.0) / OBS_HZ + CLOCK2_RATE,
+                 total_accel1_base=-0.0, lo1_hz=OBS_HZ, lo2_hz=OBS_HZ)
+    scan = oracle.Scan(fft=FFT, fs=FS, bits1=2, bits2=2, levels1=oracle.default_levels(2),
+                       levels2=oracle.default_levels(2), shuffle1=list(range(32)),
+                       shuffle2=list(range(32)), lsb1=False, lsb2=False, band=(0, 0, 512, 0),
+                       grid=0, products=products, delay=delay, geom_table=np.zeros(n_table))
+    return scan, seek2 * 2 // 8
+
+
+def test_yi_corr_end_to_end(tmp_path, engine):
+    sched, raw = write_case(tmp_path)
+    out = tmp_path / "cor"
+    run_tool("yi-corr", "--sc", sched, "--raw", raw, "--cor", out, "--sideband", "USB")
+    files = {p.name: p for p in out.glob("*.cor")}
+    names = [f"YAMAGU32_YAMAGU32_{TAG}_cli.cor", f"YAMAGU32_YAMAGU34_{TAG}_cli.cor",
+             f"YAMAGU34_YAMAGU34_{TAG}_cli.cor"]
+    assert sorted(files) == sorted(names)
+    total_f = int(1.0 * FS / FFT)
+    nsec, s11 = read_cor(files[names[0]], FFT)
+    _, s12 = read_cor(files[names[1]], FFT)
+    _, s22 = read_cor(files[names[2]], FFT)
+    assert nsec == 1
+
+    scan, off2 = derived_scan(total_f)
+    b = scan.bpf(2)
+    r1 = np.fromfile(raw / f"YAMAGU32_{TAG}.raw", np.uint8)[: total_f * b]
+    r2 = np.fromfile(raw / f"YAMAGU34_{TAG}.raw", np.uint8)[off2: off2 + total_f * b]
+    # the library on the same configuration and bytes: identical numbers
+    s = engine.open_scan(to_fxc(scan))
+    sid = s.submit(r1, r2, total_f, 0)
+    lib = s.wait(sid)
+    s.close()
+    p = float(np.mean(np.square(oracle.default_levels(2))))
+    inv = 1.0 / (0.5 * p * total_f * float(FFT) ** 2)
+    for got, ref in ((s11[0], lib["acf11"]), (s22[0], lib["acf22"]), (s12[0], lib["xcf"])):
+        want = (ref[: FFT // 2] * inv).astype(np.complex64)
+        assert np.array_equal(got.astype(np.complex64), want)
+    # and the FP64 oracle within the stated tolerance
+    ref = oracle.fp64_sector_corr(scan, r1, r2, total_f, first_frame=0)
+    for got, key in ((s11[0], "acf11"), (s22[0], "acf22")):
+        rel, ph, ab = spectral_errors(got, ref[key][: FFT // 2] * inv)
+        assert rel < 1e-5, (key, rel)
+    rel, ph, ab = spectral_errors(s12[0], ref["xcf"][: FFT // 2] * inv,
+                                  xcf_floor(ref, total_f)[: FFT // 2] * inv)
+    assert rel < 1e-5 and ph < 1e-4, (rel, ph)
+    # XCF phase slope across the band: the lag left after the clock correction
+    k = np.arange(20, 490)
+    phase = np.unwrap(np.angle(s12[0][k]))
+    slope = np.polyfit(k, phase, 1)[0]
+    lag = abs(slope) * FFT / (2 * np.pi)
+    assert abs(lag - LAG) < 0.5, lag
+
+
+def test_yi_acf_xcf_and_phased(tmp_path, engine):
+    sched, raw = write_case(tmp_path, seconds=1.05, seed=7)
+    total_f = int(1.0 * FS / FFT)
+    out = tmp_path / "cor"
+    run_tool("yi-acf", "--sc", sched, "--raw", raw, "--cor", out, "--sideband", "USB")
+    acf = sorted(p.name for p in out.glob("*.cor"))
+    assert acf == [f"YAMAGU32_YAMAGU32_{TAG}_cli.cor", f"YAMAGU34_YAMAGU34_{TAG}_cli.cor"]
+    out2 = tmp_path / "cor2"
+    run_tool("yi-xcf", "--sc", sched, "--raw", raw, "--cor", out2, "--sideband", "USB")
+    assert sorted(p.name for p in out2.glob("*.cor")) == [f"YAMAGU32_YAMAGU34_{TAG}_cli.cor"]
+    # phased: .raw and phased .cor land in the working directory
+    work = tmp_path / "work"
+    work.mkdir()
+    run_tool("yi-phasedarray", "--sc", sched, "--raw", raw, "--sideband", "USB", cwd=work)
+    praw = work / f"YAMAGU66_{TAG}.raw"
+    pcor = work / f"YAMAGU66_YAMAGU66_{TAG}_phasedarray.cor"
+    assert praw.exists() and pcor.exists()
+    scan, off2 = derived_scan(total_f, products=oracle.PROD_PHASED | oracle.PROD_RAW)
+    b = scan.bpf(2)
+    r1 = np.fromfile(raw / f"YAMAGU32_{TAG}.raw", np.uint8)[: total_f * b]
+    r2 = np.fromfile(raw / f"YAMAGU34_{TAG}.raw", np.uint8)[off2: off2 + total_f * b]
+    s = engine.open_scan(to_fxc(scan))
+    sid = s.submit(r1, r2, total_f, 0)
+    lib = s.wait(sid)
+    s.close()
+    assert praw.read_bytes() == lib["raw"].tobytes()
+    nsec, sph = read_cor(pcor, FFT)
+    p = float(np.mean(np.square(oracle.default_levels(2))))
+    inv = 1.0 / (0.5 * max(p + p, 1e-12) * total_f * float(FFT) ** 2)
+    assert np.array_equal(sph[0].astype(np.complex64),
+                          (lib["phased"][: FFT // 2] * inv).astype(np.complex64))
+
+
+def test_multi_process_schedule(tmp_path):
+    """Two <process> entries run sequentially, one output set each."""
+    sched, raw = write_case(tmp_path, seconds=2.2, seed=3)
+    x = sched.read_text().replace(
+        "</schedule>",
+        f"  <process><epoch>{EPOCH}</epoch><skip>1</skip><length>2</length><object>SRC</object>"
+        "<stations>AB</stations></process>\n</schedule>")
+    sched.write_text(x)
+    out = tmp_path / "cor"
+    r = run_tool("yi-xcf", "--sc", sched, "--raw", raw, "--cor", out, "--sideband", "USB")
+    assert "Processing all scans sequentially: 2 process entries" in r.stdout
+    names = sorted(p.name for p in out.glob("*.cor"))
+    assert names == [f"YAMAGU32_YAMAGU34_{TAG}_cli.cor", f"YAMAGU32_YAMAGU34_2024043155201_cli.cor"]

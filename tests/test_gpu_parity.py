@@ -202,6 +202,21 @@ def test_sector_vs_fp64(engine, kw, nf):
     s.close()
 
 
+@pytest.mark.parametrize("fft,nf", [(1024, 20000), (4096, 6000), (8192, 3000), (16384, 600)])
+def test_weak_correlation_long_integration(engine, fft, nf):
+    """rho = 0.01 over thousands of frames: the shared complex FFT's
+    cross-station rounding leak must not accumulate into the cross-spectrum
+    (it would reach ~1e-6 * sqrt(nf) of the XCF noise floor)."""
+    scan = make_scan(fft=fft, fs=512e6, delay=DELAY, shuffle="generic", lsb1=True,
+                     band=(8, 0, fft // 2 - 8, 8))
+    r1, r2 = signal_raw(scan, nf, seed=fft + 1, rho=0.01, delay_samples=3.3)
+    s = engine.open_scan(to_fxc(scan))
+    got = s.sector_device(dev(r1), dev(r2), nf, first_frame=5)
+    ref = oracle.fp64_sector_corr(scan, r1, r2, nf, first_frame=5)
+    assert_sector_close(got, ref, scan, f"rho=0.01 fft={fft} nf={nf}", nf=nf, ref_acf=ref)
+    s.close()
+
+
 @pytest.mark.parametrize("d1", [-2.3e-6, 5.1e-6, 1.7e-5])
 def test_sector_large_shift(engine, d1):
     """Integer shifts beyond N/16 (and beyond N: an all-zero station frame)."""
