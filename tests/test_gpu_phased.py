@@ -2,11 +2,13 @@
 against the FP64 oracle: the phased power spectrum within the stated
 tolerance, and the re-quantised phased .raw frames code-for-code except for
 samples that lie within rounding distance of a decision boundary."""
+import dataclasses
+
 import numpy as np
 import pytest
 
 import oracle
-from _cases import assert_spectra_close, make_scan, signal_raw, to_fxc
+from _cases import assert_spectra_close, make_scan, signal_raw, spectral_errors, to_fxc
 
 pytestmark = pytest.mark.gpu
 
@@ -91,3 +93,41 @@ def test_phased_host_path(engine):
         assert np.array_equal(a[k], b[k]), k
     assert np.any(a["acf11"]) and np.any(a["phased"])
     s.close()
+
+
+@pytest.mark.parametrize("fft,lsb", [(4096, False), (8192, True)])
+def test_phased_raw_round_trip(engine, fft, lsb):
+    """The phased .raw decodes with the same plan (ant1's levels and shuffle,
+    LSB when both inputs are LSB, src/main.rs:1093, 2391-2412) into a stream
+    whose auto-spectrum is the phased power spectrum's shape: the GPU decode +
+    ACF of the GPU-written frames equals the FP64 oracle's on the same bytes,
+    and its normalised shape follows the phased power."""
+    delay = dict(net_d1_base=2.1e-7, total_rate1_base=1.1e-6, lo1_hz=8.4e9, lo2_hz=8.4e9)
+    scan = make_scan(fft=fft, fs=512e6, delay=delay, shuffle="generic", lsb1=lsb, lsb2=lsb,
+                     products=oracle.PROD_PHASED | oracle.PROD_RAW, band=(0, 0, fft // 2, 0))
+    nf = 120
+    r1, r2 = signal_raw(scan, nf, seed=fft + 11, rho=0.6, delay_samples=1.5,
+                        tone_bin=fft // 5)
+    s = engine.open_scan(to_fxc(scan))
+    ph = s.sector_device(dev(r1), dev(r2), nf, first_frame=0)
+    s.close()
+    raw = ph["raw"]
+    # the round-trip scan: both "stations" are the phased stream, no delay
+    rt = make_scan(fft=fft, fs=512e6, bits1=scan.bits_out, bits2=scan.bits_out,
+                   levels1=list(scan.levels1), levels2=list(scan.levels1), shuffle="identity",
+                   lsb1=lsb, lsb2=lsb, products=oracle.PROD_ACF, delay={})
+    rt = dataclasses.replace(rt, shuffle1=list(scan.shuffle1), shuffle2=list(scan.shuffle1))
+    s2 = engine.open_scan(to_fxc(rt))
+    got = s2.sector_device(dev(raw), dev(raw), nf, first_frame=0)
+    s2.close()
+    ref = oracle.fp64_sector_corr(rt, raw, raw, nf, first_frame=0)
+    assert_spectra_close(got["acf11"], ref["acf11"], "round-trip acf")
+    # the second copy (overlap bins only) sees the same stream
+    rel, _, _ = spectral_errors(got["acf22"][: fft // 2], got["acf11"][: fft // 2])
+    assert rel < 1e-5, rel
+    # shape: the re-quantised stream's spectrum follows the phased power
+    a = got["acf11"][1:fft // 2] / np.mean(got["acf11"][1:fft // 2])
+    p = ph["phased"][1:fft // 2] / np.mean(ph["phased"][1:fft // 2])
+    assert np.corrcoef(a, p)[0, 1] > 0.9
+    k = fft // 5  # the injected tone survives the round trip
+    assert a[k - 1] > 1.8 * np.median(a) and p[k - 1] > 1.8 * np.median(p)
