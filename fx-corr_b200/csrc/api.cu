@@ -263,8 +263,6 @@ fxc_status validate_cfg(const fxc_scan_cfg* c) {
   if (!(n == 1024 || n == 2048 || n == 4096 || n == 8192 || n == 16384 || n == 32768 ||
         n == 65536))
     return fail(FXC_EUNSUPPORTED, "fft_len %u not supported (powers of two 1024..65536)", n);
-  if (n > 8192 && (c->products & (FXC_PROD_PHASED | FXC_PROD_RAW)))
-    return fail(FXC_EUNSUPPORTED, "phased products need fft_len <= 8192 in this build");
   for (uint32_t b : {c->bits1, c->bits2})
     if (!(b == 1 || b == 2 || b == 4 || b == 8))
       return fail(FXC_EUNSUPPORTED, "bits %u not supported (1, 2, 4, 8)", b);
@@ -329,27 +327,6 @@ LargeParams large_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2
 // FFT lengths above 8192: batches of frames through the global-memory path,
 // per-frame-group f64 partials, then the fixed-order reduction.  The frame
 // records of the sector must already be staged.
-fxc_status run_large_corr(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
-                          double* d_acc, cudaStream_t st) {
-  const uint32_t h = s->h;
-  const LargeParams p = large_params(s, r1, r2);
-  const int groups = (int)std::min<uint64_t>((uint64_t)kLargeGroups, s->big_frames);
-  bool first = true;
-  for (uint64_t f0 = 0; f0 < nf; f0 += s->big_frames) {
-    const uint64_t nb = std::min(s->big_frames, nf - f0);
-    CK(launch_large_fft(p, f0, nb, s->d_big[0], s->d_big[1], s->eng->sm_count, st));
-    CK(launch_large_acc(p, s->d_big[1], f0, nb, groups, first ? 1 : 0, s->d_partials, st));
-    s->all_launches += 4;
-    first = false;
-  }
-  const double u1 = 1.0 / s->scale[0], u2 = 1.0 / s->scale[1];
-  CK(launch_reduce(s->d_partials, groups, (int)h, 0.25 * u1 * u1, 0.25 * u2 * u2, 0.25 * u1 * u2,
-                   d_acc, st));
-  s->all_launches += 1;
-  s->kernel_launches += 1;
-  return FXC_OK;
-}
-
 PhasedParams phased_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
                            uint64_t first, uint8_t* d_raw_out) {
   PhasedParams p{};
@@ -381,6 +358,50 @@ PhasedParams phased_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* 
   return p;
 }
 
+// FFT lengths above 8192: per batch of frames one decode + four-step FFT,
+// then the ACF/XCF accumulation and/or the phased synthesis (+ inverse FFT and
+// re-quantisation) on the same spectra; fixed-order reductions at the end.
+fxc_status run_large(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
+                     uint64_t first, double* d_acc, uint8_t* d_raw_out, bool corr, bool phased,
+                     cudaStream_t st) {
+  const uint32_t h = s->h;
+  const LargeParams p = large_params(s, r1, r2);
+  PhasedParams pp{};
+  if (phased) pp = phased_params(s, r1, r2, nf, first, d_raw_out);
+  const int groups = (int)std::min<uint64_t>((uint64_t)kLargeGroups, s->big_frames);
+  double* part_ph = s->d_partials + (uint64_t)kLargeGroups * 4 * h;
+  bool first_batch = true;
+  for (uint64_t f0 = 0; f0 < nf; f0 += s->big_frames) {
+    const uint64_t nb = std::min(s->big_frames, nf - f0);
+    CK(launch_large_fft(p, f0, nb, s->d_big[0], s->d_big[1], s->eng->sm_count, st));
+    s->all_launches += 3;
+    if (corr) {
+      CK(launch_large_acc(p, s->d_big[1], f0, nb, groups, first_batch ? 1 : 0, s->d_partials, st));
+      s->all_launches += 1;
+    }
+    if (phased) {
+      CK(launch_large_phased(p, pp, s->d_big[0], s->d_big[1], f0, nb, groups, first_batch ? 1 : 0,
+                             part_ph, s->eng->sm_count, st));
+      s->all_launches += pp.want_raw ? 4 : 1;
+    }
+    first_batch = false;
+  }
+  if (corr) {
+    const double u1 = 1.0 / s->scale[0], u2 = 1.0 / s->scale[1];
+    CK(launch_reduce(s->d_partials, groups, (int)h, 0.25 * u1 * u1, 0.25 * u2 * u2,
+                     0.25 * u1 * u2, d_acc, st));
+    s->all_launches += 1;
+    s->kernel_launches += 1;
+  } else {
+    CK(cudaMemsetAsync(d_acc, 0, sizeof(double) * 5 * h, st));
+  }
+  if (phased) {
+    CK(launch_reduce_phased(part_ph, groups, (int)h, d_acc, st));
+    s->all_launches += 1;
+  }
+  return FXC_OK;
+}
+
 fxc_status run_sector_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
                              uint64_t first, double* d_acc, uint8_t* d_raw_out, cudaStream_t st) {
   const uint32_t h = s->h;
@@ -396,7 +417,7 @@ fxc_status run_sector_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, 
   fxc_status fst = stage_frame_info(s, first, nf, st);
   if (fst != FXC_OK) return fst;
   s->all_launches += 1;
-  if (s->n > 8192) return run_large_corr(s, r1, r2, nf, d_acc, st);
+  if (s->n > 8192) return run_large(s, r1, r2, nf, first, d_acc, d_raw_out, corr, phased, st);
   if (!corr) {
     CK(cudaMemsetAsync(d_acc, 0, sizeof(double) * 5 * h, st));
   } else {
@@ -492,7 +513,8 @@ fxc_status scan_bind(fxc_scan* s, const fxc_scan_cfg* cfg) {
   const uint32_t n = cfg->fft_len, h = n / 2 + 1;
   const uint64_t maxg = n > 8192 ? (uint64_t)kLargeGroups
                                  : (uint64_t)e->sm_count * (uint64_t)corr_ctas_per_sm(n);
-  const uint64_t pel = maxg * 4 * h;
+  // N > 8192: [group][4][H] correlation partials, then [group][H] phased partials
+  const uint64_t pel = maxg * (n > 8192 ? 5 : 4) * h;
   const uint64_t bigf = n > 8192 ? (uint64_t)large_batch_frames(n) : 0;
   const uint64_t bige = bigf * (uint64_t)n;
   const uint64_t tlen = cfg->delay.geom_table ? cfg->delay.geom_len : 0;

@@ -644,6 +644,37 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Nearest level, first index wins ties (utils.rs:384-389).  For tables with
+// more than 16 entries that are strictly monotonic (flag set by the host) a
+// binary search finds the bracket and the exact f32 comparison runs over a
+// window of +-2 entries around it.
+__device__ __forceinline__ uint32_t nearest_level(float x, const float* __restrict__ ql, int n,
+                                                  int monotonic) {
+  int lo = 0, hi = n;
+  if (monotonic != 0 && n > 16) {
+    // ascending (monotonic > 0) or descending (< 0): find first index past x
+    int a = 0, b = n;
+    while (a < b) {
+      const int m = (a + b) >> 1;
+      const bool past = monotonic > 0 ? (ql[m] > x) : (ql[m] < x);
+      if (past) b = m;
+      else a = m + 1;
+    }
+    lo = max(0, a - 2);
+    hi = min(n, a + 2);
+  }
+  uint32_t best = (uint32_t)lo;
+  float min_err = 3.40282347e38f;
+  for (int i = lo; i < hi; ++i) {
+    const float err = fabsf(x - ql[i]);
+    if (err < min_err) {
+      min_err = err;
+      best = (uint32_t)i;
+    }
+  }
+  return best;
+}
+
 // ------------------------------------------------------ staging layout
 
 constexpr int kStages = 2;

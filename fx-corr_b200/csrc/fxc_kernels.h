@@ -77,6 +77,12 @@ cudaError_t launch_large_fft(const LargeParams& p, uint64_t f0, uint64_t nb, flo
                              float2* buf1, int sms, cudaStream_t s);
 cudaError_t launch_large_acc(const LargeParams& p, const float2* Y, uint64_t f0, uint64_t nb,
                              int groups, int first_batch, double* part, cudaStream_t s);
+// Phased synthesis for the batch whose spectra are in buf1 (f64 |cb|^2 into
+// part[group][H]); with pp.want_raw also the inverse FFT (via buf0) and the
+// packed .raw frames.
+cudaError_t launch_large_phased(const LargeParams& p, const struct PhasedParams& pp, float2* buf0,
+                                float2* buf1, uint64_t f0, uint64_t nb, int groups,
+                                int first_batch, double* part, int sms, cudaStream_t s);
 cudaError_t launch_large_decode(const LargeParams& p, uint64_t f0, uint64_t nb, float* x1,
                                 float* x2, int sms, cudaStream_t s);
 cudaError_t launch_large_split(const LargeParams& p, const float2* Y, uint64_t f0, uint64_t nb,

@@ -219,6 +219,100 @@ __global__ void split_global_kernel(const LargeParams p, const float2* __restric
   }
 }
 
+// Phased synthesis per bin (src/main.rs:2254-2280) for FFT lengths above
+// 8192: each thread owns bin C*kk + q across its frame group; |cb|^2 goes to
+// the group's f64 partials and, for the .raw product, the Hermitian extension
+// of conj(cb) (cb[0].im = cb[N/2].im = 0) to W in natural order, so that the
+// forward FFT of W is N x the inverse real FFT of cb (src/utils.rs:60-66).
+__global__ void phased_global_kernel(const LargeParams p, const PhasedParams pp,
+                                     const float2* __restrict__ Y, uint64_t f0, uint64_t nb,
+                                     int first_batch, double* __restrict__ part,
+                                     float2* __restrict__ W) {
+  const int C = p.c, M = kLargeM, N = p.n, H = N / 2 + 1;
+  const int q = blockIdx.y;
+  const int kk = blockIdx.x * blockDim.x + threadIdx.x;
+  const int bin = C * kk + q;
+  if (kk >= M || bin > N / 2) return;
+  const int a1s = p.a1s, a1e = p.a1e, a2s = p.a2s, ov = a1e - a1s, sb = a2s - a1s;
+  const float u1 = 0.5f / p.st[0].scale, u2 = 0.5f / p.st[1].scale;
+  auto zi = [&](const float2* Zf, int k) {
+    k &= (N - 1);
+    return Zf[(k % C) * M + k / C];
+  };
+  double acc = 0.0;
+  const uint64_t groups = gridDim.z;
+  const uint64_t g0 = (blockIdx.z * nb) / groups, g1 = ((blockIdx.z + 1) * nb) / groups;
+  for (uint64_t fl = g0; fl < g1; ++fl) {
+    const float2* Zf = Y + fl * (uint64_t)N;
+    const FrameInfo& F = p.finfo[f0 + fl];
+    const float sg = ((f0 + fl) & 1u) ? -1.0f : 1.0f;  // station 2 sign of this frame
+    // spectrum of station s at its own bin k: unscaled, rotated by the
+    // station's fractional delay, Nyquist imaginary part zeroed, times fr_lo
+    auto station_bin = [&](int s, int k) -> float2 {
+      const float2 a = zi(Zf, k), b = zi(Zf, N - k);
+      float2 v = s == 0 ? make_float2(u1 * (a.x + b.x), u1 * (a.y - b.y))
+                        : make_float2(sg * u2 * (a.y + b.y), sg * u2 * (b.x - a.x));
+      float sn, cs;
+      sincosf((float)k * (s == 0 ? F.st1 : F.st2), &sn, &cs);
+      v = cmul(v, make_float2(cs, sn));
+      if (k == N / 2) v.y = 0.f;
+      return cmul(v, s == 0 ? F.fr_lo1 : F.fr_lo2);
+    };
+    float2 a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
+    if (p.grid == 0) {
+      a1 = station_bin(0, bin);
+      if (bin >= a1s && bin < a1e) a2 = station_bin(1, bin + sb);
+    } else {
+      a2 = station_bin(1, bin);
+      if (bin >= a2s && bin < a2s + ov) a1 = station_bin(0, bin - sb);
+    }
+    float2 cb = make_float2(a1.x * pp.w1 + a2.x * pp.w2, a1.y * pp.w1 + a2.y * pp.w2);
+    acc += (double)cnorm2(cb);
+    if (pp.want_raw) {
+      float2* wf = W + fl * (uint64_t)N;
+      if (bin == 0 || bin == N / 2) cb.y = 0.f;
+      wf[bin] = make_float2(cb.x, -cb.y);
+      if (bin != 0 && bin != N / 2) wf[N - bin] = cb;
+    }
+  }
+  double* d = part + (size_t)blockIdx.z * H + bin;
+  *d = (first_batch ? 0.0 : *d) + acc;
+}
+
+// Re-quantise and pack the phased time series (quantise_frame,
+// src/utils.rs:378-410): x[n] = Re(X[n]) / N in the row layout of the
+// FFT output, odd samples negated when both inputs are LSB, nearest of
+// ant1's levels, codes LSB-first, ant1's shuffle applied per word.
+__global__ void quant_global_kernel(const LargeParams p, const PhasedParams pp,
+                                    const float2* __restrict__ X, uint64_t f0, uint64_t nb) {
+  __shared__ float ql[256];
+  __shared__ uint32_t elut[1024];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) ql[i] = i < (int)pp.nqlevels ? pp.qlevels[i] : 0.f;
+  for (int i = threadIdx.x; i < 1024; i += blockDim.x) elut[i] = pp.enc_lut[i];
+  __syncthreads();
+  const int C = p.c, M = kLargeM, N = p.n;
+  const uint32_t spw = 32u / pp.bits_out, wpf = (uint32_t)N / spw;
+  const uint32_t qmask = (1u << pp.bits_out) - 1u;
+  const float inv_n = 1.0f / (float)N;
+  const uint64_t total = nb * (uint64_t)wpf;
+  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t fl = idx / wpf;
+    const uint32_t w = (uint32_t)(idx - fl * wpf);
+    const float2* Xf = X + fl * (uint64_t)N;
+    uint32_t word = 0;
+    for (uint32_t i = 0; i < spw; ++i) {
+      const int n = (int)(w * spw + i);
+      float x = Xf[(n % C) * M + n / C].x * inv_n;
+      if (pp.out_lsb && (n & 1)) x = -x;
+      word |= (nearest_level(x, ql, (int)pp.nqlevels, pp.qmonotonic) & qmask) << (i * pp.bits_out);
+    }
+    const uint32_t sw = elut[word & 255u] | elut[256 + ((word >> 8) & 255u)] |
+                        elut[512 + ((word >> 16) & 255u)] | elut[768 + (word >> 24)];
+    reinterpret_cast<uint32_t*>(pp.raw_out + (f0 + fl) * pp.bpf_out)[w] = sw;
+  }
+}
+
 // ------------------------------------------------------------- launchers
 
 int large_batch_frames(uint32_t n) {
@@ -232,11 +326,9 @@ static int grid_for(uint64_t work, int threads, int sms) {
   return (int)(g < (uint64_t)sms * 8 ? (g ? g : 1) : (uint64_t)sms * 8);
 }
 
-cudaError_t launch_large_fft(const LargeParams& p, uint64_t f0, uint64_t nb, float2* buf0,
-                             float2* buf1, int sms, cudaStream_t s) {
-  // decode -> buf0, DIF -> buf1, row FFTs in place on buf1
-  decode_global_kernel<<<grid_for(nb * p.n, 256, sms), 256, 0, s>>>(p, f0, nb, buf0, nullptr,
-                                                                     nullptr);
+// DIF over C columns (buf0 -> buf1), then the M-point row FFTs in place on buf1.
+static cudaError_t large_fft_core(const LargeParams& p, uint64_t nb, const float2* buf0,
+                                  float2* buf1, int sms, cudaStream_t s) {
   const uint64_t work = nb * kLargeM;
   switch (p.c) {
     case 2: dif_kernel<2><<<grid_for(work, 256, sms), 256, 0, s>>>(buf0, buf1, nb); break;
@@ -250,6 +342,30 @@ cudaError_t launch_large_fft(const LargeParams& p, uint64_t f0, uint64_t nb, flo
   if (e != cudaSuccess) return e;
   const uint64_t rows = nb * (uint64_t)p.c;
   kern<<<(unsigned)std::min<uint64_t>(rows, (uint64_t)sms), kLargeM / 16, smem, s>>>(buf1, rows);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_large_fft(const LargeParams& p, uint64_t f0, uint64_t nb, float2* buf0,
+                             float2* buf1, int sms, cudaStream_t s) {
+  // decode -> buf0, DIF -> buf1, row FFTs in place on buf1
+  decode_global_kernel<<<grid_for(nb * p.n, 256, sms), 256, 0, s>>>(p, f0, nb, buf0, nullptr,
+                                                                     nullptr);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return large_fft_core(p, nb, buf0, buf1, sms, s);
+}
+
+cudaError_t launch_large_phased(const LargeParams& p, const PhasedParams& pp, float2* buf0,
+                                float2* buf1, uint64_t f0, uint64_t nb, int groups,
+                                int first_batch, double* part, int sms, cudaStream_t s) {
+  // buf1 holds the spectra; W goes to buf0, its FFT back to buf1
+  dim3 grid((kLargeM + 255) / 256, p.c, groups);
+  phased_global_kernel<<<grid, 256, 0, s>>>(p, pp, buf1, f0, nb, first_batch, part, buf0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !pp.want_raw) return e;
+  if ((e = large_fft_core(p, nb, buf0, buf1, sms, s)) != cudaSuccess) return e;
+  const uint64_t words = nb * (uint64_t)(p.n / (32 / pp.bits_out));
+  quant_global_kernel<<<grid_for(words, 256, sms), 256, 0, s>>>(p, pp, buf1, f0, nb);
   return cudaGetLastError();
 }
 

@@ -41,6 +41,9 @@ CASES = [
     dict(fft=4096, grid=0, band=(40, 0, 2008, 40), shuffle="pairswap", lsb1=True),
     dict(fft=8192, grid=0, band=(-128, 128, 4096, 0), shuffle="generic", lsb1=True, lsb2=True),
     dict(fft=4096, bits1=2, bits2=4, grid=1, band=(12, 0, 2036, 12)),
+    # FFT lengths above 8192 (four-step global FFT path)
+    dict(fft=16384, grid=0, band=(-64, 64, 8192, 0), shuffle="generic", lsb1=True, lsb2=True),
+    dict(fft=32768, bits1=1, bits2=2, grid=1, band=(100, 0, 16284, 100), w1=0.8, w2=1.2),
 ]
 
 
@@ -95,7 +98,7 @@ def test_phased_host_path(engine):
     s.close()
 
 
-@pytest.mark.parametrize("fft,lsb", [(4096, False), (8192, True)])
+@pytest.mark.parametrize("fft,lsb", [(4096, False), (8192, True), (16384, True)])
 def test_phased_raw_round_trip(engine, fft, lsb):
     """The phased .raw decodes with the same plan (ant1's levels and shuffle,
     LSB when both inputs are LSB, src/main.rs:1093, 2391-2412) into a stream
