@@ -74,8 +74,8 @@ def signal_raw(scan, nf, seed, rho=0.05, delay_samples=0.0, tone_bin=None):
 
 
 def spectral_errors(a, b, floor=None):
-    """(max relative amplitude error, max phase error, max abs error / rms)
-    of a against reference b; `floor` (scalar or per bin) bounds the
+    """(max relative amplitude error, max phase error, max complex error /
+    peak |b|) of a against reference b; `floor` (scalar or per bin) bounds the
     relative-error denominator from below (default 5% of rms(|b|))."""
     a = np.asarray(a, np.complex128)
     b = np.asarray(b, np.complex128)
@@ -89,7 +89,7 @@ def spectral_errors(a, b, floor=None):
     rel = float(np.max(np.abs(np.abs(a) - mag) / den))
     m = (mag >= fl) & (mag > 0)
     ph = float(np.max(np.abs(np.angle(a[m] * np.conj(b[m]))))) if m.any() else 0.0
-    ab = float(np.max(np.abs(a - b)) / rms)
+    ab = float(np.max(np.abs(a - b)) / np.max(mag))
     return rel, ph, ab
 
 
@@ -97,7 +97,7 @@ def assert_spectra_close(a, b, what, rel_tol=REL_AMP_TOL, phase_tol=PHASE_TOL, f
     rel, ph, ab = spectral_errors(a, b, floor)
     assert rel <= rel_tol and ph <= phase_tol and ab <= rel_tol, (
         f"{what}: rel amp {rel:.3e} (tol {rel_tol}), phase {ph:.3e} rad (tol {phase_tol}), "
-        f"abs/rms {ab:.3e}")
+        f"abs/peak {ab:.3e}")
     return rel, ph, ab
 
 
