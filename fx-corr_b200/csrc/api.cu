@@ -110,6 +110,8 @@ struct fxc_scan {
   FrameInfo* d_finfo = nullptr;  // per-frame delay records of the sector in flight
   uint64_t finfo_cap = 0;
   float2* d_big[2] = {nullptr, nullptr};  // FFT lengths > 8192: batch scratch
+  float2* d_twl = nullptr;                // FFT lengths > 8192: W_N^j, j < N
+  uint64_t twl_cap = 0;                   // entries allocated
   uint64_t big_frames = 0;                // frames per batch
   uint32_t* d_err = nullptr;
   cudaStream_t stream = nullptr;     // compute
@@ -314,6 +316,7 @@ LargeParams large_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2
   LargeParams p{};
   station_params(s, r1, r2, p.st);
   p.finfo = s->d_finfo;
+  p.tw = s->d_twl;
   p.n = (int32_t)s->n;
   p.c = (int32_t)(s->n / 8192);
   p.a1s = (int32_t)s->cfg.a1s;
@@ -537,6 +540,14 @@ fxc_status scan_bind(fxc_scan* s, const fxc_scan_cfg* cfg) {
     }
     s->big_cap = bige;
   }
+  if (n > 8192 && n > s->twl_cap) {
+    uint8_t* p = reinterpret_cast<uint8_t*>(s->d_twl);
+    uint64_t cap = s->twl_cap * sizeof(float2);
+    if ((st = grow_charged(s, &p, &cap, (uint64_t)n * sizeof(float2))) != FXC_OK) return st;
+    s->d_twl = reinterpret_cast<float2*>(p);
+    s->twl_cap = cap / sizeof(float2);
+  }
+  if (n > 8192) CK(launch_twiddle_table((int)n, s->d_twl, s->stream));
   if (tlen > s->table_cap) {
     uint8_t* p = reinterpret_cast<uint8_t*>(s->d_table);
     uint64_t cap = s->table_cap * 8;
@@ -755,6 +766,7 @@ fxc_status fxc_scan_close(fxc_scan* s) {
   cudaFree(s->d_partials);
   cudaFree(s->d_big[0]);
   cudaFree(s->d_big[1]);
+  cudaFree(s->d_twl);
   cudaFree(s->d_finfo);
   cudaFree(s->d_lut);
   cudaFree(s->d_levels);

@@ -67,12 +67,14 @@ cudaError_t launch_reduce(const double* part, int nblk, int h, double m11, doubl
 struct LargeParams {
   StationParams st[2];
   const FrameInfo* finfo;  // records of every frame of the sector
+  const float2* tw;        // W_N^j, j < N (launch_twiddle_table)
   int32_t n, c;
   int32_t a1s, a1e, a2s, grid;
   uint32_t products;
 };
 constexpr int kLargeGroups = 16;  // frame groups (partials) per sector
 int large_batch_frames(uint32_t n);
+cudaError_t launch_twiddle_table(int n, float2* tw, cudaStream_t s);
 cudaError_t launch_large_fft(const LargeParams& p, uint64_t f0, uint64_t nb, float2* buf0,
                              float2* buf1, int sms, cudaStream_t s);
 cudaError_t launch_large_acc(const LargeParams& p, const float2* Y, uint64_t f0, uint64_t nb,

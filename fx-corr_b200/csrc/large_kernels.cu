@@ -70,8 +70,73 @@ __global__ void decode_global_kernel(const LargeParams p, uint64_t f0, uint64_t 
   }
 }
 
+// Decode + shift fused with the first (radix-C, decimation in frequency)
+// step of the four-step FFT: thread (frame, m) decodes samples m + M c of both
+// stations (z = x1 + i x2, station 2 negated on odd frames as in
+// decode_global_kernel), combines them with a C-point DFT and writes row q,
+// column m twiddled by W_N^(m q) — the complex frame never goes to HBM.
 template <int C>
-__global__ void dif_kernel(const float2* __restrict__ z, float2* __restrict__ y, uint64_t nb) {
+__global__ void decode_dif_kernel(const LargeParams p, uint64_t f0, uint64_t nb,
+                                  float2* __restrict__ y) {
+  __shared__ uint32_t lut[2048];
+  __shared__ float lv[512];
+  for (int i = threadIdx.x; i < 512; i += blockDim.x)
+    lv[i] = p.st[i >> 8].levels[i & 255] * p.st[i >> 8].scale;
+  for (int s = 0; s < 2; ++s)
+    if (p.st[s].shkind == SH_GENERIC)
+      for (int i = threadIdx.x; i < 1024; i += blockDim.x) lut[s * 1024 + i] = p.st[s].shlut[i];
+  __syncthreads();
+  constexpr int M = kLargeM;
+  constexpr int N = C * M;
+  static_assert(M == 8192, "frame / column split by shifts");
+  const uint64_t total = nb * (uint64_t)M;
+  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t fl = idx >> 13;
+    const int m = (int)(idx & (uint64_t)(M - 1));
+    const uint64_t f = f0 + fl;
+    const FrameInfo& F = p.finfo[f];
+    const uint8_t* r1 = p.st[0].raw + f * p.st[0].bpf;
+    const uint8_t* r2 = p.st[1].raw + f * p.st[1].bpf;
+    const bool odd = (f & 1u) != 0;
+    float2 v[16];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const int n = m + M * c;
+      const float a = sample_at(r1, p.st[0].bits, p.st[0].shkind, lut, lv, p.st[0].lsb, n - F.s1, N);
+      const float b = sample_at(r2, p.st[1].bits, p.st[1].shkind, lut + 1024, lv + 256,
+                                p.st[1].lsb, n - F.s2, N);
+      v[c] = make_float2(a, odd ? -b : b);
+    }
+    if constexpr (C == 2) {
+      dft2<0>(v);
+    } else if constexpr (C == 4) {
+      dft4<0>(v);
+    } else {
+      dft8<0>(v);
+    }
+    float2* yf = y + fl * (uint64_t)N;
+#pragma unroll
+    for (int q = 0; q < C; ++q) {
+      float2 val = v[out_pos<C>(q)];
+      if (q > 0) val = cmul(val, p.tw[m * q]);
+      yf[q * M + m] = val;
+    }
+  }
+}
+
+// W_N^j = exp(-2 pi i j / N), j < N, correctly rounded from FP64.
+__global__ void twiddle_table_kernel(int n, float2* __restrict__ tw) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double s, c;
+  sincospi(-2.0 * (double)j / (double)n, &s, &c);
+  tw[j] = make_float2((float)c, (float)s);
+}
+
+template <int C>
+__global__ void dif_kernel(const float2* __restrict__ z, float2* __restrict__ y, uint64_t nb,
+                           const float2* __restrict__ tw) {
   constexpr int M = kLargeM;
   constexpr int N = C * M;
   const uint64_t total = nb * (uint64_t)M;
@@ -94,11 +159,7 @@ __global__ void dif_kernel(const float2* __restrict__ z, float2* __restrict__ y,
 #pragma unroll
     for (int q = 0; q < C; ++q) {
       float2 val = v[out_pos<C>(q)];
-      if (q > 0) {
-        float s, c;
-        sincospif(-2.0f * (float)((m * q) % N) / (float)N, &s, &c);
-        val = cmul(val, make_float2(c, s));
-      }
+      if (q > 0) val = cmul(val, tw[m * q]);  // W_N^(m q), m q < N
       yf[q * M + m] = val;
     }
   }
@@ -155,8 +216,8 @@ __global__ void acc_global_kernel(const LargeParams p, const float2* __restrict_
   for (uint64_t fl = g0; fl < g1; ++fl) {
     const float2* Zf = Y + fl * (uint64_t)N;
     const FrameInfo& F = p.finfo[f0 + fl];
-    float sn, cs;
-    sincosf(fmaf((float)(bin - a_gs), F.dphi, F.phi0), &sn, &cs);
+    float sn, cs;  // SFU sin/cos: |angle| <= ~pi (ramp over the band), abs error < 4e-7
+    __sincosf(fmaf((float)(bin - a_gs), F.dphi, F.phi0), &sn, &cs);
     const float2 r = cmul(F.fr_mix, make_float2(cs, sn));
     const float sg = ((f0 + fl) & 1u) ? -1.0f : 1.0f;  // station 2 sign of this frame
     const float2 u = zi(Zf, bin), w = zi(Zf, N - bin);
@@ -327,15 +388,23 @@ static int grid_for(uint64_t work, int threads, int sms) {
 }
 
 // DIF over C columns (buf0 -> buf1), then the M-point row FFTs in place on buf1.
+static cudaError_t row_ffts(const LargeParams& p, uint64_t nb, float2* buf1, int sms,
+                           cudaStream_t s);
+
 static cudaError_t large_fft_core(const LargeParams& p, uint64_t nb, const float2* buf0,
                                   float2* buf1, int sms, cudaStream_t s) {
   const uint64_t work = nb * kLargeM;
   switch (p.c) {
-    case 2: dif_kernel<2><<<grid_for(work, 256, sms), 256, 0, s>>>(buf0, buf1, nb); break;
-    case 4: dif_kernel<4><<<grid_for(work, 256, sms), 256, 0, s>>>(buf0, buf1, nb); break;
-    case 8: dif_kernel<8><<<grid_for(work, 256, sms), 256, 0, s>>>(buf0, buf1, nb); break;
+    case 2: dif_kernel<2><<<grid_for(work, 256, sms), 256, 0, s>>>(buf0, buf1, nb, p.tw); break;
+    case 4: dif_kernel<4><<<grid_for(work, 256, sms), 256, 0, s>>>(buf0, buf1, nb, p.tw); break;
+    case 8: dif_kernel<8><<<grid_for(work, 256, sms), 256, 0, s>>>(buf0, buf1, nb, p.tw); break;
     default: return cudaErrorInvalidValue;
   }
+  return row_ffts(p, nb, buf1, sms, s);
+}
+
+static cudaError_t row_ffts(const LargeParams& p, uint64_t nb, float2* buf1, int sms,
+                           cudaStream_t s) {
   const uint32_t smem = 2 * Geom<kLargeM>::CSTRIDE * sizeof(float2);
   auto kern = cfft_kernel<kLargeM>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -347,12 +416,23 @@ static cudaError_t large_fft_core(const LargeParams& p, uint64_t nb, const float
 
 cudaError_t launch_large_fft(const LargeParams& p, uint64_t f0, uint64_t nb, float2* buf0,
                              float2* buf1, int sms, cudaStream_t s) {
-  // decode -> buf0, DIF -> buf1, row FFTs in place on buf1
-  decode_global_kernel<<<grid_for(nb * p.n, 256, sms), 256, 0, s>>>(p, f0, nb, buf0, nullptr,
-                                                                     nullptr);
+  // decode + DIF -> buf1, row FFTs in place on buf1 (buf0 is not used)
+  (void)buf0;
+  const uint64_t work = nb * kLargeM;
+  switch (p.c) {
+    case 2: decode_dif_kernel<2><<<grid_for(work, 256, sms), 256, 0, s>>>(p, f0, nb, buf1); break;
+    case 4: decode_dif_kernel<4><<<grid_for(work, 256, sms), 256, 0, s>>>(p, f0, nb, buf1); break;
+    case 8: decode_dif_kernel<8><<<grid_for(work, 256, sms), 256, 0, s>>>(p, f0, nb, buf1); break;
+    default: return cudaErrorInvalidValue;
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  return large_fft_core(p, nb, buf0, buf1, sms, s);
+  return row_ffts(p, nb, buf1, sms, s);
+}
+
+cudaError_t launch_twiddle_table(int n, float2* tw, cudaStream_t s) {
+  twiddle_table_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, tw);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_large_phased(const LargeParams& p, const PhasedParams& pp, float2* buf0,
