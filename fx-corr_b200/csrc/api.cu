@@ -366,7 +366,8 @@ PhasedParams phased_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* 
 // re-quantisation) on the same spectra; fixed-order reductions at the end.
 fxc_status run_large(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
                      uint64_t first, double* d_acc, uint8_t* d_raw_out, bool corr, bool phased,
-                     cudaStream_t st) {
+                     bool corr_done, cudaStream_t st) {
+  if (!corr && !phased) return FXC_OK;
   const uint32_t h = s->h;
   const LargeParams p = large_params(s, r1, r2);
   PhasedParams pp{};
@@ -395,7 +396,7 @@ fxc_status run_large(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t
                      0.25 * u1 * u2, d_acc, st));
     s->all_launches += 1;
     s->kernel_launches += 1;
-  } else {
+  } else if (!corr_done) {
     CK(cudaMemsetAsync(d_acc, 0, sizeof(double) * 5 * h, st));
   }
   if (phased) {
@@ -420,7 +421,18 @@ fxc_status run_sector_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, 
   fxc_status fst = stage_frame_info(s, first, nf, st);
   if (fst != FXC_OK) return fst;
   s->all_launches += 1;
-  if (s->n > 8192) return run_large(s, r1, r2, nf, first, d_acc, d_raw_out, corr, phased, st);
+  if (s->n > 8192) {
+    // FFT 16384 correlation: the two-row shared-memory kernel when the band
+    // shift is even, else the four-step path
+    bool corr_done = false;
+    if (s->n == 16384 && corr && corr_fold2_supported(corr_params(s, r1, r2, nf, first))) {
+      fst = run_corr_stage(s, r1, r2, nf, first, grid, d_acc, st);
+      if (fst != FXC_OK) return fst;
+      corr_done = true;
+    }
+    return run_large(s, r1, r2, nf, first, d_acc, d_raw_out, corr && !corr_done, phased, corr_done,
+                     st);
+  }
   if (!corr) {
     CK(cudaMemsetAsync(d_acc, 0, sizeof(double) * 5 * h, st));
   } else {
@@ -516,8 +528,10 @@ fxc_status scan_bind(fxc_scan* s, const fxc_scan_cfg* cfg) {
   const uint32_t n = cfg->fft_len, h = n / 2 + 1;
   const uint64_t maxg = n > 8192 ? (uint64_t)kLargeGroups
                                  : (uint64_t)e->sm_count * (uint64_t)corr_ctas_per_sm(n);
-  // N > 8192: [group][4][H] correlation partials, then [group][H] phased partials
-  const uint64_t pel = maxg * (n > 8192 ? 5 : 4) * h;
+  // N > 8192: [group][4][H] correlation partials, then [group][H] phased partials;
+  // N = 16384 also serves the two-row kernel's [CTA][4][H]
+  uint64_t pel = maxg * (n > 8192 ? 5 : 4) * h;
+  if (n == 16384) pel = std::max<uint64_t>(pel, (uint64_t)e->sm_count * 4 * h);
   const uint64_t bigf = n > 8192 ? (uint64_t)large_batch_frames(n) : 0;
   const uint64_t bige = bigf * (uint64_t)n;
   const uint64_t tlen = cfg->delay.geom_table ? cfg->delay.geom_len : 0;

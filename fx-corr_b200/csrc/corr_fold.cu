@@ -68,14 +68,20 @@ static_assert(kOffA % 128 == 0 && kOffFi % 16 == 0 && kOffBar % 8 == 0, "alignme
 // r < 16, as a byte offset of the level table: rotate the word so that the
 // sample's bits land at byte-offset bits 2.., mask, merge the table base
 // (which also selects the negated copy for odd samples of an LSB station).
-template <int BITS, bool IMAG, bool SPLIT>
+// ROWS = 2 (FFT 16384 as two 8192-point rows): input r of row 0 is
+// x[m] + x[m + 8192], of row 1 x[m] - x[m + 8192] (neg_hi), m = t + 512 r - shift,
+// the first radix-2 step of a decimation in frequency; the row-1 twiddle is
+// applied by the caller.
+template <int BITS, bool IMAG, bool SPLIT, int ROWS>
 __device__ __forceinline__ void fold_inputs(const uint32_t* __restrict__ words, const uint8_t* lvbase,
                                             int shift, uint32_t rots, uint32_t tbase,
-                                            float2 (&v)[16], int t) {
+                                            float2 (&v)[16], int t, bool neg_hi) {
   constexpr int T1 = kN / 16;
+  constexpr int NF = kN * ROWS;                  // frame length
   constexpr int SPW = 32 / BITS;
   constexpr int LOG2_SPW = BITS == 1 ? 5 : (BITS == 2 ? 4 : (BITS == 4 ? 3 : 2));
   constexpr int WSTEP = T1 / SPW;
+  constexpr int HW = kN / SPW;                   // words of the upper half's offset
   constexpr uint32_t OMASK = ((1u << BITS) - 1u) << 2;
   static_assert(T1 % SPW == 0, "frame stride is a whole number of words");
   const int m0 = t - shift;
@@ -91,58 +97,80 @@ __device__ __forceinline__ void fold_inputs(const uint32_t* __restrict__ words, 
     }
     return *reinterpret_cast<const float*>(lvbase + off);
   };
+  // sample m (+ kN for the upper half) with the zero fill
+  auto checked = [&](int r, int half) -> float {
+    const int m = m0 + r * T1 + half * kN;
+    const bool in = (unsigned)m < (unsigned)NF;
+    const float x = level(words[in ? w0 + r * WSTEP + half * HW : 0]);
+    return in ? x : 0.0f;
+  };
+  auto put = [&](int r, float x) {
+    if (IMAG) v[r].y = x; else v[r].x = x;
+  };
+  const uint32_t* w = words + w0;
   if (shift == 0) {
-    const uint32_t* w = words + w0;
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
-      const float x = level(w[r * WSTEP]);
-      if (IMAG) v[r].y = x; else v[r].x = x;
+      float x = level(w[r * WSTEP]);
+      if constexpr (ROWS == 2) {
+        const float hi = level(w[r * WSTEP + HW]);
+        x = neg_hi ? x - hi : x + hi;
+      }
+      put(r, x);
     }
   } else if ((unsigned)(shift + (T1 - 1)) < (unsigned)(2 * T1 - 1)) {
-    // |shift| < N/16: only r = 0 and r = 15 can fall outside the frame
-    const uint32_t* w = words + w0;
+    // |shift| < N/16: only the first sample of the lower half and the last
+    // of the upper half (or, one row, of the frame) can fall outside it
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       float x;
-      if (r == 0 || r == 15) {
-        const int m = m0 + r * T1;
-        const bool in = (unsigned)m < (unsigned)kN;
-        x = level(words[in ? w0 + r * WSTEP : 0]);
-        x = in ? x : 0.0f;
+      if constexpr (ROWS == 1) {
+        x = (r == 0 || r == 15) ? checked(r, 0) : level(w[r * WSTEP]);
       } else {
-        x = level(w[r * WSTEP]);
+        const float lo = r == 0 ? checked(r, 0) : level(w[r * WSTEP]);
+        const float hi = r == 15 ? checked(r, 1) : level(w[r * WSTEP + HW]);
+        x = neg_hi ? lo - hi : lo + hi;
       }
-      if (IMAG) v[r].y = x; else v[r].x = x;
+      put(r, x);
     }
   } else {
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
-      const int m = m0 + r * T1;
-      const bool in = (unsigned)m < (unsigned)kN;
-      const float x = level(words[in ? w0 + r * WSTEP : 0]);
-      if (IMAG) v[r].y = in ? x : 0.0f; else v[r].x = in ? x : 0.0f;
+      float x = checked(r, 0);
+      if constexpr (ROWS == 2) {
+        const float hi = checked(r, 1);
+        x = neg_hi ? x - hi : x + hi;
+      }
+      put(r, x);
     }
   }
 }
 
-template <bool IMAG>
+template <bool IMAG, int ROWS>
 __device__ __forceinline__ void fold_station(int bits, bool split, const uint32_t* words,
                                              const uint8_t* lvbase, int shift, uint32_t rots,
-                                             uint32_t tbase, float2 (&v)[16], int t) {
+                                             uint32_t tbase, float2 (&v)[16], int t, bool neg_hi) {
   switch (bits) {
-    case 1: fold_inputs<1, IMAG, false>(words, lvbase, shift, rots, tbase, v, t); break;
+    case 1: fold_inputs<1, IMAG, false, ROWS>(words, lvbase, shift, rots, tbase, v, t, neg_hi); break;
     case 2:
-      if (split) fold_inputs<2, IMAG, true>(words, lvbase, shift, rots, tbase, v, t);
-      else fold_inputs<2, IMAG, false>(words, lvbase, shift, rots, tbase, v, t);
+      if (split) fold_inputs<2, IMAG, true, ROWS>(words, lvbase, shift, rots, tbase, v, t, neg_hi);
+      else fold_inputs<2, IMAG, false, ROWS>(words, lvbase, shift, rots, tbase, v, t, neg_hi);
       break;
-    case 4: fold_inputs<4, IMAG, false>(words, lvbase, shift, rots, tbase, v, t); break;
-    default: fold_inputs<8, IMAG, false>(words, lvbase, shift, rots, tbase, v, t); break;
+    case 4: fold_inputs<4, IMAG, false, ROWS>(words, lvbase, shift, rots, tbase, v, t, neg_hi); break;
+    default: fold_inputs<8, IMAG, false, ROWS>(words, lvbase, shift, rots, tbase, v, t, neg_hi); break;
   }
 }
 
 }  // namespace
 
-__global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
+// ROWS = 1: FFT 8192.  ROWS = 2: FFT 16384 as two 8192-point rows (the radix-2
+// DIF step fused into the decode); one launch per row, `row` = 0 handles the
+// even bins, 1 the odd bins, both accumulate into the same per-CTA partials.
+template <int ROWS>
+__global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, int row) {
+  constexpr int NF = kN * ROWS;       // frame FFT length
+  constexpr int HF = NF / 2 + 1;      // bins
+  static_assert(ROWS == 1 || ROWS == 2, "one or two rows");
   extern __shared__ __align__(128) uint8_t smem[];
   const FoldLayout L = fold_layout(p.stage_bytes);
   float* lv = reinterpret_cast<float*>(smem);
@@ -209,6 +237,18 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
   }
   Twiddles<kN> tw;
   tw.init(tid);
+  // ROWS = 2: row-1 DIF twiddle bases W_NF^t, W_NF^(t+512) (= W^t W_32) and
+  // the row-1 fold's W_M^(t+1); all correctly rounded from FP64
+  float2 dtw0 = make_float2(1.f, 0.f), dtw1 = dtw0, wb1 = dtw0;
+  if constexpr (ROWS == 2) {
+    double sn, cs;
+    sincospi(-2.0 * (double)tid / (double)NF, &sn, &cs);
+    dtw0 = make_float2((float)cs, (float)sn);
+    sincospi(-2.0 * (double)(tid + NF / 32) / (double)NF, &sn, &cs);
+    dtw1 = make_float2((float)cs, (float)sn);
+    sincospi(-2.0 * (double)(tid + 1) / (double)kN, &sn, &cs);
+    wb1 = make_float2((float)cs, (float)sn);
+  }
 
   const uint64_t iters = p.nf;
   const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
@@ -249,19 +289,22 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
   const int lsbP = sp.lsb ? 1 : 0, lsbS = ss.lsb ? 1 : 0;
   bool first_flush = true;
   uint32_t since_flush = 0;
-  double* part = p.partials + (size_t)blockIdx.x * 4 * kH;
+  double* part = p.partials + (size_t)blockIdx.x * 4 * HF;
   const int colP = g0 ? 0 : 1, colS = g0 ? 1 : 0;  // output columns of the two ACFs
 
   auto flush = [&]() {
 #pragma unroll
     for (int i = 0; i < kSlots; ++i) {
       if (i == kSlots - 1 && tid != 0) continue;
+      if (ROWS == 2 && row == 1 && i == kSlots - 1) continue;  // bin N/4 is even
       const int j = tid + kT * (i >> 1);
-      const int bin = (i == kSlots - 1) ? kN / 4 : ((i & 1) ? kN / 2 - j : j);
+      const int bin = ROWS == 1 ? ((i == kSlots - 1) ? kN / 4 : ((i & 1) ? kN / 2 - j : j))
+                                : ((i == kSlots - 1) ? NF / 4
+                                   : ((i & 1) ? NF / 2 - 2 * j - row : 2 * j + row));
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
         const int col = v == 0 ? colP : (v == 1 ? colS : v);
-        double* q = part + (size_t)col * kH + bin;
+        double* q = part + (size_t)col * HF + bin;
         *q = (first_flush ? 0.0 : *q) + (double)acc[i][v];
         acc[i][v] = 0.f;
       }
@@ -300,8 +343,27 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
       // the secondary station enters odd frames negated (see sgn below)
       const uint32_t tbS = 2048u + (uint32_t)((((uint32_t)mS & (uint32_t)lsbS) ^ (uint32_t)(it & 1u))
                                               << (bitsS + 2));
-      fold_station<false>(bitsP, splitP, wP, smem, sP, pos[cP], tbP, v, tid);
-      fold_station<true>(bitsS, splitS, wS, smem, sS, pos[32 + cS], tbS, v, tid);
+      fold_station<false, ROWS>(bitsP, splitP, wP, smem, sP, pos[cP], tbP, v, tid, row == 1);
+      fold_station<true, ROWS>(bitsS, splitS, wS, smem, sS, pos[32 + cS], tbS, v, tid, row == 1);
+      if (ROWS == 2 && row == 1) {
+        // DIF twiddle W_NF^m, m = t + 512 r = W^t W_32^r: even r from
+        // b0 = W^t, odd r from b1 = W^t W_32, times W_16^(r/2)
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+          float2 w;
+          switch (r >> 1) {  // compile-time after unrolling
+            case 0: w = (r & 1) ? dtw1 : dtw0; break;
+            case 1: w = mul_w16<1>((r & 1) ? dtw1 : dtw0); break;
+            case 2: w = mul_w16<2>((r & 1) ? dtw1 : dtw0); break;
+            case 3: w = mul_w16<3>((r & 1) ? dtw1 : dtw0); break;
+            case 4: w = mul_w16<4>((r & 1) ? dtw1 : dtw0); break;
+            case 5: w = mul_w16<5>((r & 1) ? dtw1 : dtw0); break;
+            case 6: w = mul_w16<6>((r & 1) ? dtw1 : dtw0); break;
+            default: w = mul_w16<7>((r & 1) ? dtw1 : dtw0); break;
+          }
+          v[r] = cmul(v[r], w);
+        }
+      }
       dft16(v);
       float2* dst = bufA + 17 * tid;  // cpad(16 t + r) = 17 t + r
 #pragma unroll
@@ -323,15 +385,18 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
     float sn, cs;
     const int a_gs = ovs;
     const float2 mix = F.fr_mix;
-    __sincosf(fmaf((float)(tid - a_gs), F.dphi, F.phi0), &sn, &cs);
+    // bins of unit i: up = ROWS * j + row, down = NF/2 - ROWS * j - row, j = tid + T i
+    const int bup0 = ROWS * tid + row, bdn0 = NF / 2 - ROWS * tid - row;
+    __sincosf(fmaf((float)(bup0 - a_gs), F.dphi, F.phi0), &sn, &cs);
     float2 rup = cmul(mix, make_float2(cs, sn));
-    __sincosf(fmaf((float)(kN / 2 - tid - a_gs), F.dphi, F.phi0), &sn, &cs);
+    __sincosf(fmaf((float)(bdn0 - a_gs), F.dphi, F.phi0), &sn, &cs);
     float2 rdn = cmul(mix, make_float2(cs, sn));
-    __sincosf((float)kT * F.dphi, &sn, &cs);
+    __sincosf((float)(ROWS * kT) * F.dphi, &sn, &cs);
     const float2 rstep = make_float2(cs, sn);
+    const bool quarter = tid == 0 && (ROWS == 1 || row == 0);  // bin NF/4 (even)
     float2 rq = make_float2(0.f, 0.f);
-    if (tid == 0) {
-      __sincosf(fmaf((float)(kN / 4 - a_gs), F.dphi, F.phi0), &sn, &cs);
+    if (quarter) {
+      __sincosf(fmaf((float)(NF / 4 - a_gs), F.dphi, F.phi0), &sn, &cs);
       rq = cmul(mix, make_float2(cs, sn));
     }
 
@@ -353,24 +418,39 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
         case 2: wj = mul_w16<2>(tw.w[Geom<kN>::P16]); break;
         default: wj = mul_w16<3>(tw.w[Geom<kN>::P16]); break;
       }
-      const float2 a = Y[j], b = Y[j + kN / 2], c = Y[kN / 2 - j], d = Y[(kN - j) & (kN - 1)];
-      const float2 wb = cmul(wj, b), wd = cmulc(d, wj);  // W^j b, conj(W^j) d
-      const float2 zj = cadd(a, wb), zjh = csub(a, wb);  // Z[j], Z[j + N/2]
-      const float2 zmn = cadd(c, wd);                    // Z[N - j]
-      // Z[N/2 - j]; for j = 0 that is Z[N/2] = Y[0] - Y[N/2]
-      const float2 zm = j == 0 ? zjh : csub(c, wd);
+      // row-local columns: Z[j], Z[j + M/2] from Y[j], Y[j + M/2]; the mirror
+      // pair from Y[c0], Y[c0 + M/2] with c0 = M/2 - j (one row: mirror of
+      // column j is M - j) or M/2 - 1 - j (odd row: mirror is M - 1 - j)
+      const int c0 = (ROWS == 2 && row == 1) ? kN / 2 - 1 - j : kN / 2 - j;
+      const float2 a = Y[j], b = Y[j + kN / 2], c = Y[c0], d = Y[(c0 + kN / 2) & (kN - 1)];
+      // W_M^c0 = -conj(W_M^(M/2 - c0)): W^j for the even mirror, W^(j+1) for the odd one
+      float2 wm = wj;
+      if (ROWS == 2 && row == 1) {
+        switch (i) {
+          case 0: wm = wb1; break;
+          case 1: wm = mul_w16<1>(wb1); break;
+          case 2: wm = mul_w16<2>(wb1); break;
+          default: wm = mul_w16<3>(wb1); break;
+        }
+      }
+      const float2 wb = cmul(wj, b), wd = cmulc(d, wm);  // W^j b, conj(W^(M/2-c0)) d
+      const float2 zj = cadd(a, wb), zjh = csub(a, wb);  // Z[j], Z[j + M/2]
+      const float2 zmn = cadd(c, wd);                    // Z[c0 + M/2] (mirror of j)
+      // Z[c0]; for an even row and j = 0 that is Z[M/2] = Y[0] - Y[M/2]
+      const float2 zm = ((ROWS == 1 || row == 0) && j == 0) ? zjh : csub(c, wd);
       // primary = real part: P[k] = (Z[k] + conj Z[N-k]), S[k] = -i (Z[k] - conj Z[N-k])
+      const int bu = ROWS * j + row, bd = NF / 2 - ROWS * j - row;  // global bins
       prim[2 * i] = make_float2(zj.x + zmn.x, zj.y - zmn.y);
-      Q[j] = make_float2(sgn * (zj.y + zmn.y), sgn * (zmn.x - zj.x));
+      Q[bu] = make_float2(sgn * (zj.y + zmn.y), sgn * (zmn.x - zj.x));
       prim[2 * i + 1] = make_float2(zm.x + zjh.x, zm.y - zjh.y);
-      Q[kN / 2 - j] = make_float2(sgn * (zm.y + zjh.y), sgn * (zjh.x - zm.x));
+      Q[bd] = make_float2(sgn * (zm.y + zjh.y), sgn * (zjh.x - zm.x));
     }
     float2 prim_q = make_float2(0.f, 0.f);
-    if (tid == 0) {  // bin N/4: Z[N/4] = Y[N/4] - i Y[3N/4], Z[3N/4] = Y[N/4] + i Y[3N/4]
+    if (quarter) {  // column M/4: Z[M/4] = Y[M/4] - i Y[3M/4], Z[3M/4] = Y[M/4] + i Y[3M/4]
       const float2 a = Y[kN / 4], b = Y[3 * kN / 4];
       const float2 zq = make_float2(a.x + b.y, a.y - b.x), zq3 = make_float2(a.x - b.y, a.y + b.x);
       prim_q = make_float2(zq.x + zq3.x, zq.y - zq3.y);
-      Q[kN / 4] = make_float2(sgn * (zq.y + zq3.y), sgn * (zq3.x - zq.x));
+      Q[NF / 4] = make_float2(sgn * (zq.y + zq3.y), sgn * (zq3.x - zq.x));
     }
     __syncthreads();
 
@@ -393,12 +473,12 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p) {
 #pragma unroll
     for (int i = 0; i < kUnits; ++i) {
       const int j = tid + kT * i;
-      bin_acc(j, prim[2 * i], rup, acc[2 * i]);
-      bin_acc(kN / 2 - j, prim[2 * i + 1], rdn, acc[2 * i + 1]);
+      bin_acc(ROWS * j + row, prim[2 * i], rup, acc[2 * i]);
+      bin_acc(NF / 2 - ROWS * j - row, prim[2 * i + 1], rdn, acc[2 * i + 1]);
       rup = cmul(rup, rstep);
       rdn = cmulc(rdn, rstep);
     }
-    if (tid == 0) bin_acc(kN / 4, prim_q, rq, acc[kSlots - 1]);
+    if (quarter) bin_acc(NF / 4, prim_q, rq, acc[kSlots - 1]);
     if (++since_flush >= p.flush_every) flush();
   }
   if (since_flush > 0 || first_flush) flush();
@@ -412,11 +492,28 @@ uint32_t fold_smem_bytes(uint32_t stage_bytes) { return fold_layout(stage_bytes)
 
 cudaError_t launch_corr_fold(const CorrParams& p, int grid, cudaStream_t stream) {
   const uint32_t smem = fold_smem_bytes(p.stage_bytes);
-  cudaError_t e = cudaFuncSetAttribute(corr_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(corr_fold_kernel<1>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  corr_fold_kernel<<<grid, kT, smem, stream>>>(p);
+  corr_fold_kernel<1><<<grid, kT, smem, stream>>>(p, 0);
   return cudaGetLastError();
+}
+
+bool corr_fold2_supported(const CorrParams& p) {
+  // a row holds the bins of one parity: the band shift must keep it
+  return ((p.a2s - p.a1s) & 1) == 0 && fold_smem_bytes(p.stage_bytes) <= 232448u;
+}
+
+cudaError_t launch_corr_fold2(const CorrParams& p, int grid, cudaStream_t stream) {
+  const uint32_t smem = fold_smem_bytes(p.stage_bytes);
+  cudaError_t e = cudaFuncSetAttribute(corr_fold_kernel<2>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  for (int row = 0; row < 2; ++row) {
+    corr_fold_kernel<2><<<grid, kT, smem, stream>>>(p, row);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace fxc

@@ -342,6 +342,11 @@ static cudaError_t launch_mode(uint32_t n, const CorrParams& p, int grid, cudaSt
       // the FFT-8192 correlation has a kernel of its own (corr_fold.cu)
       if constexpr (MODE == MODE_CORR) return launch_corr_fold(p, grid, s);
       else return launch_one<8192, 1, MODE>(p, grid, s);
+    case 16384:
+      // FFT 16384 as two 8192-point rows (corr_fold.cu); other modes and odd
+      // band shifts take the four-step path (large_kernels.cu)
+      if constexpr (MODE == MODE_CORR) return launch_corr_fold2(p, grid, s);
+      else return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
   }
 }

@@ -60,6 +60,10 @@ int corr_ctas_per_sm(uint32_t n);
 cudaError_t launch_corr(uint32_t n, int mode, const CorrParams& p, int grid, cudaStream_t s);
 // FFT-8192 correlation (MODE_CORR), one frame pair per CTA iteration (corr_fold.cu)
 cudaError_t launch_corr_fold(const CorrParams& p, int grid, cudaStream_t s);
+// FFT-16384 correlation as two 8192-point rows (corr_fold.cu); needs an even
+// band shift (a row holds the bins of one parity)
+bool corr_fold2_supported(const CorrParams& p);
+cudaError_t launch_corr_fold2(const CorrParams& p, int grid, cudaStream_t s);
 uint32_t fold_smem_bytes(uint32_t stage_bytes);
 cudaError_t launch_reduce(const double* part, int nblk, int h, double m11, double m22, double m12,
                           double* out, cudaStream_t s);

@@ -217,12 +217,13 @@ def test_weak_correlation_long_integration(engine, fft, nf):
     s.close()
 
 
-@pytest.mark.parametrize("d1", [-2.3e-6, 5.1e-6, 1.7e-5])
-def test_sector_large_shift(engine, d1):
+@pytest.mark.parametrize("fft,d1", [(8192, -2.3e-6), (8192, 5.1e-6), (8192, 1.7e-5),
+                                    (16384, -9.1e-6), (16384, 2.0e-6), (16384, 3.3e-5)])
+def test_sector_large_shift(engine, fft, d1):
     """Integer shifts beyond N/16 (and beyond N: an all-zero station frame)."""
     delay = dict(DELAY, net_d1_base=d1)
-    scan = make_scan(fft=8192, fs=512e6, delay=delay, shuffle="generic", lsb1=True,
-                     band=(128, 0, 3968, 128))
+    scan = make_scan(fft=fft, fs=512e6, delay=delay, shuffle="generic", lsb1=True,
+                     band=(128, 0, fft // 2 - 128, 128))
     nf = 9
     r1, r2 = signal_raw(scan, nf, seed=5, rho=0.2, delay_samples=6.4)
     s = engine.open_scan(to_fxc(scan))
@@ -373,6 +374,12 @@ def test_large_spectra_vs_fp64(engine, n):
 
 LARGE_CASES = [
     dict(fft=16384, band=(256, 0, 7936, 256), grid=0, shuffle="generic", lsb1=True),
+    # FFT 16384, two-row kernel: grid 1, LSB on station 2, pair-splitting 2-bit and 4-bit
+    dict(fft=16384, band=(-40, 40, 8192, 0), grid=1, shuffle="generic", lsb2=True),
+    dict(fft=16384, bits1=4, bits2=2, band=(12, 0, 8180, 12), grid=0, shuffle="pairswap",
+         products=oracle.PROD_ACF | oracle.PROD_ACF_OVERLAP_ONLY | oracle.PROD_XCF),
+    # odd band shift: the four-step path
+    dict(fft=16384, band=(-7, 7, 8192, 0), grid=0, lsb1=True),
     dict(fft=32768, band=(-64, 64, 16384, 0), grid=1, bits1=4, bits2=4),
     dict(fft=65536, band=(0, 0, 32768, 0), grid=0, bits1=1, bits2=2,
          products=oracle.PROD_ACF | oracle.PROD_ACF_OVERLAP_ONLY | oracle.PROD_XCF),
