@@ -292,8 +292,8 @@ def run_reference(args, rank, world):
 # ------------------------------------------------------------------ main
 
 def serve_jobs(n_jobs, load, seed=5150):
-    """Seeded Poisson stream of correlation jobs: 0.1-5 s chunks at 256-1024
-    Msps, 2-bit, FFT 1024-16384, random station delays and rates, dumps every
+    """Long jobs: seeded Poisson stream of 0.1-5 s chunks at 256-1024 Msps,
+    2-bit, FFT 1024-16384, random station delays and rates, dumps every
     second; arrivals at `load` x real time (data seconds offered per second)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     mean_dur = 2.55
@@ -313,14 +313,34 @@ def serve_jobs(n_jobs, load, seed=5150):
     return jobs
 
 
-def serve_leg(fxc, torch, eng, n_jobs=20, load=2.0, slots=4):
+def short_jobs(n_jobs, rate, seed=6262):
+    """Short jobs: seeded Poisson stream at `rate` jobs/s of 1-16 ms chunks
+    (125-2000 frame pairs) at 1024 Msps, 2-bit, FFT 8192, random station
+    delays and rates, one dump per job."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    fs, fft = 1024e6, 8192
+    t = 0.0
+    jobs = []
+    for k in range(n_jobs):
+        t += float(rng.exponential(1.0 / rate))
+        dur = float(rng.uniform(1e-3, 16e-3))
+        nf = max(1, int(round(dur * fs / fft)))
+        delay = dict(frame_dt=fft / fs, fs=fs, net_d1_base=float(rng.uniform(-2e-6, 2e-6)),
+                     total_rate1_base=float(rng.uniform(-1e-6, 1e-6)),
+                     net_d2_base=float(rng.uniform(-2e-6, 2e-6)), lo1_hz=8.4e9, lo2_hz=8.4e9)
+        jobs.append(dict(arrival=t, dur=dur, fs=fs, fft=fft, nf=nf, sector_frames=0, delay=delay,
+                         seed=k))
+    return jobs
+
+
+def serve_leg(fxc, torch, eng, jobs, slots, batch, plain_jobs=None, label="", mix=""):
     """Served (fxc_server, continuous batching) vs plain (one job at a time:
     scan open, per sector a synchronous H2D + kernels + dump, scan close) on
-    the same job stream, at the offered load and saturated (all jobs queued
-    at once)."""
+    the same job stream, at the offered arrival times and saturated (all jobs
+    queued at once).  plain_jobs: the plain path runs only the first jobs of
+    the stream (its throughput per job is that of a sequential loop)."""
     import threading
 
-    jobs = serve_jobs(n_jobs, load)
     cfgs = []
     for j in jobs:
         c = fxc.ScanConfig(fft=j["fft"], fs=j["fs"], bits1=2, bits2=2,
@@ -340,13 +360,14 @@ def serve_leg(fxc, torch, eng, n_jobs=20, load=2.0, slots=4):
     torch.cuda.synchronize()
     p1, p2 = pool[0].numpy(), pool[1].numpy()
     samples = [2 * j["nf"] * j["fft"] for j in jobs]
+    np_jobs = len(jobs) if plain_jobs is None else min(plain_jobs, len(jobs))
 
     def plain_job(j, c):
         # the plain single-job path: open a scan, then per sector a synchronous
         # H2D from pinned memory, the kernels and the dump, then close
         s = eng.open_scan(c)
         b = c.bpf(2)
-        sf = j["sector_frames"]
+        sf = j["sector_frames"] or j["nf"]
         for f0 in range(0, j["nf"], sf):
             n = min(sf, j["nf"] - f0)
             s.wait(s.submit(p1[f0 * b:(f0 + n) * b], p2[f0 * b:(f0 + n) * b], n, f0))
@@ -355,7 +376,7 @@ def serve_leg(fxc, torch, eng, n_jobs=20, load=2.0, slots=4):
     def run_plain(paced):
         lat = []
         t0 = time.perf_counter()
-        for j, c in zip(jobs, cfgs):
+        for j, c in list(zip(jobs, cfgs))[:np_jobs]:
             arr = t0 + (j["arrival"] if paced else 0.0)
             now = time.perf_counter()
             if now < arr:
@@ -364,10 +385,13 @@ def serve_leg(fxc, torch, eng, n_jobs=20, load=2.0, slots=4):
             lat.append(time.perf_counter() - arr)
         return lat, time.perf_counter() - t0
 
-    sv = fxc.Server(eng, slots=slots)  # long-lived: slots keep their device state
+    sv = fxc.Server(eng, slots=slots, batch=batch)  # long-lived: slots keep their device state
+
+    cfg_cs = [c.to_c() for c in cfgs]  # the client's structs, built once
 
     def run_served(paced):
         ids = [None] * len(jobs)
+        ready = [threading.Event() for _ in jobs]
         t0 = time.perf_counter()
 
         def submitter():
@@ -377,50 +401,61 @@ def serve_leg(fxc, torch, eng, n_jobs=20, load=2.0, slots=4):
                     if dt > 0:
                         time.sleep(dt)
                 b = c.bpf(2) * j["nf"]
-                ids[k] = sv.submit(c, p1[:b], p2[:b], j["nf"], 0, j["sector_frames"])
+                ids[k] = sv.submit(c, p1[:b], p2[:b], j["nf"], 0, j["sector_frames"],
+                                   cfg_c=cfg_cs[k])
+                ready[k].set()
 
         th = threading.Thread(target=submitter)
         th.start()
+        st = []
+        for k in range(len(jobs)):  # waits run beside the submissions
+            ready[k].wait()
+            st.append(sv.wait(ids[k])[1])
         th.join()
-        st = [sv.wait(i)[1] for i in ids]
-        wall = time.perf_counter() - t0
         for x in st:
             if x["status"] != 0:
                 raise RuntimeError(f"served job failed: {x}")
+        # the server's own clock: first submission to last completion
+        wall = (max(x["t_done_ns"] for x in st) - min(x["t_submit_ns"] for x in st)) * 1e-9
         return [x["latency_s"] for x in st], wall
 
-    # warm both paths (module load; the server's slots grow to the job mix)
-    plain_job(jobs[0], cfgs[0])
-    run_served(False)
-    run_served(False)
-    # saturated: every job queued at once, median of three runs each
-    p_sat_wall = statistics.median(run_plain(False)[1] for _ in range(3))
-    s_sat_wall = statistics.median(run_served(False)[1] for _ in range(3))
-    s_lat, s_wall = run_served(True)
-    p_lat, p_wall = run_plain(True)
-    sv.close()
+    try:
+        # warm both paths (module load; the server's slots grow to the job mix
+        # and the batch autotuner runs at its first batch of each FFT length)
+        plain_job(jobs[0], cfgs[0])
+        run_served(False)
+        run_served(False)
+        # saturated: every job queued at once, median of three runs each
+        p_sat_wall = statistics.median(run_plain(False)[1] for _ in range(3))
+        s_sat_wall = statistics.median(run_served(False)[1] for _ in range(3))
+        s_lat, s_wall = run_served(True)
+        p_lat, p_wall = run_plain(True)
+    finally:
+        sv.close()
     tot = float(sum(samples))
+    tot_plain = float(sum(samples[:np_jobs]))
 
     def pct(v, q):
         return float(np.percentile(np.asarray(v) * 1e3, q))
 
+    s_jps, p_jps = len(jobs) / s_sat_wall, np_jobs / p_sat_wall
     return {
-        "jobs": len(jobs), "slots": slots, "offered_load_x_realtime": load,
-        "job_mix": "Poisson arrivals; 0.1-5 s at 256/512/1024 Msps, 2-bit, FFT 1024-16384, "
-                   "random delays/rates, 1-s dumps, pinned host buffers",
+        "workload": label, "jobs": len(jobs), "plain_jobs": np_jobs, "slots": slots,
+        "batched": bool(batch), "job_mix": mix,
         "data_s_per_job_mean": float(np.mean([j["dur"] for j in jobs])),
         "served": {"p50_ms": pct(s_lat, 50), "p99_ms": pct(s_lat, 99),
                    "gsample_s": tot / s_wall / 1e9,
-                   "saturated_jobs_per_s": len(jobs) / s_sat_wall,
+                   "saturated_jobs_per_s": s_jps,
                    "saturated_gsample_s": tot / s_sat_wall / 1e9},
         "plain": {"p50_ms": pct(p_lat, 50), "p99_ms": pct(p_lat, 99),
-                  "gsample_s": tot / p_wall / 1e9,
-                  "saturated_jobs_per_s": len(jobs) / p_sat_wall,
-                  "saturated_gsample_s": tot / p_sat_wall / 1e9},
-        "saturated_job_throughput_ratio": p_sat_wall / s_sat_wall,
+                  "gsample_s": tot_plain / p_wall / 1e9,
+                  "saturated_jobs_per_s": p_jps,
+                  "saturated_gsample_s": tot_plain / p_sat_wall / 1e9},
+        "saturated_job_throughput_ratio": s_jps / p_jps,
         "saturated_runs": "median of 3 per path",
-        "path": "fxc_server_submit/fxc_server_wait vs fxc_scan_open + per-sector synchronous "
-                "fxc_sector_submit/wait + fxc_scan_close",
+        "path": "fxc_server_submit/fxc_server_wait%s vs fxc_scan_open + per-sector synchronous "
+                "fxc_sector_submit/wait + fxc_scan_close" % (
+                    " (batched: fxc_batch_run_device in CUDA graphs, autotuned)" if batch else ""),
     }
 
 
@@ -435,6 +470,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-vs-plain leg")
     ap.add_argument("--serve-jobs", type=int, default=20)
+    ap.add_argument("--serve-short-jobs", type=int, default=2000)
     ap.add_argument("--sectors", type=int, default=SECTORS,
                     help="sectors per step (profiling cases only; the workload is 10)")
     ap.add_argument("--frames-per-sector", type=int, default=NF_SECTOR,
@@ -560,7 +596,25 @@ def main():
     # ---- serving: continuous batching vs one job at a time (rank 0 of N=1)
     serve = None
     if rank == 0 and world == 1 and not args.no_serve:
-        serve = serve_leg(fxc, torch, eng, n_jobs=args.serve_jobs)
+        def guarded(fn):
+            try:
+                return fn()
+            except Exception as e:  # report, keep the rest of the line
+                return {"error": f"{type(e).__name__}: {e}"}
+
+        serve = {
+            # the headline's served vs plain: short 2-bit FFT-8192 jobs, batched server
+            "short": guarded(lambda: serve_leg(
+                fxc, torch, eng, short_jobs(args.serve_short_jobs, rate=4000.0), slots=64,
+                batch=True, plain_jobs=200, label="short jobs, FFT 8192",
+                mix="Poisson arrivals at 4000 jobs/s; 1-16 ms at 1024 Msps (125-2000 frame "
+                    "pairs), 2-bit, FFT 8192, random delays/rates, one dump, pinned host buffers")),
+            "long": guarded(lambda: serve_leg(
+                fxc, torch, eng, serve_jobs(args.serve_jobs, 2.0), slots=4, batch=True,
+                label="long jobs, mixed FFT",
+                mix="Poisson arrivals at 2x real time; 0.1-5 s at 256/512/1024 Msps, 2-bit, "
+                    "FFT 1024-16384, random delays/rates, 1-s dumps, pinned host buffers")),
+        }
 
     # ---- roofline of the dominant kernel (correlation kernel, one sector per launch)
     launch_ms = kern_ms / max(1, kern_launches)

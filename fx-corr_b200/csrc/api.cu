@@ -66,6 +66,7 @@ struct fxc_engine {
   std::mutex mu;
   std::vector<fxc_scan*> scans;  // open scans, closed by fxc_engine_destroy
   std::vector<fxc_server*> servers;  // live servers, destroyed first by fxc_engine_destroy
+  std::vector<fxc_batch*> batches;   // live batches, destroyed next
 };
 
 struct SectorSlot {
@@ -233,9 +234,8 @@ CorrParams corr_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2, 
   return p;
 }
 
-// Per-frame delay records for nf frames starting at `first` (FP64 delay model,
-// one thread per frame) into the scan's record buffer, on stream st.
-fxc_status stage_frame_info(fxc_scan* s, uint64_t first, uint64_t nf, cudaStream_t st) {
+// Room for nf frame records in the scan's record buffer.
+fxc_status grow_frame_info(fxc_scan* s, uint64_t nf) {
   if (nf > s->finfo_cap) {
     // growing frees the old buffer; cudaFree waits for the work that reads it
     cudaFree(s->d_finfo);
@@ -245,6 +245,14 @@ fxc_status stage_frame_info(fxc_scan* s, uint64_t first, uint64_t nf, cudaStream
     CK(cudaMalloc(&s->d_finfo, cap * sizeof(FrameInfo)));
     s->finfo_cap = cap;
   }
+  return FXC_OK;
+}
+
+// Per-frame delay records for nf frames starting at `first` (FP64 delay model,
+// one thread per frame) into the scan's record buffer, on stream st.
+fxc_status stage_frame_info(fxc_scan* s, uint64_t first, uint64_t nf, cudaStream_t st) {
+  const fxc_status g = grow_frame_info(s, nf);
+  if (g != FXC_OK) return g;
   CK(launch_frame_info(delay_params(s), first, nf, (int)s->n, s->cfg.fs_hz / (double)s->n,
                        (int)s->cfg.a1s, (int)s->cfg.a2s, s->d_finfo, st));
   return FXC_OK;
@@ -509,9 +517,101 @@ fxc_status grow_charged(fxc_scan* s, uint8_t** p, uint64_t* cap, uint64_t need) 
   return FXC_OK;
 }
 
+// Takes a free sector slot of scan s and copies the sector's host inputs
+// into its device buffers on the scan's copy stream (event ev_h2d after).
+fxc_status stage_sector(fxc_scan* s, const uint8_t* raw1, uint64_t n1, const uint8_t* raw2,
+                        uint64_t n2, uint64_t nf, SectorSlot** out) {
+  if (nf && (!raw1 || !raw2)) return fail(FXC_EINVAL, "input buffer is NULL");
+  const uint64_t need1 = nf * s->bpf1, need2 = nf * s->bpf2;
+  if (n1 < need1 || n2 < need2)
+    return fail(FXC_EINVAL, "input too short: need %llu / %llu bytes for %llu frames",
+                (unsigned long long)need1, (unsigned long long)need2, (unsigned long long)nf);
+  SectorSlot* sl = nullptr;
+  for (auto& x : s->slots)
+    if (!x.busy) {
+      sl = &x;
+      break;
+    }
+  if (!sl) return fail(FXC_EBUSY, "all %zu sector slots are in flight; wait for one first",
+                       s->slots.size());
+  fxc_status st;
+  if ((st = grow_charged(s, &sl->d_raw1, &sl->cap1, need1)) != FXC_OK) return st;
+  if ((st = grow_charged(s, &sl->d_raw2, &sl->cap2, need2)) != FXC_OK) return st;
+  if (nf) {
+    CK(cudaMemcpyAsync(sl->d_raw1, raw1, need1, cudaMemcpyHostToDevice, s->copy_stream));
+    CK(cudaMemcpyAsync(sl->d_raw2, raw2, need2, cudaMemcpyHostToDevice, s->copy_stream));
+  }
+  const bool raw = (s->cfg.products & FXC_PROD_RAW) != 0;
+  const uint64_t need_o = nf * s->bpfo;
+  if (raw) {
+    if ((st = grow_charged(s, &sl->d_rawout, &sl->cap_out, need_o)) != FXC_OK) return st;
+    if ((st = grow_host(&sl->h_rawout, &sl->hcap_out, need_o)) != FXC_OK) return st;
+  }
+  CK(cudaEventRecord(sl->ev_h2d, s->copy_stream));
+  sl->nf = nf;
+  *out = sl;
+  return FXC_OK;
+}
+
+// Device-to-host copies of a computed sector (ordered on the scan's compute
+// stream), then ev_done; marks the slot in flight under a new id.
+fxc_status collect_sector(fxc_scan* s, SectorSlot* sl) {
+  const bool raw = (s->cfg.products & FXC_PROD_RAW) != 0;
+  const uint64_t need_o = sl->nf * s->bpfo;
+  CK(cudaMemcpyAsync(sl->h_acc, sl->d_acc, sizeof(double) * 5 * s->h, cudaMemcpyDeviceToHost,
+                     s->stream));
+  if (raw && need_o)
+    CK(cudaMemcpyAsync(sl->h_rawout, sl->d_rawout, need_o, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(sl->h_acc) + sizeof(double) * 5 * s->h, s->d_err,
+                     4, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaEventRecord(sl->ev_done, s->stream));
+  sl->busy = true;
+  sl->id = s->next_id++;
+  return FXC_OK;
+}
+
 }  // namespace
 
 namespace fxc {
+
+fxc_status sector_stage(fxc_scan* s, const uint8_t* raw1, uint64_t n1, const uint8_t* raw2,
+                        uint64_t n2, uint64_t nf, StagedSector* out) {
+  if (!s || !out) return fail(FXC_EINVAL, "NULL argument");
+  if (s->cfg.products & FXC_PROD_RAW)
+    return fail(FXC_EINVAL, "staged sectors do not write phased .raw frames");
+  DeviceGuard g(s->eng->device);
+  SectorSlot* sl = nullptr;
+  fxc_status st = stage_sector(s, raw1, n1, raw2, n2, nf, &sl);
+  if (st != FXC_OK) return st;
+  sl->busy = true;  // reserved until sector_collect
+  out->slot = (uint32_t)(sl - s->slots.data());
+  out->d_raw1 = sl->d_raw1;
+  out->d_raw2 = sl->d_raw2;
+  out->d_acc = sl->d_acc;
+  out->h2d = sl->ev_h2d;
+  return FXC_OK;
+}
+
+fxc_status sector_collect(fxc_scan* s, const StagedSector& ss, cudaEvent_t computed,
+                          uint64_t* sector_id) {
+  DeviceGuard g(s->eng->device);
+  SectorSlot* sl = &s->slots[ss.slot];
+  sl->busy = false;
+  if (computed) CK(cudaStreamWaitEvent(s->stream, computed, 0));
+  const fxc_status st = collect_sector(s, sl);
+  if (st != FXC_OK) return st;
+  *sector_id = sl->id;
+  return FXC_OK;
+}
+
+void sector_release(fxc_scan* s, const StagedSector& ss) {
+  DeviceGuard g(s->eng->device);
+  SectorSlot* sl = &s->slots[ss.slot];
+  cudaEventSynchronize(sl->ev_h2d);  // its copies may still be in flight
+  sl->busy = false;
+}
+
+fxc_status upload_tables(fxc_scan* s, const fxc_scan_cfg* cfg, uint64_t tlen);
 
 // Binds scan s to cfg: derived sizes, buffers grown (and charged to the HBM
 // budget) where the new configuration needs more, tables uploaded on the
@@ -581,7 +681,37 @@ fxc_status scan_bind(fxc_scan* s, const fxc_scan_cfg* cfg) {
     }
     s->acc_cap = h;
   }
-  // tables into pinned staging, then one async upload each
+  // the decode tables of a scan rebound to the same levels and shuffles are
+  // already on the device (the serving loop's common case)
+  const bool reuse = s->n != 0 && tlen == 0 && cfg->nlevels1 == s->cfg.nlevels1 &&
+                     cfg->nlevels2 == s->cfg.nlevels2 &&
+                     !std::memcmp(cfg->levels1, s->cfg.levels1, 8 * cfg->nlevels1) &&
+                     !std::memcmp(cfg->levels2, s->cfg.levels2, 8 * cfg->nlevels2) &&
+                     !std::memcmp(cfg->shuffle1, s->cfg.shuffle1, 32) &&
+                     !std::memcmp(cfg->shuffle2, s->cfg.shuffle2, 32);
+  if (!reuse && (st = upload_tables(s, cfg, tlen)) != FXC_OK) return st;
+
+  s->cfg = *cfg;
+  s->cfg.delay.geom_table = nullptr;  // the host pointer is not kept
+  s->table_bound = tlen != 0;
+  s->n = n;
+  s->h = h;
+  s->bpf1 = (uint32_t)fxc_bytes_per_frame(n, cfg->bits1);
+  s->bpf2 = (uint32_t)fxc_bytes_per_frame(n, cfg->bits2);
+  s->bpfo = (uint32_t)fxc_bytes_per_frame(n, cfg->bits_out);
+  s->shkind[0] = shuffle_kind(cfg->shuffle1);
+  s->shkind[1] = shuffle_kind(cfg->shuffle2);
+  s->scale[0] = level_scale(cfg->levels1, cfg->nlevels1);
+  s->scale[1] = level_scale(cfg->levels2, cfg->nlevels2);
+  s->partials_elems = pel;
+  s->big_frames = bigf;
+  return FXC_OK;
+}
+
+// Decode / re-quantiser tables and the geometric table into pinned staging,
+// then one async upload each on the scan's compute stream.
+fxc_status upload_tables(fxc_scan* s, const fxc_scan_cfg* cfg, uint64_t tlen) {
+  fxc_status st;
   constexpr uint64_t kLut = 0, kLv = 8192, kSh = kLv + 2048, kQl = kSh + 32, kEnc = kQl + 1024,
                      kTab = kEnc + 4096;
   if ((st = grow_host(&s->h_tab, &s->h_tab_cap, kTab + tlen * 8)) != FXC_OK) return st;
@@ -622,24 +752,10 @@ fxc_status scan_bind(fxc_scan* s, const fxc_scan_cfg* cfg) {
   CK(cudaEventRecord(ev, s->stream));
   CK(cudaStreamWaitEvent(s->copy_stream, ev, 0));
   cudaEventDestroy(ev);
-
-  s->cfg = *cfg;
-  s->cfg.delay.geom_table = nullptr;  // the host pointer is not kept
-  s->table_bound = tlen != 0;
   s->qmonotonic = up ? 1 : (down ? -1 : 0);
-  s->n = n;
-  s->h = h;
-  s->bpf1 = (uint32_t)fxc_bytes_per_frame(n, cfg->bits1);
-  s->bpf2 = (uint32_t)fxc_bytes_per_frame(n, cfg->bits2);
-  s->bpfo = (uint32_t)fxc_bytes_per_frame(n, cfg->bits_out);
-  s->shkind[0] = shuffle_kind(cfg->shuffle1);
-  s->shkind[1] = shuffle_kind(cfg->shuffle2);
-  s->scale[0] = level_scale(cfg->levels1, cfg->nlevels1);
-  s->scale[1] = level_scale(cfg->levels2, cfg->nlevels2);
-  s->partials_elems = pel;
-  s->big_frames = bigf;
   return FXC_OK;
 }
+
 
 }  // namespace fxc
 
@@ -698,6 +814,12 @@ fxc_status fxc_engine_destroy(fxc_engine* e) {
     live = e->servers;
   }
   for (fxc_server* sv : live) fxc_server_destroy(sv);
+  std::vector<fxc_batch*> bl;
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    bl = e->batches;
+  }
+  for (fxc_batch* b : bl) fxc_batch_destroy(b);
   std::vector<fxc_scan*> open;
   {
     std::lock_guard<std::mutex> lk(e->mu);
@@ -739,7 +861,8 @@ fxc_status fxc_scan_open(fxc_engine* e, const fxc_scan_cfg* cfg, fxc_scan** out)
   s->slots.resize((size_t)e->max_inflight);
   for (auto& sl : s->slots) {
     CKS(cudaEventCreateWithFlags(&sl.ev_h2d, cudaEventDisableTiming));
-    CKS(cudaEventCreateWithFlags(&sl.ev_done, cudaEventDisableTiming));
+    // a waiting host thread sleeps until the sector is done instead of polling
+    CKS(cudaEventCreateWithFlags(&sl.ev_done, cudaEventDisableTiming | cudaEventBlockingSync));
   }
 #undef CKS
   {
@@ -918,48 +1041,16 @@ fxc_status fxc_spectra_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t*
 fxc_status fxc_sector_submit(fxc_scan* s, const uint8_t* raw1, uint64_t n1, const uint8_t* raw2,
                              uint64_t n2, uint64_t nf, uint64_t first_frame, uint64_t* sector_id) {
   if (!s || !sector_id) return fail(FXC_EINVAL, "NULL argument");
-  if (nf && (!raw1 || !raw2)) return fail(FXC_EINVAL, "input buffer is NULL");
-  const uint64_t need1 = nf * s->bpf1, need2 = nf * s->bpf2;
-  if (n1 < need1 || n2 < need2)
-    return fail(FXC_EINVAL, "input too short: need %llu / %llu bytes for %llu frames",
-                (unsigned long long)need1, (unsigned long long)need2, (unsigned long long)nf);
-  SectorSlot* sl = nullptr;
-  for (auto& x : s->slots)
-    if (!x.busy) {
-      sl = &x;
-      break;
-    }
-  if (!sl) return fail(FXC_EBUSY, "all %zu sector slots are in flight; wait for one first",
-                       s->slots.size());
   DeviceGuard g(s->eng->device);
-  fxc_status st;
-  if ((st = grow_charged(s, &sl->d_raw1, &sl->cap1, need1)) != FXC_OK) return st;
-  if ((st = grow_charged(s, &sl->d_raw2, &sl->cap2, need2)) != FXC_OK) return st;
-  if (nf) {
-    CK(cudaMemcpyAsync(sl->d_raw1, raw1, need1, cudaMemcpyHostToDevice, s->copy_stream));
-    CK(cudaMemcpyAsync(sl->d_raw2, raw2, need2, cudaMemcpyHostToDevice, s->copy_stream));
-  }
+  SectorSlot* sl = nullptr;
+  fxc_status st = stage_sector(s, raw1, n1, raw2, n2, nf, &sl);
+  if (st != FXC_OK) return st;
   const bool raw = (s->cfg.products & FXC_PROD_RAW) != 0;
-  const uint64_t need_o = nf * s->bpfo;
-  if (raw) {
-    if ((st = grow_charged(s, &sl->d_rawout, &sl->cap_out, need_o)) != FXC_OK) return st;
-    if ((st = grow_host(&sl->h_rawout, &sl->hcap_out, need_o)) != FXC_OK) return st;
-  }
-  CK(cudaEventRecord(sl->ev_h2d, s->copy_stream));
   CK(cudaStreamWaitEvent(s->stream, sl->ev_h2d, 0));
   st = run_sector_device(s, sl->d_raw1, sl->d_raw2, nf, first_frame, sl->d_acc,
                          raw ? sl->d_rawout : nullptr, s->stream);
   if (st != FXC_OK) return st;
-  CK(cudaMemcpyAsync(sl->h_acc, sl->d_acc, sizeof(double) * 5 * s->h, cudaMemcpyDeviceToHost,
-                     s->stream));
-  if (raw && need_o)
-    CK(cudaMemcpyAsync(sl->h_rawout, sl->d_rawout, need_o, cudaMemcpyDeviceToHost, s->stream));
-  CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(sl->h_acc) + sizeof(double) * 5 * s->h, s->d_err,
-                     4, cudaMemcpyDeviceToHost, s->stream));
-  CK(cudaEventRecord(sl->ev_done, s->stream));
-  sl->busy = true;
-  sl->nf = nf;
-  sl->id = s->next_id++;
+  if ((st = collect_sector(s, sl)) != FXC_OK) return st;
   *sector_id = sl->id;
   return FXC_OK;
 }
@@ -973,6 +1064,10 @@ fxc_status fxc_sector_wait(fxc_scan* s, uint64_t sector_id, int32_t timeout_ms,
   if (!sl) return fail(FXC_ENOTFOUND, "sector id %llu is not in flight", (unsigned long long)sector_id);
   DeviceGuard g(s->eng->device);
   const auto t0 = std::chrono::steady_clock::now();
+  if (timeout_ms < 0) {
+    const cudaError_t q = cudaEventSynchronize(sl->ev_done);
+    if (q != cudaSuccess) return fail(FXC_ECUDA, "sector failed: %s", cudaGetErrorString(q));
+  }
   for (;;) {
     cudaError_t q = cudaEventQuery(sl->ev_done);
     if (q == cudaSuccess) break;
@@ -1098,6 +1193,71 @@ fxc_status fxc_normalize(uint32_t fft, uint64_t nf, double level_power, const do
 namespace fxc {
 
 fxc_status internal_fail(fxc_status s, const char* msg) { return fail(s, "%s", msg); }
+
+int engine_sm_count(const fxc_engine* e) { return e->sm_count; }
+int engine_device(const fxc_engine* e) { return e->device; }
+fxc_engine* scan_engine(const fxc_scan* s) { return s->eng; }
+
+fxc_status engine_reserve(fxc_engine* e, uint64_t bytes) {
+  std::lock_guard<std::mutex> lk(e->mu);
+  if (e->in_use + bytes > e->budget)
+    return fail(FXC_EBUSY, "HBM budget exhausted (%llu + %llu > %llu bytes)",
+                (unsigned long long)e->in_use, (unsigned long long)bytes,
+                (unsigned long long)e->budget);
+  e->in_use += bytes;
+  return FXC_OK;
+}
+
+void engine_release(fxc_engine* e, uint64_t bytes) {
+  std::lock_guard<std::mutex> lk(e->mu);
+  e->in_use -= std::min(e->in_use, bytes);
+}
+
+fxc_status batch_describe(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
+                          uint64_t first, double* d_acc, BatchScan* out, int* group) {
+  *group = -1;
+  if (!d_acc) return fail(FXC_EINVAL, "d_acc is NULL");
+  fxc_status st = nf ? check_device_inputs(s, r1, r2) : FXC_OK;
+  if (st != FXC_OK) return st;
+  const bool corr = (s->cfg.products & (FXC_PROD_ACF | FXC_PROD_XCF)) != 0;
+  const bool phased = (s->cfg.products & (FXC_PROD_PHASED | FXC_PROD_RAW)) != 0;
+  if (nf == 0 || !corr || phased || s->n > 16384) return FXC_OK;
+  CorrParams p = corr_params(s, r1, r2, nf, first);
+  if (s->n == 16384 && !corr_fold2_supported(p)) return FXC_OK;
+  if ((st = grow_frame_info(s, nf)) != FXC_OK) return st;
+  p.finfo = s->d_finfo;
+  p.partials = nullptr;  // the batch's
+  BatchScan b{};
+  b.p = p;
+  b.acc = d_acc;
+  const double u1 = 1.0 / s->scale[0], u2 = 1.0 / s->scale[1];
+  b.m11 = 0.25 * u1 * u1;
+  b.m22 = 0.25 * u2 * u2;
+  b.m12 = 0.25 * u1 * u2;
+  b.n = s->n;
+  b.h = s->h;
+  *out = b;
+  *group = s->n == 1024 ? BG_1024 : s->n == 2048 ? BG_2048 : s->n == 4096 ? BG_4096
+         : s->n == 8192 ? BG_8192 : BG_16384;
+  return FXC_OK;
+}
+
+fxc_status run_sector_internal(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
+                               uint64_t first, double* d_acc, cudaStream_t st) {
+  const fxc_status c = nf ? check_device_inputs(s, r1, r2) : FXC_OK;
+  if (c != FXC_OK) return c;
+  if (!d_acc) return fail(FXC_EINVAL, "d_acc is NULL");
+  if (s->cfg.products & FXC_PROD_RAW)
+    return fail(FXC_EINVAL, "a batch does not write phased .raw frames; use fxc_sector_run_device");
+  return run_sector_device(s, r1, r2, nf, first, d_acc, nullptr, st);
+}
+
+void engine_track_batch(fxc_engine* e, fxc_batch* b, bool add) {
+  std::lock_guard<std::mutex> lk(e->mu);
+  auto& v = e->batches;
+  if (add) v.push_back(b);
+  else v.erase(std::remove(v.begin(), v.end(), b), v.end());
+}
 
 void engine_track_server(fxc_engine* e, fxc_server* sv, bool add) {
   std::lock_guard<std::mutex> lk(e->mu);

@@ -161,18 +161,68 @@ __device__ __forceinline__ void fold_station(int bits, bool split, const uint32_
   }
 }
 
-}  // namespace
 
-// ROWS = 1: FFT 8192.  ROWS = 2: FFT 16384 as two 8192-point rows (the radix-2
-// DIF step fused into the decode); one launch per row, `row` = 0 handles the
-// even bins, 1 the odd bins, both accumulate into the same per-CTA partials.
+// Per-CTA state of the fold kernels that does not depend on the scan: the
+// twiddle power chains, the two-row DIF twiddle bases, and the number of
+// staging iterations consumed so far (it sets the mbarrier slot and phase, so
+// a persistent CTA can run spans of several scans back to back).
 template <int ROWS>
-__global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, int row) {
+struct FoldCta {
+  Twiddles<kN> tw;
+  float2 dtw0, dtw1, wb1;
+  uint32_t seq;
+};
+
+template <int ROWS>
+__device__ __forceinline__ void fold_cta_init(uint8_t* smem, FoldCta<ROWS>& c) {
+  const int tid = threadIdx.x;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
+  int* flag = reinterpret_cast<int*>(smem + kOffFlag);
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    *flag = 0;
+    fence_proxy_async();
+  }
+  c.tw.init(tid);
+  // ROWS = 2: row-1 DIF twiddle bases W_NF^t, W_NF^(t+512) (= W^t W_32) and
+  // the row-1 fold's W_M^(t+1); all correctly rounded from FP64
+  c.dtw0 = make_float2(1.f, 0.f);
+  c.dtw1 = c.dtw0;
+  c.wb1 = c.dtw0;
+  if constexpr (ROWS == 2) {
+    constexpr int NF = 2 * kN;
+    double sn, cs;
+    sincospi(-2.0 * (double)tid / (double)NF, &sn, &cs);
+    c.dtw0 = make_float2((float)cs, (float)sn);
+    sincospi(-2.0 * (double)(tid + NF / 32) / (double)NF, &sn, &cs);
+    c.dtw1 = make_float2((float)cs, (float)sn);
+    sincospi(-2.0 * (double)(tid + 1) / (double)kN, &sn, &cs);
+    c.wb1 = make_float2((float)cs, (float)sn);
+  }
+  c.seq = 0;
+}
+
+// Never leave a bulk copy in flight into a finished CTA's shared memory.
+__device__ __forceinline__ void fold_cta_drain(uint8_t* smem) {
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
+  const int* flag = reinterpret_cast<const int*>(smem + kOffFlag);
+  if (threadIdx.x == 0 && *flag) {
+    for (int s = 0; s < kStages; ++s) mbar_wait(&bars[s], 0, kWaitPolls);
+  }
+}
+
+// Frame pairs [it0, it1) of the sector described by p (ROWS = 1: FFT 8192;
+// ROWS = 2: FFT 16384 as two 8192-point rows, the radix-2 DIF step fused into
+// the decode, `row` 0 the even bins and 1 the odd bins), accumulated into the
+// f64 partials at part ([4][NF/2 + 1]; each row writes only its own bins).
+// Returns false when a bounded wait gave up (the CTA must stop).
+template <int ROWS>
+__device__ __forceinline__ bool fold_span(const CorrParams& p, int row, uint64_t it0, uint64_t it1,
+                                          double* part, uint8_t* smem, const FoldLayout& L,
+                                          FoldCta<ROWS>& c) {
   constexpr int NF = kN * ROWS;       // frame FFT length
   constexpr int HF = NF / 2 + 1;      // bins
   static_assert(ROWS == 1 || ROWS == 2, "one or two rows");
-  extern __shared__ __align__(128) uint8_t smem[];
-  const FoldLayout L = fold_layout(p.stage_bytes);
   float* lv = reinterpret_cast<float*>(smem);
   uint32_t* pos = reinterpret_cast<uint32_t*>(smem + kOffPos);
   FrameInfo* finfo = reinterpret_cast<FrameInfo*>(smem + kOffFi);
@@ -183,6 +233,8 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, in
   float2* bufB = reinterpret_cast<float2*>(smem + L.off_b);
   uint8_t* stage = smem + L.off_stage;
   const int tid = threadIdx.x;
+  const Twiddles<kN>& tw = c.tw;
+  const uint32_t seq0 = c.seq;
 
   // primary station (real part of the FFT, products indexed on its bins) first
   const bool g0 = p.grid == 0;
@@ -194,25 +246,27 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, in
   const bool preP = bitsP > 2 && sp.shkind != SH_IDENTITY;
   const bool preS = bitsS > 2 && ss.shkind != SH_IDENTITY;
 
-  // ---- constant tables
+  // ---- constant tables of this scan (the previous span, if any, has passed
+  // its last decode: every thread is past its barriers)
+  __syncthreads();
   for (int i = tid; i < 1024; i += kT) {
     // per station: 2^b levels, then their negations (the two sign groups of a
     // warp's table loads fall in different banks)
     const StationParams& q = (i < 512) ? sp : ss;
-    const int n = 1 << q.bits, c = i & 511;
-    const float x = c < 2 * n ? q.levels[c & (n - 1)] * q.scale : 0.0f;
-    lv[i] = c >= n ? -x : x;
+    const int n = 1 << q.bits, c2 = i & 511;
+    const float x = c2 < 2 * n ? q.levels[c2 & (n - 1)] * q.scale : 0.0f;
+    lv[i] = c2 >= n ? -x : x;
   }
   for (int i = tid; i < 64; i += kT) {
     // rotate amounts of sample slot c: bit j of the sample is word bit p_j
-    const int k = i >> 5, c = i & 31;
+    const int k = i >> 5, cc = i & 31;
     const StationParams& q = k ? ss : sp;
     const int b = q.bits;
     const bool natural = (k ? preS : preP) || q.shkind == SH_IDENTITY;
     uint32_t r = 0;
-    if (c * b < 32) {
-      const int p0 = natural ? c * b : q.perm[c * b];
-      const int p1 = b >= 2 ? (natural ? c * b + 1 : q.perm[c * b + 1]) : 0;
+    if (cc * b < 32) {
+      const int p0 = natural ? cc * b : q.perm[cc * b];
+      const int p1 = b >= 2 ? (natural ? cc * b + 1 : q.perm[cc * b + 1]) : 0;
       r = (uint32_t)((p0 - 2) & 31) | ((uint32_t)((p1 - 3) & 31) << 8);
     }
     pos[i] = r;
@@ -225,44 +279,24 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, in
   // a 2-bit shuffle keeps every sample's two bits adjacent and in order, or not
   auto split2 = [](const StationParams& q) {
     if (q.bits != 2 || q.shkind == SH_IDENTITY) return false;
-    for (int c = 0; c < 16; ++c)
-      if (q.perm[2 * c + 1] != q.perm[2 * c] + 1 || (q.perm[2 * c] & 1)) return true;
+    for (int cc = 0; cc < 16; ++cc)
+      if (q.perm[2 * cc + 1] != q.perm[2 * cc] + 1 || (q.perm[2 * cc] & 1)) return true;
     return false;
   };
   const bool splitP = split2(sp), splitS = split2(ss);
-  if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
-    *flag = 0;
-    fence_proxy_async();
-  }
-  Twiddles<kN> tw;
-  tw.init(tid);
-  // ROWS = 2: row-1 DIF twiddle bases W_NF^t, W_NF^(t+512) (= W^t W_32) and
-  // the row-1 fold's W_M^(t+1); all correctly rounded from FP64
-  float2 dtw0 = make_float2(1.f, 0.f), dtw1 = dtw0, wb1 = dtw0;
-  if constexpr (ROWS == 2) {
-    double sn, cs;
-    sincospi(-2.0 * (double)tid / (double)NF, &sn, &cs);
-    dtw0 = make_float2((float)cs, (float)sn);
-    sincospi(-2.0 * (double)(tid + NF / 32) / (double)NF, &sn, &cs);
-    dtw1 = make_float2((float)cs, (float)sn);
-    sincospi(-2.0 * (double)(tid + 1) / (double)kN, &sn, &cs);
-    wb1 = make_float2((float)cs, (float)sn);
-  }
+  const float2 dtw0 = c.dtw0, dtw1 = c.dtw1, wb1 = c.wb1;
 
-  const uint64_t iters = p.nf;
-  const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
-  const uint64_t it1 = ((blockIdx.x + 1) * iters) / gridDim.x;
   const uint32_t bpfP = sp.bpf, bpfS = ss.bpf;
   const uint8_t* rawP = sp.raw;
   const uint8_t* rawS = ss.raw;
+  const FrameInfo* gfi = p.finfo;
 
   // slot: [FrameInfo][primary frame][secondary frame]
   auto issue = [&](uint64_t it) {
-    const int slot = (int)((it - it0) % kStages);
+    const int slot = (int)((seq0 + (uint32_t)(it - it0)) % kStages);
     uint8_t* dst = stage + slot * L.stage_stride;
     mbar_expect_tx(&bars[slot], kFiBytes + bpfP + bpfS);
-    bulk_g2s(dst, p.finfo + it, kFiBytes, &bars[slot]);
+    bulk_g2s(dst, gfi + it, kFiBytes, &bars[slot]);
     bulk_g2s(dst + kFiBytes, rawP + it * bpfP, bpfP, &bars[slot]);
     bulk_g2s(dst + kFiBytes + bpfP, rawS + it * bpfS, bpfS, &bars[slot]);
   };
@@ -287,9 +321,10 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, in
   const bool ov_only = (p.products & 16u) != 0;
   const float xconj = g0 ? 1.0f : -1.0f;  // XCF = S1 conj(S2): conj(P conj(S)) for grid 1
   const int lsbP = sp.lsb ? 1 : 0, lsbS = ss.lsb ? 1 : 0;
+  const uint32_t flush_every = p.flush_every;
+  uint32_t* err = p.err;
   bool first_flush = true;
   uint32_t since_flush = 0;
-  double* part = p.partials + (size_t)blockIdx.x * 4 * HF;
   const int colP = g0 ? 0 : 1, colS = g0 ? 1 : 0;  // output columns of the two ACFs
 
   auto flush = [&]() {
@@ -313,13 +348,15 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, in
     since_flush = 0;
   };
 
+  bool ok = true;
   for (uint64_t it = it0; it < it1; ++it) {
-    const int slot = (int)((it - it0) % kStages);
-    const uint32_t parity = (uint32_t)(((it - it0) / kStages) & 1u);
-    const int fb = (int)((it - it0) & 1u);
+    const uint32_t q_it = seq0 + (uint32_t)(it - it0);
+    const int slot = (int)(q_it % kStages);
+    const uint32_t parity = (q_it / kStages) & 1u;
+    const int fb = (int)(q_it & 1u);
     if (!mbar_wait(&bars[slot], parity, kWaitPolls)) {
       atomicOr(flag, 1);
-      atomicOr(p.err, ERR_WAIT_TIMEOUT);
+      atomicOr(err, ERR_WAIT_TIMEOUT);
     }
     uint8_t* st = stage + slot * L.stage_stride;
     uint32_t* wP = reinterpret_cast<uint32_t*>(st + kFiBytes);
@@ -378,7 +415,10 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, in
     }
     float2* Q = (Y == bufA) ? bufB : bufA;  // free buffer: secondary spectrum by bin
     __syncthreads();
-    if (*flag) break;  // no thread writes the flag before the next barrier
+    if (*flag) {  // no thread writes the flag before the next barrier
+      ok = false;
+      break;
+    }
 
     // ---- trailing radix-2 pass + two-for-one split (x2) at the bin pairs
     const FrameInfo& F = finfo[fb];
@@ -422,7 +462,7 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, in
       // pair from Y[c0], Y[c0 + M/2] with c0 = M/2 - j (one row: mirror of
       // column j is M - j) or M/2 - 1 - j (odd row: mirror is M - 1 - j)
       const int c0 = (ROWS == 2 && row == 1) ? kN / 2 - 1 - j : kN / 2 - j;
-      const float2 a = Y[j], b = Y[j + kN / 2], c = Y[c0], d = Y[(c0 + kN / 2) & (kN - 1)];
+      const float2 a = Y[j], b = Y[j + kN / 2], cc = Y[c0], d = Y[(c0 + kN / 2) & (kN - 1)];
       // W_M^c0 = -conj(W_M^(M/2 - c0)): W^j for the even mirror, W^(j+1) for the odd one
       float2 wm = wj;
       if (ROWS == 2 && row == 1) {
@@ -435,9 +475,9 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, in
       }
       const float2 wb = cmul(wj, b), wd = cmulc(d, wm);  // W^j b, conj(W^(M/2-c0)) d
       const float2 zj = cadd(a, wb), zjh = csub(a, wb);  // Z[j], Z[j + M/2]
-      const float2 zmn = cadd(c, wd);                    // Z[c0 + M/2] (mirror of j)
+      const float2 zmn = cadd(cc, wd);                   // Z[c0 + M/2] (mirror of j)
       // Z[c0]; for an even row and j = 0 that is Z[M/2] = Y[0] - Y[M/2]
-      const float2 zm = ((ROWS == 1 || row == 0) && j == 0) ? zjh : csub(c, wd);
+      const float2 zm = ((ROWS == 1 || row == 0) && j == 0) ? zjh : csub(cc, wd);
       // primary = real part: P[k] = (Z[k] + conj Z[N-k]), S[k] = -i (Z[k] - conj Z[N-k])
       const int bu = ROWS * j + row, bd = NF / 2 - ROWS * j - row;  // global bins
       prim[2 * i] = make_float2(zj.x + zmn.x, zj.y - zmn.y);
@@ -479,13 +519,57 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, in
       rdn = cmulc(rdn, rstep);
     }
     if (quarter) bin_acc(NF / 4, prim_q, rq, acc[kSlots - 1]);
-    if (++since_flush >= p.flush_every) flush();
+    if (++since_flush >= flush_every) flush();
   }
   if (since_flush > 0 || first_flush) flush();
-  // never leave a bulk copy in flight into a finished CTA's shared memory
-  if (tid == 0 && *flag) {
-    for (int s = 0; s < kStages; ++s) mbar_wait(&bars[s], 0, kWaitPolls);
+  c.seq = seq0 + (uint32_t)(it1 - it0);
+  return ok;
+}
+
+}  // namespace
+
+// ROWS = 1: FFT 8192.  ROWS = 2: FFT 16384 as two 8192-point rows; one launch
+// per row, `row` = 0 handles the even bins, 1 the odd bins, both accumulate
+// into the same per-CTA partials.
+template <int ROWS>
+__global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, int row) {
+  constexpr int HF = kN * ROWS / 2 + 1;
+  extern __shared__ __align__(128) uint8_t smem[];
+  const FoldLayout L = fold_layout(p.stage_bytes);
+  FoldCta<ROWS> c;
+  fold_cta_init<ROWS>(smem, c);
+  const uint64_t iters = p.nf;
+  const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
+  const uint64_t it1 = ((blockIdx.x + 1) * iters) / gridDim.x;
+  fold_span<ROWS>(p, row, it0, it1, p.partials + (size_t)blockIdx.x * 4 * HF, smem, L, c);
+  fold_cta_drain(smem);
+}
+
+// Batched: a persistent grid takes the items of batch group `grp` by ticket;
+// every item is a frame range of one scan's sector (its own tables, frame
+// records and raw words) with its own partials.  The layout is sized for the
+// largest stage (8-bit stations), so one launch serves every bit depth.
+template <int ROWS>
+__global__ void __launch_bounds__(kT, 1) corr_fold_batch_kernel(const BatchArgs a, int grp) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const FoldLayout L = fold_layout(2u * (uint32_t)(kN * ROWS));
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(smem + kOffFlag + 4);
+  FoldCta<ROWS> c;
+  fold_cta_init<ROWS>(smem, c);
+  const uint32_t n_items = a.hdr->nitems[grp];
+  const BatchItem* items = a.hdr->items + a.hdr->item0[grp];
+  const BatchScan* scans = a.hdr->scans;
+  for (;;) {
+    if (threadIdx.x == 0) *ticket = atomicAdd(&a.hdr->ticket[grp], 1u);
+    __syncthreads();
+    const uint32_t k = *ticket;  // fold_span opens with a barrier before the next write
+    if (k >= n_items) break;
+    const BatchItem w = items[k];
+    if (!fold_span<ROWS>(scans[w.scan].p, (int)w.row, w.f0, w.f1, a.partials + w.part, smem, L,
+                         c))
+      break;
   }
+  fold_cta_drain(smem);
 }
 
 uint32_t fold_smem_bytes(uint32_t stage_bytes) { return fold_layout(stage_bytes).total; }
@@ -514,6 +598,33 @@ cudaError_t launch_corr_fold2(const CorrParams& p, int grid, cudaStream_t stream
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+uint32_t fold_batch_smem_bytes(int rows) { return fold_layout(2u * (uint32_t)(kN * rows)).total; }
+
+cudaError_t prepare_fold_batch(int rows) {
+  const int smem = (int)fold_batch_smem_bytes(rows);
+  return rows == 1 ? cudaFuncSetAttribute(corr_fold_batch_kernel<1>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                   : cudaFuncSetAttribute(corr_fold_batch_kernel<2>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+int fold_batch_ctas_per_sm(int rows) {
+  int nb = 0;
+  const cudaError_t e =
+      rows == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, corr_fold_batch_kernel<1>, kT,
+                                                                fold_batch_smem_bytes(1))
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, corr_fold_batch_kernel<2>, kT,
+                                                                fold_batch_smem_bytes(2));
+  return e == cudaSuccess ? nb : 0;
+}
+
+cudaError_t launch_fold_batch(int rows, const BatchArgs& a, int grp, int grid, cudaStream_t s) {
+  const uint32_t smem = fold_batch_smem_bytes(rows);
+  if (rows == 1) corr_fold_batch_kernel<1><<<grid, kT, smem, s>>>(a, grp);
+  else corr_fold_batch_kernel<2><<<grid, kT, smem, s>>>(a, grp);
+  return cudaGetLastError();
 }
 
 }  // namespace fxc

@@ -27,17 +27,44 @@
 
 namespace fxc {
 
+// Per-CTA setup of corr_kernel: mbarriers, error flag, twiddle chains.
+template <int N, int FPC>
+__device__ __forceinline__ void corr_cta_init(const SmemLayout& L, uint8_t* smem, Twiddles<N>& tw) {
+  constexpr int T1 = N / 16;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.off_bar);
+  int* flag = reinterpret_cast<int*>(smem + L.off_flag);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    *flag = 0;
+    fence_proxy_async();
+  }
+  tw.init(threadIdx.x % T1);
+}
+
+__device__ __forceinline__ void corr_cta_drain(const SmemLayout& L, uint8_t* smem) {
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.off_bar);
+  const int* flag = reinterpret_cast<const int*>(smem + L.off_flag);
+  // never leave a bulk copy in flight into a finished CTA's shared memory
+  if (threadIdx.x == 0 && *flag) {
+    for (int s = 0; s < kStages; ++s) mbar_wait(&bars[s], 0, kWaitPolls);
+  }
+}
+
+// Iterations [it0, it1) (FPC frame pairs each, frames below fend) of the
+// sector described by p; MODE_CORR accumulates into the f64 partials at part
+// ([4][H]).  seq counts the staging iterations this CTA consumed before (the
+// mbarrier slot and phase).  Returns false when a bounded wait gave up.
 template <int N, int FPC, int MODE>
-__global__ void __launch_bounds__(FPC * N / 16, (N >= 8192 ? 1 : 2))
-corr_kernel(const CorrParams p) {
+__device__ __forceinline__ bool corr_span(const CorrParams& p, uint64_t it0, uint64_t it1,
+                                          uint64_t fend, double* part, uint8_t* smem,
+                                          const SmemLayout& L, const Twiddles<N>& tw,
+                                          uint32_t& seq, uint32_t flush_every) {
   constexpr int T1 = N / 16;
   constexpr int T = FPC * T1;
   constexpr int H = N / 2 + 1;
   constexpr int BPT = (N / 2) / T;
   static_assert(BPT * T == N / 2 && BPT >= 2, "bins per thread");
 
-  extern __shared__ __align__(128) uint8_t smem[];
-  const SmemLayout L = smem_layout<N, FPC>(p.stage_bytes);
   float2* bufA = reinterpret_cast<float2*>(smem + L.off_a);
   float2* bufB = reinterpret_cast<float2*>(smem + L.off_b);
   uint8_t* stage = smem + L.off_stage;
@@ -50,38 +77,33 @@ corr_kernel(const CorrParams p) {
   const int tid = threadIdx.x;
   const int g = tid / T1;  // frame slot of this thread in an iteration
   const int t = tid % T1;  // thread index within its frame pair
+  const uint32_t seq0 = seq;
 
-  // ---- constant tables: levels (scaled by an exact power of two), shuffle LUTs
+  // ---- constant tables of this scan (the previous span, if any, is done
+  // with them: every thread is past its barriers)
+  __syncthreads();
   for (int i = tid; i < 512; i += T) lv[i] = p.st[i >> 8].levels[i & 255] * p.st[i >> 8].scale;
   for (int s = 0; s < 2; ++s)
     if (p.st[s].shkind == SH_GENERIC)
       for (int i = tid; i < 1024; i += T) lut[s * 1024 + i] = p.st[s].shlut[i];
-  if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
-    *flag = 0;
-    fence_proxy_async();
-  }
-  Twiddles<N> tw;
-  tw.init(t);
 
-  // ---- this CTA's iterations (FPC frame pairs each)
-  const uint64_t iters = (p.nf + FPC - 1) / FPC;
-  const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
-  const uint64_t it1 = ((blockIdx.x + 1) * iters) / gridDim.x;
   const uint32_t bpf1 = p.st[0].bpf, bpf2 = p.st[1].bpf;
+  const uint8_t* raw1 = p.st[0].raw;
+  const uint8_t* raw2 = p.st[1].raw;
+  const FrameInfo* gfi = p.finfo;
   constexpr uint32_t kRaw1 = FPC * kFiBytes;  // offset of station 1 bytes in a slot
 
   auto issue = [&](uint64_t it) {
-    const int slot = (int)((it - it0) % kStages);
+    const int slot = (int)((seq0 + (uint32_t)(it - it0)) % kStages);
     const uint64_t f0 = it * FPC;
-    const uint64_t nvalid = (p.nf - f0) < (uint64_t)FPC ? (p.nf - f0) : (uint64_t)FPC;
+    const uint64_t nvalid = (fend - f0) < (uint64_t)FPC ? (fend - f0) : (uint64_t)FPC;
     const uint32_t bf = (uint32_t)(nvalid * kFiBytes);
     const uint32_t b1 = (uint32_t)(nvalid * bpf1), b2 = (uint32_t)(nvalid * bpf2);
     uint8_t* dst = stage + slot * L.stage_stride;
     mbar_expect_tx(&bars[slot], bf + b1 + b2);
-    bulk_g2s(dst, p.finfo + f0, bf, &bars[slot]);
-    bulk_g2s(dst + kRaw1, p.st[0].raw + f0 * bpf1, b1, &bars[slot]);
-    bulk_g2s(dst + kRaw1 + FPC * bpf1, p.st[1].raw + f0 * bpf2, b2, &bars[slot]);
+    bulk_g2s(dst, gfi + f0, bf, &bars[slot]);
+    bulk_g2s(dst + kRaw1, raw1 + f0 * bpf1, b1, &bars[slot]);
+    bulk_g2s(dst + kRaw1 + FPC * bpf1, raw2 + f0 * bpf2, b2, &bars[slot]);
   };
   __syncthreads();
   if (tid == 0)
@@ -99,9 +121,9 @@ corr_kernel(const CorrParams p) {
   const bool want_acf = (p.products & 1u) != 0;
   const bool want_xcf = (p.products & 2u) != 0;
   const bool ov_only = (p.products & 16u) != 0;
+  uint32_t* err = p.err;
   bool first_flush = true;
   uint32_t since_flush = 0;
-  double* part = p.partials + (size_t)blockIdx.x * 4 * H;
 
   auto flush = [&]() {
 #pragma unroll
@@ -119,15 +141,17 @@ corr_kernel(const CorrParams p) {
     since_flush = 0;
   };
 
+  bool ok = true;
   for (uint64_t it = it0; it < it1; ++it) {
-    const int slot = (int)((it - it0) % kStages);
-    const uint32_t parity = (uint32_t)(((it - it0) / kStages) & 1u);
+    const uint32_t q_it = seq0 + (uint32_t)(it - it0);
+    const int slot = (int)(q_it % kStages);
+    const uint32_t parity = (q_it / kStages) & 1u;
     const uint64_t frame_local = it * FPC + g;
-    const bool valid = frame_local < p.nf;
+    const bool valid = frame_local < fend;
 
     if (!mbar_wait(&bars[slot], parity, kWaitPolls)) {
       atomicOr(flag, 1);
-      atomicOr(p.err, ERR_WAIT_TIMEOUT);
+      atomicOr(err, ERR_WAIT_TIMEOUT);
     }
     uint8_t* st = stage + slot * L.stage_stride;
     uint32_t* w1 = reinterpret_cast<uint32_t*>(st + kRaw1);
@@ -137,7 +161,10 @@ corr_kernel(const CorrParams p) {
                     lut + 1024, tid, T);
     if (t == 0 && valid) finfo[g] = reinterpret_cast<const FrameInfo*>(st)[g];
     __syncthreads();
-    if (*flag) break;
+    if (*flag) {
+      ok = false;
+      break;
+    }
     const int s1 = valid ? finfo[g].s1 : 0;
     const int s2 = valid ? finfo[g].s2 : 0;
     const PackedStation pa{w1 + g * (bpf1 / 4), lv, (uint32_t)p.st[0].bits,
@@ -200,7 +227,7 @@ corr_kernel(const CorrParams p) {
     // ---- MODE_CORR: accumulate every valid frame of the iteration
 #pragma unroll 1
     for (int f = 0; f < FPC; ++f) {
-      if (it * FPC + f >= p.nf) break;
+      if (it * FPC + f >= fend) break;
       const float2* Z = (fin_b ? bufB : bufA) + f * Geom<N>::CSTRIDE;
       const FrameInfo& F = finfo[f];
       // Ramp rotation of owned bin tid + T*i: SFU sin/cos (|angle| <= ~pi,
@@ -258,16 +285,61 @@ corr_kernel(const CorrParams p) {
         bin_acc(N / 2, cmul(F.fr_mix, make_float2(cs, sn)), acc[BPT]);
       }
     }
-    if (++since_flush >= p.flush_every) flush();
+    if (++since_flush >= flush_every) flush();
     __syncthreads();
   }
   if constexpr (MODE == MODE_CORR) {
-    if (since_flush > 0 || first_flush) flush();
+    if (ok && (since_flush > 0 || first_flush)) flush();
   }
-  // never leave a bulk copy in flight into a finished CTA's shared memory
-  if (tid == 0 && *flag) {
-    for (int s = 0; s < kStages; ++s) mbar_wait(&bars[s], 0, kWaitPolls);
+  seq = seq0 + (uint32_t)(it1 - it0);
+  return ok;
+}
+
+template <int N, int FPC, int MODE>
+__global__ void __launch_bounds__(FPC * N / 16, (N >= 8192 ? 1 : 2))
+corr_kernel(const CorrParams p) {
+  constexpr int H = N / 2 + 1;
+  extern __shared__ __align__(128) uint8_t smem[];
+  const SmemLayout L = smem_layout<N, FPC>(p.stage_bytes);
+  Twiddles<N> tw;
+  corr_cta_init<N, FPC>(L, smem, tw);
+  // ---- this CTA's iterations (FPC frame pairs each)
+  const uint64_t iters = (p.nf + FPC - 1) / FPC;
+  const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
+  const uint64_t it1 = ((blockIdx.x + 1) * iters) / gridDim.x;
+  uint32_t seq = 0;
+  corr_span<N, FPC, MODE>(p, it0, it1, p.nf, p.partials + (size_t)blockIdx.x * 4 * H, smem, L, tw,
+                          seq, p.flush_every);
+  corr_cta_drain(L, smem);
+}
+
+// Batched: a persistent grid takes the items of batch group `grp` by ticket;
+// every item is a frame range of one scan's sector (frames aligned to FPC)
+// with its own partials.  The layout is sized for the largest stage (8-bit
+// stations), so one launch serves every bit depth.
+template <int N, int FPC, int MINB>
+__global__ void __launch_bounds__(FPC * N / 16, MINB) corr_batch_kernel(const BatchArgs a, int grp) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const SmemLayout L = smem_layout<N, FPC>(2u * FPC * N);
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(smem + L.off_flag + 4);
+  Twiddles<N> tw;
+  corr_cta_init<N, FPC>(L, smem, tw);
+  const uint32_t n_items = a.hdr->nitems[grp];
+  const BatchItem* items = a.hdr->items + a.hdr->item0[grp];
+  const BatchScan* scans = a.hdr->scans;
+  uint32_t seq = 0;
+  for (;;) {
+    if (threadIdx.x == 0) *ticket = atomicAdd(&a.hdr->ticket[grp], 1u);
+    __syncthreads();
+    const uint32_t k = *ticket;  // corr_span opens with a barrier before the next write
+    if (k >= n_items) break;
+    const BatchItem w = items[k];
+    // f32 accumulators flushed every 32 frames, whatever the variant
+    if (!corr_span<N, FPC, MODE_CORR>(scans[w.scan].p, w.f0 / FPC, (w.f1 + FPC - 1) / FPC, w.f1,
+                                      a.partials + w.part, smem, L, tw, seq, 32u / FPC))
+      break;
   }
+  corr_cta_drain(L, smem);
 }
 
 // Fixed-order sum of the per-CTA partials.  The multipliers (exact powers of
@@ -320,6 +392,62 @@ __global__ void frame_info_kernel(const DelayParams p, uint64_t first, uint64_t 
   out[i] = fi;
 }
 
+// Last sector of the batch whose first frame (bins = false) or first bin
+// (bins = true) is <= x; sectors are numbered in ascending order of both.
+__device__ __forceinline__ uint32_t batch_find(const BatchScan* sc, uint32_t n, uint64_t x,
+                                               bool bins) {
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t m = (lo + hi) >> 1;
+    const uint64_t st = bins ? sc[m].bin0 : sc[m].fi0;
+    if (st <= x) lo = m;
+    else hi = m;
+  }
+  return lo;
+}
+
+// Frame records of every sector of a batch (grid-stride over all frames);
+// also rearms the groups' tickets for the launches that follow.
+__global__ void batch_frame_info_kernel(const BatchArgs a) {
+  const uint32_t ns = a.hdr->nscans;
+  const uint64_t total = a.hdr->nframes;
+  if (blockIdx.x == 0 && threadIdx.x < kBatchGroups) a.hdr->ticket[threadIdx.x] = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += stride) {
+    const BatchScan& b = a.hdr->scans[batch_find(a.hdr->scans, ns, x, false)];
+    const uint64_t i = x - b.fi0;
+    FrameInfo fi;
+    frame_info(b.p.dl, b.p.first_frame + i, (int)b.n, b.p.df_hz, b.p.a1s, b.p.a2s, &fi);
+    const_cast<FrameInfo*>(b.p.finfo)[i] = fi;
+  }
+}
+
+// Fixed-order sum of each sector's item partials (grid-stride over all bins
+// of the batch), with the same multipliers and output layout as
+// reduce_partials_kernel.
+__global__ void batch_reduce_kernel(const BatchArgs a) {
+  const uint32_t ns = a.hdr->nscans;
+  const uint64_t total = a.hdr->nbins;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += stride) {
+    const BatchScan& b = a.hdr->scans[batch_find(a.hdr->scans, ns, x, true)];
+    const uint64_t k = x - b.bin0;
+    const uint64_t h = b.h;
+    const double* q = a.partials + b.part + k;
+    double s[4] = {0, 0, 0, 0};
+    for (uint32_t i = 0; i < b.nparts; ++i, q += 4 * h) {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) s[v] += q[(size_t)v * h];
+    }
+    double* out = b.acc;
+    out[k] = b.m11 * s[0];
+    out[h + k] = b.m22 * s[1];
+    out[2 * h + 2 * k] = b.m12 * s[2];
+    out[2 * h + 2 * k + 1] = b.m12 * s[3];
+    out[4 * h + k] = 0.0;
+  }
+}
+
 // ------------------------------------------------------------- launchers
 
 template <int N, int FPC, int MODE>
@@ -361,6 +489,101 @@ cudaError_t launch_corr(uint32_t n, int mode, const CorrParams& p, int grid, cud
   if (mode == MODE_CORR) return launch_mode<MODE_CORR>(n, p, grid, s);
   if (mode == MODE_SPECTRA) return launch_mode<MODE_SPECTRA>(n, p, grid, s);
   return launch_mode<MODE_DECODE>(n, p, grid, s);
+}
+
+// ------------------------------------------------------- batched launchers
+
+namespace {
+
+// Variants of the batched kernels: FFT length, frames per CTA iteration and
+// resident CTAs per SM (shared memory with 8-bit staging: FPC*N = 1024 ->
+// 32 KB, 2048 -> 54 KB, 4096 -> 95 KB, 8192 -> 183 KB).
+template <int N, int FPC>
+constexpr int batch_minb() {
+  return FPC * N <= 1024 ? 6 : (FPC * N <= 2048 ? 4 : (FPC * N <= 4096 ? 2 : 1));
+}
+
+template <int N, int FPC>
+uint32_t batch_smem() {
+  return smem_layout<N, FPC>(2u * FPC * N).total;
+}
+
+template <int N, int FPC>
+cudaError_t batch_prepare_one() {
+  return cudaFuncSetAttribute(corr_batch_kernel<N, FPC, batch_minb<N, FPC>()>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem<N, FPC>());
+}
+
+template <int N, int FPC>
+int batch_ctas_one() {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, corr_batch_kernel<N, FPC, batch_minb<N, FPC>()>,
+                                                    FPC * N / 16, batch_smem<N, FPC>()) != cudaSuccess)
+    return 0;
+  return nb;
+}
+
+template <int N, int FPC>
+cudaError_t batch_launch_one(const BatchArgs& a, int grp, int grid, cudaStream_t s) {
+  corr_batch_kernel<N, FPC, batch_minb<N, FPC>()><<<grid, FPC * N / 16, batch_smem<N, FPC>(), s>>>(a, grp);
+  return cudaGetLastError();
+}
+
+// Calls f.template operator()<N, FPC>() for the variant (g, fpc); returns
+// cudaErrorInvalidValue for a variant that does not exist.
+#define FXC_BATCH_VARIANTS(g, fpc, CALL)              \
+  switch ((g) * 16 + (fpc)) {                         \
+    case BG_1024 * 16 + 1: return CALL(1024, 1);      \
+    case BG_1024 * 16 + 2: return CALL(1024, 2);      \
+    case BG_1024 * 16 + 4: return CALL(1024, 4);      \
+    case BG_2048 * 16 + 1: return CALL(2048, 1);      \
+    case BG_2048 * 16 + 2: return CALL(2048, 2);      \
+    case BG_2048 * 16 + 4: return CALL(2048, 4);      \
+    case BG_4096 * 16 + 1: return CALL(4096, 1);      \
+    case BG_4096 * 16 + 2: return CALL(4096, 2);      \
+    default: break;                                   \
+  }
+
+}  // namespace
+
+uint32_t fold_batch_smem_bytes(int rows);
+cudaError_t prepare_fold_batch(int rows);
+cudaError_t launch_fold_batch(int rows, const BatchArgs& a, int grp, int grid, cudaStream_t s);
+int fold_batch_ctas_per_sm(int rows);
+
+cudaError_t batch_prepare(int g, int fpc) {
+  if (g == BG_8192 || g == BG_16384) return prepare_fold_batch(g == BG_8192 ? 1 : 2);
+#define FXC_PREP(N, F) batch_prepare_one<N, F>()
+  FXC_BATCH_VARIANTS(g, fpc, FXC_PREP)
+#undef FXC_PREP
+  return cudaErrorInvalidValue;
+}
+
+int batch_group_ctas_per_sm(int g, int fpc) {
+  if (g == BG_8192 || g == BG_16384) return fold_batch_ctas_per_sm(g == BG_8192 ? 1 : 2);
+#define FXC_CTAS(N, F) batch_ctas_one<N, F>()
+  FXC_BATCH_VARIANTS(g, fpc, FXC_CTAS)
+#undef FXC_CTAS
+  return 0;
+}
+
+cudaError_t launch_batch_group(int g, int fpc, const BatchArgs& a, int grid, cudaStream_t s) {
+  if (grid <= 0) return cudaErrorInvalidValue;
+  if (g == BG_8192 || g == BG_16384) return launch_fold_batch(g == BG_8192 ? 1 : 2, a, g, grid, s);
+#define FXC_LAUNCH(N, F) batch_launch_one<N, F>(a, g, grid, s)
+  FXC_BATCH_VARIANTS(g, fpc, FXC_LAUNCH)
+#undef FXC_LAUNCH
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_batch_frame_info(const BatchArgs& a, int grid, cudaStream_t s) {
+  batch_frame_info_kernel<<<grid, 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_reduce(const BatchArgs& a, int grid, cudaStream_t s) {
+  batch_reduce_kernel<<<grid, 256, 0, s>>>(a);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_reduce(const double* part, int nblk, int h, double m11, double m22, double m12,

@@ -94,6 +94,70 @@ cudaError_t launch_large_decode(const LargeParams& p, uint64_t f0, uint64_t nb, 
 cudaError_t launch_large_split(const LargeParams& p, const float2* Y, uint64_t f0, uint64_t nb,
                                float2* s1, float2* s2, int sms, cudaStream_t s);
 
+// ------------------------------------------------------------ batched sectors
+//
+// One launch per FFT length runs the sectors of many scans: a persistent grid
+// takes work items (a frame range of one sector) by an atomic ticket, each CTA
+// reloading the item's scan tables; every item writes its own f64 partials,
+// summed per sector in item order by one reduction over the whole batch.
+
+// Batch groups: the kernels a batch may launch, one per FFT length (16384 =
+// the two-row kernel, even band shifts only).
+enum { BG_1024 = 0, BG_2048 = 1, BG_4096 = 2, BG_8192 = 3, BG_16384 = 4, kBatchGroups = 5 };
+
+// Frames [f0, f1) of the sector of scan `scan` (for the two-row kernel, the
+// bins of parity `row`), accumulated into partials + part ([4][H] f64).
+struct BatchItem {
+  uint32_t scan, row;
+  uint64_t f0, f1;
+  uint64_t part;
+};
+
+struct BatchScan {
+  CorrParams p;         // the sector: raw words, tables, frame records, error word
+  double* acc;          // [5][H] output (acf11, acf22, xcf re/im, phased = 0)
+  double m11, m22, m12; // reduction multipliers (two-for-one 2x, level scaling)
+  uint64_t part;        // partials offset of the sector's first item
+  uint64_t fi0;         // first frame of the sector in the batch's frame numbering
+  uint64_t bin0;        // first bin of the sector in the batch's bin numbering
+  uint32_t nparts;      // partial slots (items; two-row items share one per row pair)
+  uint32_t n, h;        // FFT length, bins
+  uint32_t pad;
+};
+
+// Device-resident description of one batch: the kernels read every count and
+// table address from it, so that a captured graph serves every batch of the
+// same group set.
+struct BatchHeader {
+  const BatchScan* scans;  // the batch's tables (after the header in the arena)
+  const BatchItem* items;
+  uint32_t nscans;
+  uint32_t ticket[kBatchGroups];  // reset before each launch
+  uint32_t nitems[kBatchGroups];
+  uint32_t item0[kBatchGroups];
+  uint32_t pad;
+  uint64_t nframes;  // frames of all sectors
+  uint64_t nbins;    // bins of all sectors
+};
+
+struct BatchArgs {
+  BatchHeader* hdr;
+  double* partials;
+};
+
+// Batch kernel variants: group g with `fpc` frame pairs per CTA iteration
+// (FFT 1024: 1, 2, 4; 2048: 1, 2, 4; 4096: 1, 2; the fold kernels of FFT
+// 8192 / 16384 take fpc = 1).  batch_prepare sets the variant's shared-memory
+// limit (once, before any launch or capture); batch_group_ctas_per_sm is its
+// occupancy (0: no such variant); launch_batch_group runs `grid` persistent CTAs.
+cudaError_t batch_prepare(int g, int fpc);
+int batch_group_ctas_per_sm(int g, int fpc);
+cudaError_t launch_batch_group(int g, int fpc, const BatchArgs& a, int grid, cudaStream_t s);
+// Frame records of every sector of the batch; the fixed-order reduction of
+// every sector's partials into its acc (grid-stride, any grid size).
+cudaError_t launch_batch_frame_info(const BatchArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_batch_reduce(const BatchArgs& a, int grid, cudaStream_t s);
+
 cudaError_t launch_phased(uint32_t n, const PhasedParams& p, int grid, cudaStream_t s);
 cudaError_t launch_reduce_phased(const double* part, int nblk, int h, double* out, cudaStream_t s);
 cudaError_t launch_frame_info(const DelayParams& p, uint64_t first, uint64_t nf, int n,

@@ -11,6 +11,13 @@
 // other on the device.  A job whose buffers do not fit the budget waits for
 // another job to finish, and fails with FXC_EBUSY only when no other job is
 // running to free memory.
+//
+// Batched mode (opts.batch): a worker only stages its sectors (host-to-device
+// copies into its scan's sector slots) and posts them; one dispatcher thread
+// takes every posted sector (one per scan) and computes them together with one
+// fxc_batch_run_device call on its own stream, keeping at most two batches in
+// flight so that the next batch gathers the sectors posted meanwhile; each
+// worker then queues its sector's device-to-host copies behind that batch.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,6 +52,20 @@ struct Job {
   bool done = false;
 };
 
+// A staged sector waiting for, or computed by, a dispatcher batch.
+struct Posted {
+  fxc_scan* s = nullptr;
+  fxc::StagedSector ss{};
+  uint64_t nf = 0, first = 0;
+  cudaEvent_t done = nullptr;  // recorded after the batch that computed it
+  bool launched = false;
+  fxc_status st = FXC_OK;
+  std::string err;
+};
+
+constexpr int kBatchEvents = 4;  // batches in flight at most, plus slack
+constexpr uint32_t kMaxBatch = 1024;
+
 }  // namespace
 
 struct fxc_server {
@@ -59,6 +80,14 @@ struct fxc_server {
   int idle_holding = 0;  // idle slots that still hold device buffers
   bool pressure = false; // a job waits for HBM: idle slots release theirs
   bool stopping = false;
+  // batched mode
+  fxc_batch* batch = nullptr;
+  std::thread dispatcher;
+  std::deque<Posted*> posted;
+  std::condition_variable cv_post, cv_launched;
+  bool disp_stop = false;
+  cudaStream_t disp_stream = nullptr;
+  cudaEvent_t ev[kBatchEvents] = {};
 };
 
 namespace {
@@ -120,6 +149,62 @@ fxc_status run_job(fxc_server* sv, fxc_scan** sp, Job* J) {
     if (st == FXC_OK) J->stats.sectors += 1;
     return st;
   };
+  if (sv->batch && !(cfg.products & FXC_PROD_RAW)) {
+    // batched: stage, post to the dispatcher, collect behind its batch
+    std::deque<std::pair<Posted, uint64_t>> posts;  // (post, sector index)
+    auto finish_posted = [&]() -> fxc_status {
+      Posted& p = posts.front().first;
+      const uint64_t sec = posts.front().second;
+      {
+        std::unique_lock<std::mutex> lk(sv->mu);
+        sv->cv_launched.wait(lk, [&] { return p.launched; });
+      }
+      fxc_status st = p.st;
+      uint64_t id = 0;
+      if (st == FXC_OK) st = fxc::sector_collect(s, p.ss, p.done, &id);
+      else fxc::sector_release(s, p.ss);
+      if (st == FXC_OK) {
+        const uint64_t f0 = sec * sf;
+        inflight.push_back({id, sec, f0, p.nf});
+        st = finish_one();
+      } else if (!p.err.empty()) {
+        fxc::internal_fail(st, p.err.c_str());
+      }
+      posts.pop_front();
+      return st;
+    };
+    for (uint64_t sec = 0; sec < nsec && result == FXC_OK; ++sec) {
+      const uint64_t f0 = sec * sf;
+      const uint64_t nfs = j.nf ? std::min(sf, j.nf - f0) : 0;
+      Posted np;
+      np.s = s;
+      np.nf = nfs;
+      np.first = j.first_frame + f0;
+      fxc_status st;
+      for (;;) {
+        st = fxc::sector_stage(s, j.raw1 + f0 * b1, nfs * b1, j.raw2 + f0 * b2, nfs * b2, nfs,
+                               &np.ss);
+        if (st != FXC_EBUSY || posts.empty()) break;
+        // every sector slot in flight: finish the oldest
+        if ((st = finish_posted()) != FXC_OK) break;
+      }
+      if (st != FXC_OK) {
+        result = st;
+        break;
+      }
+      posts.emplace_back(np, sec);
+      {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->posted.push_back(&posts.back().first);
+      }
+      sv->cv_post.notify_one();
+    }
+    while (!posts.empty()) {
+      const fxc_status st = finish_posted();
+      if (result == FXC_OK) result = st;
+    }
+    return result;
+  }
   // sectors in flight: as many as the scan's sector slots (the engine's
   // max_inflight) take; a submit that finds them all busy drains the oldest
   for (uint64_t sec = 0; sec < nsec && result == FXC_OK; ++sec) {
@@ -167,6 +252,18 @@ void worker(fxc_server* sv) {
       continue;
     }
     if (sv->queue.empty()) break;  // stopping, nothing left
+    if (sv->stopping) {
+      // shutting down: a job that has not started fails at once
+      for (Job* Q : sv->queue) {
+        Q->stats.status = FXC_EBUSY;
+        Q->stats.t_start_ns = Q->stats.t_done_ns = now_ns();
+        Q->error = "the server was destroyed before the job started";
+        Q->done = true;
+      }
+      sv->queue.clear();
+      sv->cv_done.notify_all();
+      break;
+    }
     Job* J = sv->queue.front();
     sv->queue.pop_front();
     sv->running += 1;
@@ -186,6 +283,97 @@ void worker(fxc_server* sv) {
   if (scan) fxc_scan_close(scan);
 }
 
+// Batched mode: computes every posted sector (one per scan and batch) with
+// one fxc_batch_run_device call; at most two batches in flight.
+void dispatcher(fxc_server* sv) {
+  const int dev = fxc::engine_device(sv->eng);
+  cudaSetDevice(dev);
+  std::deque<int> inflight;  // event indices of batches in flight
+  int next_ev = 0;
+  std::vector<Posted*> take;
+  std::vector<Posted*> later;
+  std::vector<fxc_scan*> scans;
+  std::vector<const uint8_t*> r1, r2;
+  std::vector<uint64_t> nfs, firsts;
+  std::vector<double*> accs;
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> lk(sv->mu);
+      sv->cv_post.wait(lk, [&] { return sv->disp_stop || !sv->posted.empty(); });
+      if (sv->posted.empty()) break;  // stopping, nothing left
+    }
+    // the previous batch but one must be done: the next one gathers meanwhile
+    while ((int)inflight.size() >= 2) {
+      cudaEventSynchronize(sv->ev[inflight.front()]);
+      inflight.pop_front();
+    }
+    take.clear();
+    later.clear();
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      std::vector<fxc_scan*> seen;
+      while (!sv->posted.empty() && take.size() < kMaxBatch) {
+        Posted* p = sv->posted.front();
+        sv->posted.pop_front();
+        if (std::find(seen.begin(), seen.end(), p->s) != seen.end()) {
+          later.push_back(p);  // a scan's next sector waits for the next batch
+          continue;
+        }
+        seen.push_back(p->s);
+        take.push_back(p);
+      }
+      for (auto it = later.rbegin(); it != later.rend(); ++it) sv->posted.push_front(*it);
+    }
+    scans.clear();
+    r1.clear();
+    r2.clear();
+    nfs.clear();
+    firsts.clear();
+    accs.clear();
+    for (Posted* p : take) {
+      cudaStreamWaitEvent(sv->disp_stream, p->ss.h2d, 0);
+      scans.push_back(p->s);
+      r1.push_back(p->ss.d_raw1);
+      r2.push_back(p->ss.d_raw2);
+      nfs.push_back(p->nf);
+      firsts.push_back(p->first);
+      accs.push_back(p->ss.d_acc);
+    }
+    fxc_status st = fxc_batch_run_device(sv->batch, scans.data(), r1.data(), r2.data(), nfs.data(),
+                                         firsts.data(), accs.data(), (uint32_t)take.size(),
+                                         sv->disp_stream);
+    std::string err;
+    if (st == FXC_EBUSY || st == FXC_ENOMEM) {
+      // no room for the batch's tables: each sector on its scan's own buffers
+      st = FXC_OK;
+      for (Posted* p : take) {
+        const fxc_status s1 = fxc::run_sector_internal(p->s, p->ss.d_raw1, p->ss.d_raw2, p->nf,
+                                                       p->first, p->ss.d_acc, sv->disp_stream);
+        if (s1 != FXC_OK) {
+          st = s1;
+          break;
+        }
+      }
+    }
+    if (st != FXC_OK) err = fxc_last_error();
+    const int e = next_ev;
+    next_ev = (next_ev + 1) % kBatchEvents;
+    cudaEventRecord(sv->ev[e], sv->disp_stream);
+    inflight.push_back(e);
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      for (Posted* p : take) {
+        p->done = sv->ev[e];
+        p->st = st;
+        p->err = err;
+        p->launched = true;
+      }
+    }
+    sv->cv_launched.notify_all();
+  }
+  cudaStreamSynchronize(sv->disp_stream);
+}
+
 }  // namespace
 
 extern "C" {
@@ -194,9 +382,36 @@ fxc_status fxc_server_create(fxc_engine* e, const fxc_server_opts* opts, fxc_ser
   if (!e || !out) return fxc::internal_fail(FXC_EINVAL, "NULL argument");
   *out = nullptr;
   const int slots = (opts && opts->slots > 0) ? opts->slots : 4;
-  if (slots > 64) return fxc::internal_fail(FXC_EINVAL, "at most 64 slots");
+  if (slots > 256) return fxc::internal_fail(FXC_EINVAL, "at most 256 slots");
   auto* sv = new fxc_server();
   sv->eng = e;
+  if (opts && opts->batch) {
+    fxc_batch_opts bo{};
+    bo.use_graphs = 1;
+    bo.autotune = 1;
+    fxc_status st = fxc_batch_create(e, &bo, &sv->batch);
+    if (st != FXC_OK) {
+      delete sv;
+      return st;
+    }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(fxc::engine_device(e));
+    bool ok = cudaStreamCreateWithFlags(&sv->disp_stream, cudaStreamNonBlocking) == cudaSuccess;
+    for (int k = 0; k < kBatchEvents && ok; ++k)
+      ok = cudaEventCreateWithFlags(&sv->ev[k], cudaEventDisableTiming | cudaEventBlockingSync) ==
+           cudaSuccess;
+    cudaSetDevice(prev);
+    if (!ok) {
+      for (auto& ev : sv->ev)
+        if (ev) cudaEventDestroy(ev);
+      if (sv->disp_stream) cudaStreamDestroy(sv->disp_stream);
+      fxc_batch_destroy(sv->batch);
+      delete sv;
+      return fxc::internal_fail(FXC_ECUDA, "server: dispatcher stream or events");
+    }
+    sv->dispatcher = std::thread(dispatcher, sv);
+  }
   for (int k = 0; k < slots; ++k) sv->workers.emplace_back(worker, sv);
   fxc::engine_track_server(e, sv, true);
   *out = sv;
@@ -263,6 +478,20 @@ fxc_status fxc_server_destroy(fxc_server* sv) {
   }
   sv->cv_work.notify_all();
   for (auto& t : sv->workers) t.join();
+  if (sv->dispatcher.joinable()) {
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->disp_stop = true;
+    }
+    sv->cv_post.notify_all();
+    sv->dispatcher.join();
+  }
+  if (sv->batch) {
+    for (auto& ev : sv->ev)
+      if (ev) cudaEventDestroy(ev);
+    if (sv->disp_stream) cudaStreamDestroy(sv->disp_stream);
+    fxc_batch_destroy(sv->batch);
+  }
   for (auto& kv : sv->jobs) delete kv.second;
   fxc::engine_track_server(sv->eng, sv, false);
   delete sv;

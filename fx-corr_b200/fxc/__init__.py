@@ -35,7 +35,9 @@ EXPORTS = [
     "fxc_level_power", "fxc_normalize", "fxc_bytes_per_frame", "fxc_probe_fp32_peak",
     "fxc_scan_set_profiling", "fxc_scan_profile", "fxc_sector_run_device_noalloc",
     "fxc_server_create", "fxc_server_submit", "fxc_server_wait", "fxc_server_destroy",
-    "fxc_host_alloc", "fxc_host_free",
+    "fxc_host_alloc", "fxc_host_free", "fxc_batch_create", "fxc_batch_destroy",
+    "fxc_batch_run_device", "fxc_batch_autotune", "fxc_batch_shape", "fxc_batch_launches",
+    "fxc_batch_set_shape",
 ]
 NOALLOC_MAX_FRAMES = 32768
 
@@ -94,7 +96,11 @@ class DeviceOpts(C.Structure):
 
 
 class ServerOpts(C.Structure):
-    _fields_ = [("slots", C.c_int32)]
+    _fields_ = [("slots", C.c_int32), ("batch", C.c_int32)]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("use_graphs", C.c_int32), ("autotune", C.c_int32), ("item_frames", C.c_uint32)]
 
 
 class JobC(C.Structure):
@@ -164,6 +170,16 @@ def lib():
         "fxc_server_destroy": ([vp], st),
         "fxc_host_alloc": ([C.c_uint64, C.POINTER(vp)], st),
         "fxc_host_free": ([vp], st),
+        "fxc_batch_create": ([vp, C.POINTER(BatchOpts), C.POINTER(vp)], st),
+        "fxc_batch_destroy": ([vp], st),
+        "fxc_batch_run_device": ([vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                  C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(vp),
+                                  C.c_uint32, vp], st),
+        "fxc_batch_autotune": ([vp, C.c_uint32], st),
+        "fxc_batch_shape": ([vp, C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_uint32),
+                             C.POINTER(C.c_int32), f64p], st),
+        "fxc_batch_launches": ([vp], C.c_uint64),
+        "fxc_batch_set_shape": ([vp, C.c_uint32, C.c_int32, C.c_uint32], st),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -270,6 +286,7 @@ class Engine:
         self.device = device
         self._scans = weakref.WeakSet()
         self._servers = weakref.WeakSet()
+        self._batches = weakref.WeakSet()
 
     def open_scan(self, cfg: ScanConfig) -> "Scan":
         s = Scan(self, cfg)
@@ -283,6 +300,8 @@ class Engine:
                 s.h = None
             for sv in list(self._servers):
                 sv.h = None
+            for b in list(self._batches):
+                b.h = None
             lib().fxc_engine_destroy(self.h)
             self.h = None
 
@@ -412,23 +431,77 @@ class Scan:
         return out
 
 
+class Batch:
+    """Batched sectors of many scans (fxc_batch_*): one sector of each scan in
+    a few launches, optionally replayed from captured CUDA graphs, with kernel
+    shapes from the autotuner."""
+
+    def __init__(self, eng: Engine, use_graphs: bool = False, autotune: bool = False,
+                 item_frames: int = 0):
+        self.eng = eng
+        h = C.c_void_p()
+        o = BatchOpts(int(use_graphs), int(autotune), item_frames)
+        check(lib().fxc_batch_create(eng.h, C.byref(o), C.byref(h)))
+        self.h = h
+        eng._batches.add(self)
+
+    def run_device(self, scans, d_raw1, d_raw2, nf, first_frame, d_acc, stream=None):
+        """One sector per scan; every argument but stream is a sequence of the
+        same length (torch CUDA tensors for the buffers)."""
+        n = len(scans)
+        VP = C.c_void_p * n
+        U64 = C.c_uint64 * n
+        check(lib().fxc_batch_run_device(
+            self.h, VP(*[s.h.value for s in scans]), VP(*[_ptr(x) for x in d_raw1]),
+            VP(*[_ptr(x) for x in d_raw2]), U64(*nf), U64(*first_frame),
+            VP(*[_ptr(x) for x in d_acc]), n, _stream(stream)))
+
+    def autotune(self, fft: int):
+        check(lib().fxc_batch_autotune(self.h, fft))
+
+    def shape(self, fft: int) -> dict:
+        fpc, itf, ctas, g = C.c_int32(), C.c_uint32(), C.c_int32(), C.c_double()
+        check(lib().fxc_batch_shape(self.h, fft, C.byref(fpc), C.byref(itf), C.byref(ctas),
+                                    C.byref(g)))
+        return dict(fpc=fpc.value, item_frames=itf.value, ctas_per_sm=ctas.value,
+                    gsps=g.value)
+
+    def set_shape(self, fft: int, fpc: int, item_frames: int):
+        check(lib().fxc_batch_set_shape(self.h, fft, fpc, item_frames))
+
+    def launches(self) -> int:
+        return int(lib().fxc_batch_launches(self.h))
+
+    def close(self):
+        if self.h and self.eng.h:
+            lib().fxc_batch_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Server:
     """The serving loop (fxc_server_*): jobs of one scan configuration each,
     admitted into ``slots`` concurrent device contexts as they free up."""
 
-    def __init__(self, eng: Engine, slots: int = 4):
+    def __init__(self, eng: Engine, slots: int = 4, batch: bool = False):
         self.eng = eng
         h = C.c_void_p()
-        check(lib().fxc_server_create(eng.h, C.byref(ServerOpts(slots)), C.byref(h)))
+        check(lib().fxc_server_create(eng.h, C.byref(ServerOpts(slots, int(batch))), C.byref(h)))
         self.h = h
         self._jobs = {}
         eng._servers.add(self)
 
     def submit(self, cfg: ScanConfig, raw1, raw2, nf: int, first_frame: int = 0,
-               sector_frames: int = 0) -> int:
+               sector_frames: int = 0, cfg_c=None) -> int:
         """Queue a job; raw1/raw2 are host arrays (page-locked torch tensors
-        or numpy arrays) that must stay alive until wait()."""
-        c = cfg.to_c()
+        or numpy arrays) that must stay alive until wait().  cfg_c: cfg.to_c()
+        built beforehand (a caller submitting many jobs of few configurations)."""
+        c = cfg.to_c() if cfg_c is None else cfg_c
         sf = sector_frames or max(nf, 1)
         nsec = (nf + sf - 1) // sf if nf else 1
         out = np.zeros((nsec, 5 * cfg.h))

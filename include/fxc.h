@@ -212,11 +212,16 @@ FXC_API fxc_status fxc_sector_run_device_noalloc(const fxc_scan_cfg* cfg, const 
  * device state of a finished job (partials, frame records, staging buffers,
  * tables) is reused by the next job of its slot.  Each job's products are
  * those of fxc_sector_submit/wait over the same sectors, bit for bit, alone
- * or in any mix. */
+ * or in any mix; with opts.batch they are those of fxc_batch_run_device over
+ * the same sectors (within the FP32 tolerance of the per-scan path), again
+ * identical alone and in any mix. */
 typedef struct fxc_server fxc_server;
 
 typedef struct fxc_server_opts {
-  int32_t slots;             /* jobs on the device at once (0 = 4) */
+  int32_t slots;             /* jobs on the device at once (0 = 4, at most 256) */
+  int32_t batch;             /* 1: the sectors of all running jobs are computed
+                                together, one fxc_batch call (CUDA graphs,
+                                autotuned shapes) per round of ready sectors */
 } fxc_server_opts;
 
 typedef struct fxc_job {
@@ -246,8 +251,63 @@ FXC_API fxc_status fxc_server_submit(fxc_server* sv, const fxc_job* job, uint64_
 /* Waits for a job (timeout_ms < 0: no limit) and forgets it. */
 FXC_API fxc_status fxc_server_wait(fxc_server* sv, uint64_t job_id, int32_t timeout_ms,
                                    fxc_job_stats* stats);
-/* Finishes the queued jobs, then releases the slots. */
+/* Finishes the running jobs, fails the queued ones that have not started
+ * (FXC_EBUSY), then releases the slots. */
 FXC_API fxc_status fxc_server_destroy(fxc_server* sv);
+
+/* ---- batched sectors of many scans --------------------------------------
+ * No reference counterpart (the reference runs one scan per process).  A
+ * batch runs one sector of each of many distinct scans in a few launches:
+ * the frame records of every sector in one launch, every sector of one FFT
+ * length in one persistent kernel (1-8 bit stations mixed; work items of a
+ * few hundred frames handed out to the CTAs by an atomic ticket), and one
+ * fixed-order reduction for all.  With use_graphs the launches of each set of
+ * FFT lengths are captured once in a CUDA graph and replayed.  The frames per
+ * CTA iteration and frames per work item of each FFT length come from an
+ * autotuner that times the kernel variants on a synthetic batch (at first use
+ * of the length when opts.autotune is set, or by fxc_batch_autotune).
+ * Sectors the batch kernels do not cover (phased products, FFT lengths above
+ * 16384, FFT 16384 with an odd band shift, empty sectors) run through the
+ * per-scan path on the same stream.  A sector's products equal
+ * fxc_sector_run_device's within the library's FP32 tolerance, and are
+ * identical bit for bit whatever else shares the batch (the item split
+ * depends only on the sector's frame count and the batch's tuning). */
+typedef struct fxc_batch fxc_batch;
+
+typedef struct fxc_batch_opts {
+  int32_t use_graphs;        /* capture and replay CUDA graphs */
+  int32_t autotune;          /* tune an FFT length at its first batch */
+  uint32_t item_frames;      /* frames per work item; 0 = tuned or the default */
+} fxc_batch_opts;
+
+FXC_API fxc_status fxc_batch_create(fxc_engine* e, const fxc_batch_opts* opts, fxc_batch** out);
+FXC_API fxc_status fxc_batch_destroy(fxc_batch* b);
+/* One sector of each of `count` distinct scans of b's engine: device inputs
+ * (16-byte aligned), device outputs d_acc[i] of 5 * H doubles as in
+ * fxc_sector_run_device, enqueued on `stream`.  Host arrays are read before
+ * the call returns.  Calls on one batch are serialised (a later call may use
+ * another stream; it waits for the earlier call's device work). */
+FXC_API fxc_status fxc_batch_run_device(fxc_batch* b, fxc_scan* const* scans,
+                                        const uint8_t* const* d_raw1,
+                                        const uint8_t* const* d_raw2, const uint64_t* nf,
+                                        const uint64_t* first_frame, double* const* d_acc,
+                                        uint32_t count, void* stream);
+/* Times every kernel variant x work-item size of one FFT length (1024..16384)
+ * on a synthetic 2-bit batch and keeps the fastest (blocks the host for tens
+ * of milliseconds). */
+FXC_API fxc_status fxc_batch_autotune(fxc_batch* b, uint32_t fft_len);
+/* The shape in use for an FFT length: frame pairs per CTA iteration, frames
+ * per work item, resident CTAs per SM, and the tuner's measured
+ * Gsample/s (0 if not tuned). */
+FXC_API fxc_status fxc_batch_shape(fxc_batch* b, uint32_t fft_len, int32_t* fpc,
+                                   uint32_t* item_frames, int32_t* ctas_per_sm, double* gsps);
+/* Pins the shape of an FFT length: fpc a variant the length has (1024 and
+ * 2048: 1, 2, 4; 4096: 1, 2; 8192 and 16384: 1), item_frames a positive
+ * multiple of 32. */
+FXC_API fxc_status fxc_batch_set_shape(fxc_batch* b, uint32_t fft_len, int32_t fpc,
+                                       uint32_t item_frames);
+/* Kernels the batch launched so far (graph replays count their kernels). */
+FXC_API uint64_t fxc_batch_launches(fxc_batch* b);
 
 /* Page-locked host memory for sector buffers (no reference counterpart: the
  * reference reads into pageable Vec<u8>, src/main.rs:2133-2147); copies from

@@ -123,3 +123,83 @@ def test_bad_job_is_reported_and_server_continues(engine):
     assert ei.value.status == fxc.EUNSUPPORTED
     assert all(st["status"] == 0 for _, st in ok)
     sv.close()
+
+
+# ----------------------------------------------------------- batched mode
+
+def close_dumps(a, b, jobs_nf):
+    """Batched vs per-scan dumps: FP32 agreement (different partial-sum
+    grouping), cross-spectra against their noise floor."""
+    from _cases import assert_spectra_close, xcf_floor
+
+    assert len(a) == len(b)
+    for da, db in zip(a, b):
+        for k in ("acf11", "acf22"):
+            if np.any(db[k]):
+                assert_spectra_close(da[k], db[k], k)
+            else:
+                assert not np.any(da[k]), k
+        fl = xcf_floor(db, jobs_nf)
+        if fl is not None:
+            assert_spectra_close(da["xcf"], db["xcf"], "xcf", floor=fl)
+        assert np.array_equal(da["phased"], db["phased"])
+
+
+def test_batched_alone_equals_mix_and_matches_plain(engine):
+    import fxc
+
+    jobs = make_jobs(7, 14)
+    sv = fxc.Server(engine, slots=8, batch=True)
+    alone = [run(sv, [j])[0] for j in jobs]
+    mixed = run(sv, jobs)
+    for (da, sa), (dm, sm) in zip(alone, mixed):
+        same(da, dm)  # the item split depends only on the sector and the tuned shape
+        assert sa["sectors"] == sm["sectors"] == len(da)
+    sv.close()
+    plain = fxc.Server(engine, slots=4)
+    ref = run(plain, jobs)
+    plain.close()
+    for j, (dm, _), (dr, _) in zip(jobs, mixed, ref):
+        close_dumps(dm, dr, max(1, min(j["nf"], j["sector_frames"] or j["nf"])))
+
+
+def test_batched_many_short_jobs(engine):
+    """Hundreds of one-sector jobs share batches; each equals its alone run."""
+    import fxc
+
+    rng = np.random.Generator(np.random.PCG64(99))
+    jobs = []
+    for k in range(96):
+        fft = int(rng.choice([1024, 8192]))
+        scan = make_scan(fft=fft, fs=1024e6, bits1=2, bits2=2, shuffle="generic",
+                         band=(0, 0, fft // 2, 0), delay=dict(DELAY, net_d2_base=1e-7 * k), seed=k)
+        nf = int(rng.integers(1, 300))
+        r1, r2 = random_raw(scan, nf, seed=500 + k)
+        jobs.append(dict(cfg=to_fxc(scan), raw1=r1, raw2=r2, nf=nf, first_frame=k,
+                         sector_frames=0))
+    sv = fxc.Server(engine, slots=32, batch=True)
+    mixed = run(sv, jobs)
+    for j, (dm, st) in zip(jobs[::12], mixed[::12]):
+        alone = run(sv, [j])[0][0]
+        same(alone, dm)
+        assert st["status"] == 0
+    sv.close()
+
+
+def test_batched_tight_budget(engine):
+    """Under a tight HBM budget the batched server still finishes every job
+    (a batch that does not fit falls back to the per-scan buffers)."""
+    import fxc
+
+    jobs = make_jobs(3, 8)
+    plain = fxc.Server(engine, slots=2)
+    ref = run(plain, jobs)
+    plain.close()
+    small = fxc.Engine(0, hbm_budget_bytes=200 << 20)
+    sv = fxc.Server(small, slots=4, batch=True)
+    got = run(sv, jobs)
+    for j, (dr, _), (dg, st) in zip(jobs, ref, got):
+        assert st["status"] == 0
+        close_dumps(dg, dr, max(1, min(j["nf"], j["sector_frames"] or j["nf"])))
+    sv.close()
+    small.close()
