@@ -333,6 +333,59 @@ def short_jobs(n_jobs, rate, seed=6262):
     return jobs
 
 
+def batch_leg(fxc, torch, eng, n_sectors=64, calls=20, warm=3, seed=8383):
+    """Device-resident batched throughput: one fxc_batch call = one sector
+    each of n_sectors distinct short 2-bit FFT-8192 scans (125-2000 frame
+    pairs, random delays), replayed from a CUDA graph with the autotuned
+    shape; CUDA events around each call on the calling stream."""
+    jobs = short_jobs(n_sectors, rate=1.0, seed=seed)
+    scans, r1, r2, accs, nfs = [], [], [], [], []
+    tot = sum(j["nf"] for j in jobs) * (N * BITS // 8)
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    d = torch.randint(0, 256, (2, tot), dtype=torch.uint8, device="cuda", generator=g)
+    off = 0
+    for j in jobs:
+        c = fxc.ScanConfig(fft=j["fft"], fs=j["fs"], bits1=2, bits2=2,
+                           levels1=[-3.0, -1.0, 1.0, 3.0], levels2=[-3.0, -1.0, 1.0, 3.0],
+                           shuffle1=shuffle_internal(101), shuffle2=shuffle_internal(102),
+                           products=fxc.PROD_ACF | fxc.PROD_XCF, delay=j["delay"])
+        scans.append(eng.open_scan(c))
+        n = j["nf"] * c.bpf(2)
+        r1.append(d[0, off:off + n])
+        r2.append(d[1, off:off + n])
+        off += n
+        accs.append(torch.empty(5 * c.h, dtype=torch.float64, device="cuda"))
+        nfs.append(j["nf"])
+    b = fxc.Batch(eng, use_graphs=True, autotune=True)
+    st = torch.cuda.current_stream()
+    firsts = [0] * n_sectors
+    for _ in range(warm):
+        b.run_device(scans, r1, r2, nfs, firsts, accs, stream=st)
+    torch.cuda.synchronize()
+    l0 = b.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(calls):
+        b.run_device(scans, r1, r2, nfs, firsts, accs, stream=st)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / calls
+    for s in scans:
+        s.check()
+    samples = 2.0 * N * sum(nfs)
+    out = {"gsample_s": samples / (ms * 1e-3) / 1e9, "ms_per_call": ms,
+           "sectors_per_call": n_sectors, "frame_pairs_per_call": int(sum(nfs)),
+           "kernels_per_call": (b.launches() - l0) / calls, "shape_fft8192": b.shape(N),
+           "input_bytes_per_call": 2 * tot,
+           "path": "fxc_batch_run_device (CUDA graph replay: frame records, one persistent "
+                   "corr_fold_batch_kernel, one reduction), device-resident inputs"}
+    b.close()
+    for s in scans:
+        s.close()
+    del d
+    return out
+
+
 def serve_leg(fxc, torch, eng, jobs, slots, batch, plain_jobs=None, label="", mix=""):
     """Served (fxc_server, continuous batching) vs plain (one job at a time:
     scan open, per sector a synchronous H2D + kernels + dump, scan close) on
@@ -469,6 +522,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-vs-plain leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-sectors leg")
     ap.add_argument("--serve-jobs", type=int, default=20)
     ap.add_argument("--serve-short-jobs", type=int, default=2000)
     ap.add_argument("--sectors", type=int, default=SECTORS,
@@ -593,6 +647,11 @@ def main():
                        "flight across steps"}
     clk = clocks.stop()
 
+    # ---- batched sectors of many short scans, device-resident (rank 0 of N=1)
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        batched = batch_leg(fxc, torch, eng)
+
     # ---- serving: continuous batching vs one job at a time (rank 0 of N=1)
     serve = None
     if rank == 0 and world == 1 and not args.no_serve:
@@ -663,6 +722,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "batched": batched,
             "serving": serve,
             "gpu_launches": all_launches,
             "clocks": clk,

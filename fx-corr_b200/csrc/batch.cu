@@ -215,9 +215,10 @@ fxc_status autotune_locked(fxc_batch* b, int g) {
   } flag(b->tuning[g]);
   const Shape saved = b->shape[g];
   const uint32_t fft_len = kGroupN[g];
-  // synthetic batch: 8 scans of 2-bit stations, 2^24 samples per sector each
-  constexpr int kScans = 8;
-  const uint64_t frames = (1ull << 24) / fft_len;
+  // synthetic batch: 16 scans of 2-bit stations, 2^25 samples per sector each
+  // (a few items per CTA, as in a serving batch)
+  constexpr int kScans = 16;
+  const uint64_t frames = (1ull << 25) / fft_len;
   const uint64_t bpf = fxc_bytes_per_frame(fft_len, 2);
   const double fs = 1024e6;
   fxc_scan_cfg cfg{};

@@ -246,9 +246,29 @@ __device__ __forceinline__ bool fold_span(const CorrParams& p, int row, uint64_t
   const bool preP = bitsP > 2 && sp.shkind != SH_IDENTITY;
   const bool preS = bitsS > 2 && ss.shkind != SH_IDENTITY;
 
-  // ---- constant tables of this scan (the previous span, if any, has passed
-  // its last decode: every thread is past its barriers)
+  const uint32_t bpfP = sp.bpf, bpfS = ss.bpf;
+  const uint8_t* rawP = sp.raw;
+  const uint8_t* rawS = ss.raw;
+  const FrameInfo* gfi = p.finfo;
+
+  // slot: [FrameInfo][primary frame][secondary frame]
+  auto issue = [&](uint64_t it) {
+    const int slot = (int)((seq0 + (uint32_t)(it - it0)) % kStages);
+    uint8_t* dst = stage + slot * L.stage_stride;
+    mbar_expect_tx(&bars[slot], kFiBytes + bpfP + bpfS);
+    bulk_g2s(dst, gfi + it, kFiBytes, &bars[slot]);
+    bulk_g2s(dst + kFiBytes, rawP + it * bpfP, bpfP, &bars[slot]);
+    bulk_g2s(dst + kFiBytes + bpfP, rawS + it * bpfS, bpfS, &bars[slot]);
+  };
+  // The previous span, if any, is past its last decode and its last frame's
+  // barriers: the staging ring and the tables are free.  The first frames'
+  // copies go out first, the tables are built while they are in flight.
   __syncthreads();
+  if (tid == 0) {
+    fence_proxy_async();
+    for (uint64_t it = it0; it < it1 && it < it0 + kStages; ++it) issue(it);
+  }
+  // ---- constant tables of this scan
   for (int i = tid; i < 1024; i += kT) {
     // per station: 2^b levels, then their negations (the two sign groups of a
     // warp's table loads fall in different banks)
@@ -285,24 +305,7 @@ __device__ __forceinline__ bool fold_span(const CorrParams& p, int row, uint64_t
   };
   const bool splitP = split2(sp), splitS = split2(ss);
   const float2 dtw0 = c.dtw0, dtw1 = c.dtw1, wb1 = c.wb1;
-
-  const uint32_t bpfP = sp.bpf, bpfS = ss.bpf;
-  const uint8_t* rawP = sp.raw;
-  const uint8_t* rawS = ss.raw;
-  const FrameInfo* gfi = p.finfo;
-
-  // slot: [FrameInfo][primary frame][secondary frame]
-  auto issue = [&](uint64_t it) {
-    const int slot = (int)((seq0 + (uint32_t)(it - it0)) % kStages);
-    uint8_t* dst = stage + slot * L.stage_stride;
-    mbar_expect_tx(&bars[slot], kFiBytes + bpfP + bpfS);
-    bulk_g2s(dst, gfi + it, kFiBytes, &bars[slot]);
-    bulk_g2s(dst + kFiBytes, rawP + it * bpfP, bpfP, &bars[slot]);
-    bulk_g2s(dst + kFiBytes + bpfP, rawS + it * bpfS, bpfS, &bars[slot]);
-  };
   __syncthreads();
-  if (tid == 0)
-    for (uint64_t it = it0; it < it1 && it < it0 + kStages; ++it) issue(it);
 
   // acc[2i]: bin tid + T i, acc[2i+1]: bin N/2 - tid - T i, acc[2 kUnits]: bin N/4 (tid 0).
   // Columns: primary ACF, secondary ACF (at the primary bin), XCF re, im.

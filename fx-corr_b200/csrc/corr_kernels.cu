@@ -79,14 +79,6 @@ __device__ __forceinline__ bool corr_span(const CorrParams& p, uint64_t it0, uin
   const int t = tid % T1;  // thread index within its frame pair
   const uint32_t seq0 = seq;
 
-  // ---- constant tables of this scan (the previous span, if any, is done
-  // with them: every thread is past its barriers)
-  __syncthreads();
-  for (int i = tid; i < 512; i += T) lv[i] = p.st[i >> 8].levels[i & 255] * p.st[i >> 8].scale;
-  for (int s = 0; s < 2; ++s)
-    if (p.st[s].shkind == SH_GENERIC)
-      for (int i = tid; i < 1024; i += T) lut[s * 1024 + i] = p.st[s].shlut[i];
-
   const uint32_t bpf1 = p.st[0].bpf, bpf2 = p.st[1].bpf;
   const uint8_t* raw1 = p.st[0].raw;
   const uint8_t* raw2 = p.st[1].raw;
@@ -105,9 +97,19 @@ __device__ __forceinline__ bool corr_span(const CorrParams& p, uint64_t it0, uin
     bulk_g2s(dst + kRaw1, raw1 + f0 * bpf1, b1, &bars[slot]);
     bulk_g2s(dst + kRaw1 + FPC * bpf1, raw2 + f0 * bpf2, b2, &bars[slot]);
   };
+  // The previous span, if any, is past its last decode and its last
+  // iteration's barriers: the staging ring and the tables are free.  The
+  // first iterations' copies go out first, the tables are built meanwhile.
   __syncthreads();
-  if (tid == 0)
+  if (tid == 0) {
+    fence_proxy_async();
     for (uint64_t it = it0; it < it1 && it < it0 + kStages; ++it) issue(it);
+  }
+  for (int i = tid; i < 512; i += T) lv[i] = p.st[i >> 8].levels[i & 255] * p.st[i >> 8].scale;
+  for (int s = 0; s < 2; ++s)
+    if (p.st[s].shkind == SH_GENERIC)
+      for (int i = tid; i < 1024; i += T) lut[s * 1024 + i] = p.st[s].shlut[i];
+  __syncthreads();
 
   float acc[BPT + 1][4];
 #pragma unroll
