@@ -577,10 +577,15 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_batch_kernel(const BatchArgs 
 
 uint32_t fold_smem_bytes(uint32_t stage_bytes) { return fold_layout(stage_bytes).total; }
 
+// The shared-memory limit of a kernel is a per-function attribute shared by
+// every host thread: it is always set to the largest layout (8-bit stations),
+// so that a concurrent launch with a larger stage never meets a limit another
+// thread has just lowered.
 cudaError_t launch_corr_fold(const CorrParams& p, int grid, cudaStream_t stream) {
   const uint32_t smem = fold_smem_bytes(p.stage_bytes);
   cudaError_t e = cudaFuncSetAttribute(corr_fold_kernel<1>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)fold_smem_bytes(2u * kN));
   if (e != cudaSuccess) return e;
   corr_fold_kernel<1><<<grid, kT, smem, stream>>>(p, 0);
   return cudaGetLastError();
@@ -594,7 +599,8 @@ bool corr_fold2_supported(const CorrParams& p) {
 cudaError_t launch_corr_fold2(const CorrParams& p, int grid, cudaStream_t stream) {
   const uint32_t smem = fold_smem_bytes(p.stage_bytes);
   cudaError_t e = cudaFuncSetAttribute(corr_fold_kernel<2>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)fold_smem_bytes(4u * kN));
   if (e != cudaSuccess) return e;
   for (int row = 0; row < 2; ++row) {
     corr_fold_kernel<2><<<grid, kT, smem, stream>>>(p, row);

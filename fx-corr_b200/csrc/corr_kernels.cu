@@ -456,7 +456,10 @@ template <int N, int FPC, int MODE>
 static cudaError_t launch_one(const CorrParams& p, int grid, cudaStream_t stream) {
   const SmemLayout L = smem_layout<N, FPC>(p.stage_bytes);
   auto kern = corr_kernel<N, FPC, MODE>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  // the limit is shared by every host thread: always the largest layout
+  // (8-bit stations), never lowered under a concurrent launch
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_layout<N, FPC>(2u * FPC * N).total);
   if (e != cudaSuccess) return e;
   kern<<<grid, FPC * N / 16, L.total, stream>>>(p);
   return cudaGetLastError();

@@ -256,7 +256,11 @@ template <int N, int FPC>
 static cudaError_t launch_phased_one(const PhasedParams& p, int grid, cudaStream_t stream) {
   const uint32_t smem = smem_layout<N, FPC>(p.stage_bytes).total + 1024 + 4096;
   auto kern = phased_kernel<N, FPC>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the limit is shared by every host thread: always the largest layout
+  // (8-bit stations), never lowered under a concurrent launch
+  cudaError_t e = cudaFuncSetAttribute(
+      kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      (int)(smem_layout<N, FPC>(2u * FPC * N).total + 1024 + 4096));
   if (e != cudaSuccess) return e;
   kern<<<grid, FPC * N / 16, smem, stream>>>(p);
   return cudaGetLastError();
