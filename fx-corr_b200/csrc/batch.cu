@@ -74,16 +74,20 @@ struct fxc_batch {
   Shape shape[kBatchGroups];
   bool tuning[kBatchGroups] = {};  // the tuner's own batches run untuned
   bool prepared[kBatchGroups][5] = {};
-  // device arena [header][scans][items] mirrors the pinned staging
-  uint8_t* d_arena = nullptr;
-  uint64_t arena_cap = 0;
-  uint8_t* h_arena = nullptr;
-  uint64_t h_cap = 0;
-  uint64_t scans_cap = 0, items_cap = 0;
+  // two device arenas [header][scans][items], each mirroring its pinned
+  // staging, used by alternate calls: a call need not wait for the previous
+  // call's upload (queued behind that call's inputs) before staging its own
+  struct Arena {
+    uint8_t* d = nullptr;
+    uint64_t cap = 0;
+    uint8_t* h = nullptr;
+    uint64_t hcap = 0;
+    cudaEvent_t staged = nullptr;  // this staging's last upload has been read
+  } arena[2];
+  int next_arena = 0;
   double* d_part = nullptr;
   uint64_t part_cap = 0;  // doubles
   uint64_t charged = 0;
-  cudaEvent_t ev_staged = nullptr;  // the staging's last upload has been read
   cudaEvent_t ev_done = nullptr;    // the last call's device work
   cudaStream_t cap_stream = nullptr;
   std::map<uint64_t, cudaGraphExec_t> execs;  // by group set and variants
@@ -135,26 +139,26 @@ fxc_status set_shape(fxc_batch* b, int g, int fpc, uint32_t item_frames) {
 
 // Grows the device arena / partials (waiting for the previous call's work,
 // whose graphs point at the old buffers) and the pinned staging.
-fxc_status grow(fxc_batch* b, uint64_t arena_bytes, uint64_t part_elems) {
-  if (arena_bytes > b->arena_cap || part_elems > b->part_cap) {
+fxc_status grow(fxc_batch* b, fxc_batch::Arena& A, uint64_t arena_bytes, uint64_t part_elems) {
+  if (arena_bytes > A.cap || part_elems > b->part_cap) {
     BCK(cudaEventSynchronize(b->ev_done));
     drop_graphs(b);
   }
-  if (arena_bytes > b->arena_cap) {
-    const uint64_t want = std::max<uint64_t>(arena_bytes, 2 * b->arena_cap);
+  if (arena_bytes > A.cap) {
+    const uint64_t want = std::max<uint64_t>(arena_bytes, 2 * A.cap);
     fxc_status st = engine_reserve(b->eng, want);
     if (st != FXC_OK) return st;
-    cudaFree(b->d_arena);
-    engine_release(b->eng, b->arena_cap);
-    b->charged -= std::min(b->charged, b->arena_cap);
-    b->d_arena = nullptr;
-    b->arena_cap = 0;
-    const cudaError_t e = cudaMalloc(&b->d_arena, want);
+    cudaFree(A.d);
+    engine_release(b->eng, A.cap);
+    b->charged -= std::min(b->charged, A.cap);
+    A.d = nullptr;
+    A.cap = 0;
+    const cudaError_t e = cudaMalloc(&A.d, want);
     if (e != cudaSuccess) {
       engine_release(b->eng, want);
       BCK(e);
     }
-    b->arena_cap = want;
+    A.cap = want;
     b->charged += want;
   }
   if (part_elems > b->part_cap) {
@@ -174,13 +178,13 @@ fxc_status grow(fxc_batch* b, uint64_t arena_bytes, uint64_t part_elems) {
     b->part_cap = want;
     b->charged += want * 8;
   }
-  if (arena_bytes > b->h_cap) {
-    BCK(cudaEventSynchronize(b->ev_staged));
-    if (b->h_arena) cudaFreeHost(b->h_arena);
-    b->h_arena = nullptr;
-    b->h_cap = 0;
-    BCK(cudaMallocHost(&b->h_arena, b->arena_cap));
-    b->h_cap = b->arena_cap;
+  if (arena_bytes > A.hcap) {
+    BCK(cudaEventSynchronize(A.staged));
+    if (A.h) cudaFreeHost(A.h);
+    A.h = nullptr;
+    A.hcap = 0;
+    BCK(cudaMallocHost(&A.h, A.cap));
+    A.hcap = A.cap;
   }
   return FXC_OK;
 }
@@ -417,25 +421,29 @@ fxc_status run_batch(fxc_batch* b, fxc_scan* const* scans, const uint8_t* const*
     const uint64_t off_scans = align_up(sizeof(BatchHeader), 256);
     const uint64_t off_items = off_scans + align_up(ents.size() * sizeof(BatchScan), 256);
     const uint64_t bytes = off_items + items.size() * sizeof(BatchItem);
-    fxc_status st = grow(b, bytes, std::max<uint64_t>(part, 1));
+    const int ai = b->next_arena;
+    b->next_arena ^= 1;
+    fxc_batch::Arena& A = b->arena[ai];
+    fxc_status st = grow(b, A, bytes, std::max<uint64_t>(part, 1));
     if (st != FXC_OK) return st;
-    BCK(cudaEventSynchronize(b->ev_staged));
-    hdr.scans = reinterpret_cast<const BatchScan*>(b->d_arena + off_scans);
-    hdr.items = reinterpret_cast<const BatchItem*>(b->d_arena + off_items);
-    std::memcpy(b->h_arena, &hdr, sizeof hdr);
+    BCK(cudaEventSynchronize(A.staged));  // the call before the previous one
+    hdr.scans = reinterpret_cast<const BatchScan*>(A.d + off_scans);
+    hdr.items = reinterpret_cast<const BatchItem*>(A.d + off_items);
+    std::memcpy(A.h, &hdr, sizeof hdr);
     for (size_t k = 0; k < ents.size(); ++k)
-      std::memcpy(b->h_arena + off_scans + k * sizeof(BatchScan), &ents[k].bs, sizeof(BatchScan));
-    std::memcpy(b->h_arena + off_items, items.data(), items.size() * sizeof(BatchItem));
-    BCK(cudaMemcpyAsync(b->d_arena, b->h_arena, bytes, cudaMemcpyHostToDevice, stream));
-    BCK(cudaEventRecord(b->ev_staged, stream));
+      std::memcpy(A.h + off_scans + k * sizeof(BatchScan), &ents[k].bs, sizeof(BatchScan));
+    std::memcpy(A.h + off_items, items.data(), items.size() * sizeof(BatchItem));
+    BCK(cudaMemcpyAsync(A.d, A.h, bytes, cudaMemcpyHostToDevice, stream));
+    BCK(cudaEventRecord(A.staged, stream));
 
     BatchArgs a;
-    a.hdr = reinterpret_cast<BatchHeader*>(b->d_arena);
+    a.hdr = reinterpret_cast<BatchHeader*>(A.d);
     a.partials = b->d_part;
     // the graph's kernels take the header and partials addresses as
     // arguments: graphs are dropped whenever either moves (grow)
     uint64_t key = mask;
     for (int g = 0; g < kBatchGroups; ++g) key |= (uint64_t)b->shape[g].fpc << (8 + 4 * g);
+    key |= (uint64_t)ai << 40;
     const int grid_aux = b->sms * 8;
     auto enqueue = [&](cudaStream_t s, bool full) -> fxc_status {
       const uint64_t fgrid = full ? (uint64_t)grid_aux
@@ -513,7 +521,8 @@ fxc_status fxc_batch_create(fxc_engine* e, const fxc_batch_opts* opts, fxc_batch
     return internal_fail(FXC_ECUDA, m);
   };
   cudaError_t err;
-  if ((err = cudaEventCreateWithFlags(&b->ev_staged, cudaEventDisableTiming)) != cudaSuccess ||
+  if ((err = cudaEventCreateWithFlags(&b->arena[0].staged, cudaEventDisableTiming)) != cudaSuccess ||
+      (err = cudaEventCreateWithFlags(&b->arena[1].staged, cudaEventDisableTiming)) != cudaSuccess ||
       (err = cudaEventCreateWithFlags(&b->ev_done, cudaEventDisableTiming)) != cudaSuccess ||
       (err = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking)) != cudaSuccess)
     return bail(err);
@@ -528,11 +537,13 @@ fxc_status fxc_batch_destroy(fxc_batch* b) {
   DeviceGuardB dg(b->device);
   if (b->ev_done) cudaEventSynchronize(b->ev_done);
   drop_graphs(b);
-  cudaFree(b->d_arena);
+  for (auto& A : b->arena) {
+    cudaFree(A.d);
+    if (A.h) cudaFreeHost(A.h);
+    if (A.staged) cudaEventDestroy(A.staged);
+  }
   cudaFree(b->d_part);
-  if (b->h_arena) cudaFreeHost(b->h_arena);
   engine_release(b->eng, b->charged);
-  if (b->ev_staged) cudaEventDestroy(b->ev_staged);
   if (b->ev_done) cudaEventDestroy(b->ev_done);
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
   delete b;

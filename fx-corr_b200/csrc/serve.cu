@@ -55,6 +55,7 @@ struct Job {
 // A staged sector waiting for, or computed by, a dispatcher batch.
 struct Posted {
   fxc_scan* s = nullptr;
+  std::condition_variable* cv = nullptr;  // the posting worker's (woken alone)
   fxc::StagedSector ss{};
   uint64_t nf = 0, first = 0;
   cudaEvent_t done = nullptr;  // recorded after the batch that computed it
@@ -84,7 +85,7 @@ struct fxc_server {
   fxc_batch* batch = nullptr;
   std::thread dispatcher;
   std::deque<Posted*> posted;
-  std::condition_variable cv_post, cv_launched;
+  std::condition_variable cv_post;
   bool disp_stop = false;
   cudaStream_t disp_stream = nullptr;
   cudaEvent_t ev[kBatchEvents] = {};
@@ -152,12 +153,13 @@ fxc_status run_job(fxc_server* sv, fxc_scan** sp, Job* J) {
   if (sv->batch && !(cfg.products & FXC_PROD_RAW)) {
     // batched: stage, post to the dispatcher, collect behind its batch
     std::deque<std::pair<Posted, uint64_t>> posts;  // (post, sector index)
+    std::condition_variable cv_mine;  // the dispatcher wakes this worker only
     auto finish_posted = [&]() -> fxc_status {
       Posted& p = posts.front().first;
       const uint64_t sec = posts.front().second;
       {
         std::unique_lock<std::mutex> lk(sv->mu);
-        sv->cv_launched.wait(lk, [&] { return p.launched; });
+        cv_mine.wait(lk, [&] { return p.launched; });
       }
       fxc_status st = p.st;
       uint64_t id = 0;
@@ -178,6 +180,7 @@ fxc_status run_job(fxc_server* sv, fxc_scan** sp, Job* J) {
       const uint64_t nfs = j.nf ? std::min(sf, j.nf - f0) : 0;
       Posted np;
       np.s = s;
+      np.cv = &cv_mine;
       np.nf = nfs;
       np.first = j.first_frame + f0;
       fxc_status st;
@@ -361,15 +364,17 @@ void dispatcher(fxc_server* sv) {
     cudaEventRecord(sv->ev[e], sv->disp_stream);
     inflight.push_back(e);
     {
+      // notified under the lock: a worker cannot run on (and drop its post)
+      // before the dispatcher is done with it
       std::lock_guard<std::mutex> lk(sv->mu);
       for (Posted* p : take) {
         p->done = sv->ev[e];
         p->st = st;
         p->err = err;
         p->launched = true;
+        p->cv->notify_one();
       }
     }
-    sv->cv_launched.notify_all();
   }
   cudaStreamSynchronize(sv->disp_stream);
 }
