@@ -203,14 +203,14 @@ def flops_per_station_sample(n):
 
 # -------------------------------------------------------------- CPU legs
 
-def cpu_sample(cfg_o, get_sector, nsec, nfs, target_s=10.0):
-    """Times the oracle port (OpenMP, all host threads) sector by sector over
-    the scan until about target_s seconds of CPU work; returns (Gsample/s,
-    frames, threads, seconds)."""
+def cpu_sample(cfg_o, get_sector, nsec, nfs, target_s=10.0, threads=None):
+    """Times the oracle port (OpenMP, all host threads unless `threads`)
+    sector by sector over the scan until about target_s seconds of CPU work;
+    returns (Gsample/s, frames, threads, seconds)."""
     import oracle
 
     oracle.build()
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     frames, spent = 0, 0.0
     for i in range(nsec):
         r1, r2 = get_sector(i)
@@ -722,6 +722,14 @@ def main():
         cpu = {"value": v, "unit": "Gsample/s", "cores": thr, "kind": "port",
                "sample": f"first {nf_cpu} frame pairs of the scan ({dt:.1f} s of CPU work, "
                          f"C restatement, OpenMP over all host threads)"}
+        # the reference's own default pool: logical cores - 2 (src/main.rs:920-924)
+        thr_d = max(1, (os.cpu_count() or 1) - 2)
+        v_d, nf_d, _, dt_d = cpu_sample(
+            cfg_o, lambda i: (sec1[i].cpu().numpy(), sec2[i].cpu().numpy()), SECTORS_, NFS,
+            target_s=3.0, threads=thr_d)
+        cpu["at_reference_default_threads"] = {
+            "value": v_d, "threads": thr_d,
+            "sample": f"first {nf_d} frame pairs ({dt_d:.1f} s of CPU work)"}
 
     if rank == 0:
         line = {

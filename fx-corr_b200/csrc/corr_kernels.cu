@@ -19,6 +19,10 @@
 //      |S|^2 / S1 conj(S2) accumulation (src/main.rs:2491-2568) into per-thread
 //      f32 registers, flushed every 32 frames into per-CTA f64 partials;
 // reduce_partials_kernel then sums the per-CTA partials in a fixed order.
+// The frame loop is corr_span: the single-sector kernel runs it once per CTA
+// over the CTA's share of the sector, the batched kernel (corr_batch_kernel)
+// once per work item taken by ticket from a list spanning many scans, with
+// batch_frame_info_kernel and batch_reduce_kernel on either side.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
