@@ -219,14 +219,21 @@ phased_kernel(const PhasedParams p) {
       if (valid) {
         const float inv_n = 1.0f / (float)N;
         uint8_t* out = p.raw_out + frame_local * p.bpf_out;
+        // Consecutive lanes pack consecutive words, spw samples apart: each
+        // lane starts its word at a different sample (rot) so that the 16
+        // lanes of a half-warp read 16 different bank pairs of Y at every
+        // step instead of one.
+        const uint32_t lane = (uint32_t)t & 31u;
+        const uint32_t rot = spw >= 16 ? lane : lane / (16u / spw);
         for (uint32_t w = (uint32_t)t; w < wpf; w += T1) {
           uint32_t word = 0;
           for (uint32_t i = 0; i < spw; ++i) {
-            const uint32_t n = w * spw + i;
+            const uint32_t ii = (i + rot) & (spw - 1u);
+            const uint32_t n = w * spw + ii;
             float x = Y[n].x * inv_n;
             if (p.out_lsb && (n & 1u)) x = -x;
             word |= (nearest_level(x, ql, (int)p.nqlevels, p.qmonotonic) & qmask)
-                    << (i * p.bits_out);
+                    << (ii * p.bits_out);
           }
           const uint32_t sw = elut[word & 255u] | elut[256 + ((word >> 8) & 255u)] |
                               elut[512 + ((word >> 16) & 255u)] | elut[768 + (word >> 24)];
