@@ -242,6 +242,23 @@ def cpu_inputs_numpy(cfg, nf):
     return r1, r2
 
 
+def replica_throughput(dist, samples, ms, device):
+    """Whole-job throughput of independent replicas (the path shards by scan
+    or sector with no data-path collective): every rank's samples over the
+    slowest rank's time.  Returns (Gsample/s, slowest ms); dist None = one
+    process."""
+    if dist is None:
+        return samples / (ms * 1e-3) / 1e9, ms
+    import torch
+
+    t_ms = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    t_n = torch.tensor([float(samples)], dtype=torch.float64, device=device)
+    dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t_n, op=dist.ReduceOp.SUM)
+    ms, samples = float(t_ms.item()), float(t_n.item())
+    return samples / (ms * 1e-3) / 1e9, ms
+
+
 def run_reference(args, rank, world):
     """--impl reference: the CPU restatement of the reference path on this
     box's host cores, K bounded-sample steps."""
@@ -573,13 +590,6 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     cfg = scan_config(fxc)
     eng = fxc.Engine(local, max_inflight=3)
     scan = eng.open_scan(cfg)
@@ -622,9 +632,8 @@ def main():
     kern_ms, kern_launches, all_launches = scan.profile(reset=True)
     scan.set_profiling(False)
     scan.check()
-    ms = max_over_ranks(ms)
     samples_per_step = 2 * SECTORS_ * NFS * N
-    value = world * samples_per_step / (ms * 1e-3) / 1e9
+    value, ms = replica_throughput(dist, samples_per_step, ms, "cuda")
 
     # ---- end to end through the host-buffer C ABI (pinned host inputs)
     e2e = None
@@ -655,8 +664,9 @@ def main():
         e2e_run(args.e2e_steps)
         t1 = time.perf_counter()
         barrier()
-        e2e_ms = max_over_ranks((t1 - t0) * 1e3 / args.e2e_steps)
-        e2e = {"value": world * samples_per_step / (e2e_ms * 1e-3) / 1e9, "unit": "Gsample/s",
+        e2e_v, e2e_ms = replica_throughput(dist, samples_per_step, (t1 - t0) * 1e3 / args.e2e_steps,
+                                           "cuda")
+        e2e = {"value": e2e_v, "unit": "Gsample/s",
                "h2d_bytes_per_step": 2 * SECTORS_ * sec_bytes,
                "d2h_bytes_per_step": SECTORS_ * (5 * h * 8 + 4), "ms_per_step": e2e_ms,
                "path": "fxc_sector_submit/fxc_sector_wait, pinned host buffers, 3 sectors in "
