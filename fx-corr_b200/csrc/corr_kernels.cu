@@ -351,21 +351,40 @@ __global__ void __launch_bounds__(FPC * N / 16, MINB) corr_batch_kernel(const Ba
 // Fixed-order sum of the per-CTA partials.  The multipliers (exact powers of
 // two) undo the two-for-one 2x factor of each spectrum and the per-station
 // level scaling.  Writes acf11, acf22, xcf (re,im) and zeroes the phased slot.
-__global__ void reduce_partials_kernel(const double* __restrict__ part, int nblk, int h,
-                                       double m11, double m22, double m12,
-                                       double* __restrict__ out) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= h) return;
+// A 256-thread block covers 32 bins: each of its 8 warps sums one contiguous
+// eighth of the slots in slot order (coalesced 256-byte rows), then the eight
+// warp sums are added in warp order; the order depends only on nblk, so the
+// result is deterministic.
+constexpr int kRedBins = 32, kRedGroups = 8;
+
+__global__ void __launch_bounds__(kRedBins * kRedGroups)
+reduce_partials_kernel(const double* __restrict__ part, int nblk, int h, double m11, double m22,
+                       double m12, double* __restrict__ out) {
+  __shared__ double sm[kRedGroups][4][kRedBins];
+  const int lane = threadIdx.x & 31, grp = threadIdx.x >> 5;
+  const int k = blockIdx.x * kRedBins + lane;
+  const int b0 = (nblk * grp) / kRedGroups, b1 = (nblk * (grp + 1)) / kRedGroups;
   double s[4] = {0, 0, 0, 0};
-  for (int b = 0; b < nblk; ++b) {
-    const double* q = part + (size_t)b * 4 * h;
+  if (k < h) {
+    for (int b = b0; b < b1; ++b) {
+      const double* q = part + (size_t)b * 4 * h + k;
 #pragma unroll
-    for (int v = 0; v < 4; ++v) s[v] += q[(size_t)v * h + k];
+      for (int v = 0; v < 4; ++v) s[v] += q[(size_t)v * h];
+    }
   }
-  out[k] = m11 * s[0];
-  out[h + k] = m22 * s[1];
-  out[2 * h + 2 * k] = m12 * s[2];
-  out[2 * h + 2 * k + 1] = m12 * s[3];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) sm[grp][v][lane] = s[v];
+  __syncthreads();
+  if (grp != 0 || k >= h) return;
+  double t[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int g = 0; g < kRedGroups; ++g)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) t[v] += sm[g][v][lane];
+  out[k] = m11 * t[0];
+  out[h + k] = m22 * t[1];
+  out[2 * h + 2 * k] = m12 * t[2];
+  out[2 * h + 2 * k + 1] = m12 * t[3];
   out[4 * h + k] = 0.0;
 }
 
@@ -597,7 +616,8 @@ cudaError_t launch_batch_reduce(const BatchArgs& a, int grid, cudaStream_t s) {
 
 cudaError_t launch_reduce(const double* part, int nblk, int h, double m11, double m22, double m12,
                           double* out, cudaStream_t s) {
-  reduce_partials_kernel<<<(h + 255) / 256, 256, 0, s>>>(part, nblk, h, m11, m22, m12, out);
+  reduce_partials_kernel<<<(h + kRedBins - 1) / kRedBins, kRedBins * kRedGroups, 0, s>>>(
+      part, nblk, h, m11, m22, m12, out);
   return cudaGetLastError();
 }
 

@@ -250,13 +250,25 @@ phased_kernel(const PhasedParams p) {
 }
 
 // Fixed-order sum of the per-CTA phased partials into acc[4H, 5H).
-__global__ void reduce_phased_kernel(const double* __restrict__ part, int nblk, int h,
-                                     double* __restrict__ out) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= h) return;
+// (32 bins per block; each of 8 warps sums a contiguous eighth of the slots in
+// slot order, the warp sums are added in warp order: deterministic.)
+__global__ void __launch_bounds__(256) reduce_phased_kernel(const double* __restrict__ part,
+                                                            int nblk, int h,
+                                                            double* __restrict__ out) {
+  __shared__ double sm[8][32];
+  const int lane = threadIdx.x & 31, grp = threadIdx.x >> 5;
+  const int k = blockIdx.x * 32 + lane;
+  const int b0 = (nblk * grp) / 8, b1 = (nblk * (grp + 1)) / 8;
   double s = 0.0;
-  for (int b = 0; b < nblk; ++b) s += part[(size_t)b * h + k];
-  out[4 * h + k] = s;
+  if (k < h)
+    for (int b = b0; b < b1; ++b) s += part[(size_t)b * h + k];
+  sm[grp][lane] = s;
+  __syncthreads();
+  if (grp != 0 || k >= h) return;
+  double t = 0.0;
+#pragma unroll
+  for (int g = 0; g < 8; ++g) t += sm[g][lane];
+  out[4 * h + k] = t;
 }
 
 template <int N, int FPC>
@@ -284,7 +296,7 @@ cudaError_t launch_phased(uint32_t n, const PhasedParams& p, int grid, cudaStrea
 }
 
 cudaError_t launch_reduce_phased(const double* part, int nblk, int h, double* out, cudaStream_t s) {
-  reduce_phased_kernel<<<(h + 255) / 256, 256, 0, s>>>(part, nblk, h, out);
+  reduce_phased_kernel<<<(h + 31) / 32, 256, 0, s>>>(part, nblk, h, out);
   return cudaGetLastError();
 }
 
