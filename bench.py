@@ -690,7 +690,7 @@ def main():
         serve = {
             # the headline's served vs plain: short 2-bit FFT-8192 jobs, batched server
             "short": guarded(lambda: serve_leg(
-                fxc, torch, eng, short_jobs(args.serve_short_jobs, rate=4000.0), slots=64,
+                fxc, torch, eng, short_jobs(args.serve_short_jobs, rate=4000.0), slots=32,
                 batch=True, plain_jobs=200, label="short jobs, FFT 8192",
                 mix="Poisson arrivals at 4000 jobs/s; 1-16 ms at 1024 Msps (125-2000 frame "
                     "pairs), 2-bit, FFT 8192, random delays/rates, one dump, pinned host buffers")),
