@@ -147,6 +147,10 @@ std::vector<Spec> specs() {
   v.push_back({"pipeline-depth", {}, Kind::One, false, false, 1, "N",
                "Reader-worker queue depth [chunks] (auto when omitted)", false,
                opt_u(&Args::pipeline_depth)});
+  v.push_back({"jobs", {}, Kind::One, false, false, 1, "N",
+               "Run up to N <process> entries of the schedule at once, their sectors computed "
+               "together in batches on the GPU (this build's extension) [default: 1, one after "
+               "another]", false, opt_u(&Args::jobs)});
   v.push_back({"debug", {}, Kind::Flag, false, false, 0, "",
                "Enable diagnostic debug logging to file (all frames)", false,
                flag(&Args::debug)});

@@ -30,6 +30,7 @@ struct Args {
   std::vector<std::string> tsys, diameter, eta, gain, sefd;
   bool fringe = false;
   std::optional<size_t> cpu, chunk_frames, pipeline_depth, process_index;
+  std::optional<size_t> jobs;  // extension: <process> entries run at once
   bool razoku5bay = false, debug = false, stdout_log = false, compact_logs = false;
   std::string delay_reference = "ant2";
 };

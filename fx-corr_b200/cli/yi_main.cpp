@@ -18,7 +18,9 @@
 #include <cstring>
 #include <deque>
 #include <memory>
+#include <exception>
 #include <mutex>
+#include <set>
 #include <optional>
 #include <stdexcept>
 #include <string>
@@ -68,6 +70,33 @@ struct Fail : std::runtime_error {
 // (main.rs:36-108, yi-corr only).
 FILE* g_tee = nullptr;
 std::mutex g_log_mu;
+
+// Output files held by the processes running at once (--jobs): two
+// processes that would write the same file take turns, as they would one
+// after another.
+std::mutex g_out_mu;
+std::condition_variable g_out_cv;
+std::set<std::string> g_out_busy;
+
+struct OutputClaim {
+  std::vector<std::string> paths;
+  explicit OutputClaim(std::vector<std::string> p) : paths(std::move(p)) {
+    std::unique_lock<std::mutex> lk(g_out_mu);
+    g_out_cv.wait(lk, [&] {
+      for (const auto& x : paths)
+        if (g_out_busy.count(x)) return false;
+      return true;
+    });
+    for (const auto& x : paths) g_out_busy.insert(x);
+  }
+  ~OutputClaim() {
+    {
+      std::lock_guard<std::mutex> lk(g_out_mu);
+      for (const auto& x : paths) g_out_busy.erase(x);
+    }
+    g_out_cv.notify_all();
+  }
+};
 
 void logf(const char* fmt, ...) __attribute__((format(printf, 1, 2)));
 void logf(const char* fmt, ...) {
@@ -305,7 +334,11 @@ std::string join_csv(const int* v, int n) {
   return s;
 }
 
-void run_once(const Args& args, Mode mode, const std::optional<Schedule>& sch, fxc_engine* eng) {
+// With `server` (--jobs > 1) the sectors are submitted as one-dump jobs to
+// a batched server shared by the processes running at once; otherwise they
+// stream through a scan of this process.
+void run_once(const Args& args, Mode mode, const std::optional<Schedule>& sch, fxc_engine* eng,
+              fxc_server* server = nullptr) {
   const bool fringe_enabled = mode == Mode::PhasedArray && args.fringe;
   if (args.fringe && mode != Mode::PhasedArray) logf("[info] --fringe is ignored for this mode");
   if (fringe_enabled)
@@ -666,10 +699,12 @@ void run_once(const Args& args, Mode mode, const std::optional<Schedule>& sch, f
   d.lo1_hz = lo1_hz;
   d.lo2_hz = lo2_hz;
   fxc_scan* scan = nullptr;
-  ck(fxc_scan_open(eng, &cfg, &scan), "fxc_scan_open");
+  if (!server) ck(fxc_scan_open(eng, &cfg, &scan), "fxc_scan_open");
   struct ScanCloser {
     fxc_scan* s;
-    ~ScanCloser() { fxc_scan_close(s); }
+    ~ScanCloser() {
+      if (s) fxc_scan_close(s);
+    }
   } closer{scan};
 
   // writers (main.rs:2074-2096)
@@ -685,6 +720,20 @@ void run_once(const Args& args, Mode mode, const std::optional<Schedule>& sch, f
   CorStation s1{a1_name, a1_code, {ant1_ecef[0], ant1_ecef[1], ant1_ecef[2]}};
   CorStation s2{a2_name, a2_code, {ant2_ecef[0], ant2_ecef[1], ant2_ecef[2]}};
   CorStation sm{"YAMAGU66", (uint8_t)'M', {ant1_ecef[0], ant1_ecef[1], ant1_ecef[2]}};
+  std::unique_ptr<OutputClaim> claim;
+  if (server) {
+    std::vector<std::string> outs;
+    if (write_phased_cor)
+      outs.push_back(join(o_dir, "YAMAGU66_YAMAGU66_" + c_tag + "_" + cor_label + ".cor"));
+    if (write_acf_cor) {
+      outs.push_back(join(o_dir, n1f + "_" + n1f + "_" + c_tag + "_" + cor_label + ".cor"));
+      outs.push_back(join(o_dir, n2f + "_" + n2f + "_" + c_tag + "_" + cor_label + ".cor"));
+    }
+    if (write_xcf_cor)
+      outs.push_back(join(o_dir, n1f + "_" + n2f + "_" + c_tag + "_" + cor_label + ".cor"));
+    if (write_raw) outs.push_back(o_path);
+    claim = std::make_unique<OutputClaim>(std::move(outs));
+  }
   std::unique_ptr<CorWriter> cw_ph, cw_11, cw_12, cw_22;
   if (write_phased_cor)
     cw_ph = std::make_unique<CorWriter>(
@@ -714,12 +763,28 @@ void run_once(const Args& args, Mode mode, const std::optional<Schedule>& sch, f
   struct Inflight {
     uint64_t id;
     SectorBuf* buf;
+    std::vector<double> out;    // server jobs: acf11 | acf22 | xcf | phased
+    std::vector<uint8_t> raw;   // server jobs: phased .raw frames
   };
   std::deque<Inflight> inflight;
+  // on an error, server jobs still reading this process's reader buffers
+  // finish before the buffers are freed (declared after the reader, so
+  // destroyed before it)
+  struct DrainJobs {
+    std::deque<Inflight>* q;
+    fxc_server* sv;
+    ~DrainJobs() {
+      if (!sv) return;
+      for (auto& in : *q) {
+        fxc_job_stats js;
+        fxc_server_wait(sv, in.id, -1, &js);
+      }
+    }
+  } drain{&inflight, server};
   uint64_t emitted = 0;
   const auto t_start = std::chrono::steady_clock::now();
   auto finish = [&]() {
-    Inflight in = inflight.front();
+    Inflight in = std::move(inflight.front());
     inflight.pop_front();
     const uint64_t nf = in.buf->nf;
     const size_t si = in.buf->index;
@@ -734,7 +799,17 @@ void run_once(const Args& args, Mode mode, const std::optional<Schedule>& sch, f
       o.raw_out = raw_frames.data();
       o.raw_out_len = raw_frames.size();
     }
-    ck(fxc_sector_wait(scan, in.id, -1, &o), "sector");
+    if (server) {
+      fxc_job_stats js;
+      ck(fxc_server_wait(server, in.id, -1, &js), "sector");
+      std::memcpy(acc11.data(), in.out.data(), sizeof(double) * h);
+      std::memcpy(acc22.data(), in.out.data() + h, sizeof(double) * h);
+      std::memcpy(xcf.data(), in.out.data() + 2 * h, sizeof(double) * 2 * h);
+      std::memcpy(ph.data(), in.out.data() + 4 * h, sizeof(double) * h);
+      if (write_raw) raw_frames = std::move(in.raw);
+    } else {
+      ck(fxc_sector_wait(scan, in.id, -1, &o), "sector");
+    }
     reader.release(in.buf);
     if (raw_out && !raw_frames.empty() &&
         std::fwrite(raw_frames.data(), 1, raw_frames.size(), raw_out) != raw_frames.size())
@@ -761,16 +836,38 @@ void run_once(const Args& args, Mode mode, const std::optional<Schedule>& sch, f
       ck(fxc_normalize((uint32_t)fft_len, nf, lp2, acc22.data(), nullptr, spec.data()), "normalize");
       cw_22->write_sector(ts, integ, spec.data());
     }
-    std::printf("\r[info] %s second %zu/%zu (%.2f%%)",
-                mode == Mode::PhasedArray ? "Synthesised" : "Processed", si + 1, counts.size(),
-                100.0 * (double)emitted / (double)total_f);
-    std::fflush(stdout);
+    if (!server) {  // processes running at once would overwrite each other's line
+      std::printf("\r[info] %s second %zu/%zu (%.2f%%)",
+                  mode == Mode::PhasedArray ? "Synthesised" : "Processed", si + 1, counts.size(),
+                  100.0 * (double)emitted / (double)total_f);
+      std::fflush(stdout);
+    }
   };
   uint64_t first_frame = 0;
   for (;;) {
+    // server jobs hold their reader buffers until done: leave the reader one
+    if (server && (int)inflight.size() >= depth - 1) finish();
     SectorBuf* b = reader.next();
     if (!b) break;
     uint64_t id = 0;
+    if (server) {
+      Inflight in{0, b, std::vector<double>(5 * h), {}};
+      if (write_raw) in.raw.resize(b->nf * bpf_o);
+      fxc_job j;
+      std::memset(&j, 0, sizeof j);
+      j.cfg = &cfg;
+      j.raw1 = b->b1;
+      j.raw2 = b->b2;
+      j.nf = b->nf;
+      j.first_frame = first_frame;
+      j.sector_frames = 0;
+      j.out = in.out.data();
+      j.raw_out = write_raw ? in.raw.data() : nullptr;
+      ck(fxc_server_submit(server, &j, &in.id), "fxc_server_submit");
+      first_frame += b->nf;
+      inflight.push_back(std::move(in));
+      continue;
+    }
     for (;;) {
       const fxc_status st = fxc_sector_submit(scan, b->b1, b->nf * bpf1, b->b2, b->nf * bpf2, b->nf,
                                               first_frame, &id);
@@ -782,10 +879,10 @@ void run_once(const Args& args, Mode mode, const std::optional<Schedule>& sch, f
       break;
     }
     first_frame += b->nf;
-    inflight.push_back({id, b});
+    inflight.push_back({id, b, {}, {}});
   }
   while (!inflight.empty()) finish();
-  if (!counts.empty()) std::printf("\n");
+  if (!counts.empty() && !server) std::printf("\n");
   const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
   logf("[info] I/O reader summary: avg=%.1f MiB/s total=%.1f MiB, %.3f s",
        (double)reader.bytes_read() / (1024.0 * 1024.0) / std::max(el, 1e-9),
@@ -860,6 +957,59 @@ int real_main(int argc, char** argv) {
   } ec{eng};
   const bool run_all = sch && sch->processes.size() > 1 && !args.process_index && !args.epoch &&
                        !args.ra && !args.dec && !args.length && args.skip == 0.0;
+  if (run_all && args.jobs && *args.jobs > 1) {
+    // this build's extension: up to --jobs processes at once, their sectors
+    // computed together by a batched server (fixed kernel shapes, so the
+    // products do not depend on timing)
+    const size_t np = sch->processes.size();
+    const size_t nj = std::min(*args.jobs, np);
+    logf("[info] Processing all scans, %zu at a time: %zu process entries", nj, np);
+    fxc_server_opts so;
+    std::memset(&so, 0, sizeof so);
+    so.slots = (int32_t)std::min<size_t>(256, std::max<size_t>(4, 2 * nj));
+    so.batch = 2;
+    fxc_server* sv = nullptr;
+    ck(fxc_server_create(eng, &so, &sv), "fxc_server_create");
+    struct ServerCloser {
+      fxc_server* s;
+      ~ServerCloser() { fxc_server_destroy(s); }
+    } sc{sv};
+    std::mutex mu;
+    size_t next = 0;
+    std::exception_ptr first_error;
+    auto worker = [&]() {
+      for (;;) {
+        size_t idx;
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          if (next >= np || first_error) return;
+          idx = next++;
+        }
+        const ProcessEntry& p = sch->processes[idx];
+        logf("[info] process %zu/%zu: epoch=%s skip=%g length=%s", idx + 1, np, p.epoch.c_str(),
+             p.skip_sec, p.length_sec ? std::to_string(*p.length_sec).c_str() : "-");
+        Args ra = args;
+        ra.process_index = idx;
+        ra.compact_logs = true;
+        const auto t0 = std::chrono::steady_clock::now();
+        try {
+          run_once(ra, mode, sch, eng, sv);
+          logf("[info] process %zu/%zu elapsed: %.3fs", idx + 1, np,
+               std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+        } catch (...) {
+          logf("[error] process %zu/%zu failed after %.3fs", idx + 1, np,
+               std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+          std::lock_guard<std::mutex> lk(mu);
+          if (!first_error) first_error = std::current_exception();
+        }
+      }
+    };
+    std::vector<std::thread> ths;
+    for (size_t k = 0; k < nj; ++k) ths.emplace_back(worker);
+    for (auto& t : ths) t.join();
+    if (first_error) std::rethrow_exception(first_error);
+    return 0;
+  }
   if (run_all) {
     const size_t np = sch->processes.size();
     logf("[info] Processing all scans sequentially: %zu process entries", np);

@@ -393,7 +393,7 @@ fxc_status fxc_server_create(fxc_engine* e, const fxc_server_opts* opts, fxc_ser
   if (opts && opts->batch) {
     fxc_batch_opts bo{};
     bo.use_graphs = 1;
-    bo.autotune = 1;
+    bo.autotune = opts->batch == 1 ? 1 : 0;  // 2: fixed shapes, timing-independent products
     fxc_status st = fxc_batch_create(e, &bo, &sv->batch);
     if (st != FXC_OK) {
       delete sv;

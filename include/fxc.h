@@ -221,7 +221,9 @@ typedef struct fxc_server_opts {
   int32_t slots;             /* jobs on the device at once (0 = 4, at most 256) */
   int32_t batch;             /* 1: the sectors of all running jobs are computed
                                 together, one fxc_batch call (CUDA graphs,
-                                autotuned shapes) per round of ready sectors */
+                                autotuned shapes) per round of ready sectors;
+                                2: the same with the default kernel shapes, so
+                                that the products do not depend on timing */
 } fxc_server_opts;
 
 typedef struct fxc_job {

@@ -189,3 +189,49 @@ def test_multi_process_schedule(tmp_path):
     assert "Processing all scans sequentially: 2 process entries" in r.stdout
     names = sorted(p.name for p in out.glob("*.cor"))
     assert names == [f"YAMAGU32_YAMAGU34_{TAG}_cli.cor", f"YAMAGU32_YAMAGU34_2024043155201_cli.cor"]
+
+
+def _cor_records(path: Path, fft: int):
+    b = path.read_bytes()
+    nsec = int.from_bytes(b[28:32], "little", signed=True)
+    rec = 128 + fft // 2 * 8
+    heads = [b[256 + k * rec:256 + k * rec + 128] for k in range(nsec)]
+    return b[:256], heads, read_cor(path, fft)[1]
+
+
+def test_multi_process_jobs_match_sequential(tmp_path):
+    """--jobs (this build's extension) runs the <process> entries at once, their
+    sectors computed together by a batched server: the same files with the same
+    header bytes, spectra within FP32 rounding of the one-after-another run;
+    phased products (per-scan path inside the server) identical byte for byte."""
+    sched, raw = write_case(tmp_path, seconds=3.3, seed=5)
+    # <length> counts from the epoch, as in the reference: skip k, length k + 1
+    procs = "".join(
+        f"  <process><epoch>{EPOCH}</epoch><skip>{k}</skip><length>{k + 1}</length>"
+        "<object>SRC</object><stations>AB</stations></process>\n" for k in (1, 2))
+    sched.write_text(sched.read_text().replace("</schedule>", procs + "</schedule>"))
+    seq, par = tmp_path / "seq", tmp_path / "par"
+    run_tool("yi-corr", "--sc", sched, "--raw", raw, "--cor", seq, "--sideband", "USB")
+    r = run_tool("yi-corr", "--sc", sched, "--raw", raw, "--cor", par, "--sideband", "USB",
+                 "--jobs", "3")
+    assert "Processing all scans, 3 at a time: 3 process entries" in r.stdout
+    names = sorted(p.name for p in seq.glob("*.cor"))
+    assert len(names) == 9 and names == sorted(p.name for p in par.glob("*.cor"))
+    for name in names:
+        h_s, sh_s, sp_s = _cor_records(seq / name, FFT)
+        h_p, sh_p, sp_p = _cor_records(par / name, FFT)
+        assert h_s == h_p and sh_s == sh_p, name
+        for a, b in zip(sp_p, sp_s):
+            assert np.max(np.abs(a - b)) <= 1e-5 * np.max(np.abs(b)), name
+    # phased outputs go to the working directory
+    (tmp_path / "ph_seq").mkdir()
+    (tmp_path / "ph_par").mkdir()
+    run_tool("yi-phasedarray", "--sc", sched, "--raw", raw, "--sideband", "USB",
+             cwd=tmp_path / "ph_seq")
+    run_tool("yi-phasedarray", "--sc", sched, "--raw", raw, "--sideband", "USB", "--jobs", "3",
+             cwd=tmp_path / "ph_par")
+    files = sorted(p.name for p in (tmp_path / "ph_seq").iterdir() if p.is_file())
+    assert files and files == sorted(p.name for p in (tmp_path / "ph_par").iterdir()
+                                     if p.is_file())
+    for name in files:
+        assert (tmp_path / "ph_seq" / name).read_bytes() == (tmp_path / "ph_par" / name).read_bytes()
