@@ -390,6 +390,9 @@ Schedule parse_xml_schedule(const std::string& path) {
       if (try_f64(*s, &v)) e.length_sec = v;
     }
     e.object = p->child_text("object");
+    if (auto s = p->child_text("fft"); s && !s->empty()) e.fft = parse_usize(trim(*s), "process/fft");
+    if (auto s = p->child_text("bit"); s && !s->empty()) e.bit = parse_usize(trim(*s), "process/bit");
+    if (auto s = p->child_text("level"); s && !s->empty()) e.level = trim(*s);
     e.stations = p->child_text("stations");
     if (e.stations) {
       std::string stn;

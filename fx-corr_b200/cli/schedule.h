@@ -30,6 +30,11 @@ struct ProcessEntry {
   double skip_sec = 0.0;
   std::optional<double> length_sec;
   std::optional<std::string> object, stations, ra, dec;
+  // this build's extension (the reference has one <stream> fft and takes the
+  // bit depth from the command line): per-process FFT length, bit depth of
+  // both stations and level table
+  std::optional<size_t> fft, bit;
+  std::optional<std::string> level;
 };
 
 struct Schedule {

@@ -365,12 +365,34 @@ void run_once(const Args& args, Mode mode, const std::optional<Schedule>& sch, f
     }
   }
   // configuration merge, with the reference's precedence (main.rs:1061-1110)
-  const size_t fft_len =
+  size_t fft_len =
       args.fft == kDefaultFft ? (sch && sch->fft ? *sch->fft : args.fft) : args.fft;
   const std::vector<std::string> bit_a = args.bin.empty() ? std::vector<std::string>{"2"} : args.bin;
-  const auto bits = per_antenna_usize(bit_a, sch && sch->ant1_bit ? *sch->ant1_bit : 2);
+  auto bits = per_antenna_usize(bit_a, sch && sch->ant1_bit ? *sch->ant1_bit : 2);
+  // this build's per-process extension: <fft>, <bit> (both stations) and
+  // <level> inside <process> override the values above; a <bit> without a
+  // <level> takes the uniform table of 2^b half-integer steps
+  std::optional<std::string> proc_level;
+  if (proc && proc->fft) fft_len = *proc->fft;
+  if (proc && proc->bit) {
+    bits = {*proc->bit, *proc->bit};
+    proc_level = proc->level;
+    if (!proc_level) {
+      std::string d;
+      const long n = 1L << *proc->bit;
+      for (long i = 0; i < n; ++i) {
+        char b[32];
+        std::snprintf(b, sizeof b, "%s%.1f", i ? "," : "", (double)i - 0.5 * (double)(n - 1));
+        d += b;
+      }
+      proc_level = d;
+    }
+  } else if (proc && proc->level) {
+    proc_level = proc->level;
+  }
   const size_t bit1 = bits.first, bit2 = bits.second, bit_out = std::max(bit1, bit2);
-  const auto level_args = normalize_level_args(args.level, bit1, bit2);
+  const auto level_args = proc_level ? std::vector<std::string>{*proc_level}
+                                     : normalize_level_args(args.level, bit1, bit2);
   const auto lv_s = per_antenna_str(
       level_args, sch && sch->ant1_level ? *sch->ant1_level : std::string("-1.5,-0.5,0.5,1.5"));
   const std::vector<double> levels1 = parse_levels(bit1, lv_s.first);

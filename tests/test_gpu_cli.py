@@ -235,3 +235,77 @@ def test_multi_process_jobs_match_sequential(tmp_path):
                                      if p.is_file())
     for name in files:
         assert (tmp_path / "ph_seq" / name).read_bytes() == (tmp_path / "ph_par" / name).read_bytes()
+
+
+def _derived_mixed(total_f, fft, bits, levels):
+    """derived_scan for another FFT length and bit depth (same stations,
+    clocks and zero geometry); the reader starts station 2 at the word
+    boundary at or before the clock offset (main.rs:1577-1616), the rest of
+    the offset stays in the delay model."""
+    spw = 32 // bits
+    seek2 = round(CLOCK2_S * FS) // spw * spw
+    d_seek = seek2 / FS
+    n_table = max(math.ceil(total_f * fft / FS), 1) + 1
+    delay = dict(time_offset_s=0.0, clock2_delay_s=CLOCK2_S, clock2_rate_sps=CLOCK2_RATE,
+                 d_seek=d_seek, net_d1_base=CLOCK2_S - d_seek, total_rate1_base=CLOCK2_RATE,
+                 total_accel1_base=-0.0, lo1_hz=OBS_HZ, lo2_hz=OBS_HZ)
+    scan = oracle.Scan(fft=fft, fs=FS, bits1=bits, bits2=bits, levels1=list(levels),
+                       levels2=list(levels), shuffle1=list(range(32)), shuffle2=list(range(32)),
+                       lsb1=False, lsb2=False, band=(0, 0, fft // 2, 0), grid=0,
+                       products=oracle.PROD_ACF | oracle.PROD_XCF, delay=delay,
+                       geom_table=np.zeros(n_table))
+    return scan, seek2 * bits // 8
+
+
+def test_mixed_fft_and_bits_per_process(tmp_path, engine):
+    """Config 4's mixed classes in one schedule, through this build's
+    per-process <fft>/<bit>/<level> extension: FFT 1024 / 4096 / 16384 at
+    2 / 1 / 4 bits (the last with the default uniform level table).  The
+    one-after-another run equals the library on each derived configuration
+    bit for bit; the --jobs run (one batched server, three FFT lengths at
+    once) matches it within FP32 rounding."""
+    sched, raw = write_case(tmp_path, seconds=0.1, seed=9)
+    procs = [("2024/043 15:53:00", "2024043155300", 1024, 2, [-3.0, -1.0, 1.0, 3.0], True),
+             ("2024/043 15:54:00", "2024043155400", 4096, 1, [-1.0, 1.0], True),
+             ("2024/043 15:55:00", "2024043155500", 16384, 4, oracle.default_levels(4), False)]
+    xml = sched.read_text()
+    a, b = xml.index("<process>"), xml.index("</process>") + len("</process>")
+    entries = ""
+    for k, (ep, tag, fft, bits, lv, explicit) in enumerate(procs):
+        lvs = f"<level>{','.join(f'{x:g}' for x in lv)}</level>" if explicit else ""
+        entries += (f"<process><epoch>{ep}</epoch><length>1</length><fft>{fft}</fft>"
+                    f"<bit>{bits}</bit>{lvs}<object>SRC</object><stations>AB</stations>"
+                    "</process>\n  ")
+        n = int(1.1 * FS)
+        n -= n % fft
+        x1, x2 = oracle.synth_station_pair(n, 40 + k, rho=0.1, delay_samples=LAG + CLOCK2_S * FS)
+        ident = list(range(32))
+        (raw / f"YAMAGU32_{tag}.raw").write_bytes(
+            oracle.encode_station(x1, bits, lv, ident, False).tobytes())
+        (raw / f"YAMAGU34_{tag}.raw").write_bytes(
+            oracle.encode_station(x2, bits, lv, ident, False).tobytes())
+    sched.write_text(xml[:a] + entries + xml[b:])
+    seq, par = tmp_path / "seq", tmp_path / "par"
+    run_tool("yi-corr", "--sc", sched, "--raw", raw, "--cor", seq, "--sideband", "USB")
+    run_tool("yi-corr", "--sc", sched, "--raw", raw, "--cor", par, "--sideband", "USB",
+             "--jobs", "3")
+    for ep, tag, fft, bits, lv, _ in procs:
+        total_f = int(1.0 * FS / fft)
+        names = [f"YAMAGU32_YAMAGU32_{tag}_cli.cor", f"YAMAGU32_YAMAGU34_{tag}_cli.cor",
+                 f"YAMAGU34_YAMAGU34_{tag}_cli.cor"]
+        scan, off2 = _derived_mixed(total_f, fft, bits, lv)
+        bpf = scan.bpf(bits)
+        r1 = np.fromfile(raw / f"YAMAGU32_{tag}.raw", np.uint8)[: total_f * bpf]
+        r2 = np.fromfile(raw / f"YAMAGU34_{tag}.raw", np.uint8)[off2: off2 + total_f * bpf]
+        s = engine.open_scan(to_fxc(scan))
+        lib = s.wait(s.submit(r1, r2, total_f, 0))
+        s.close()
+        p = float(np.mean(np.square(lv)))
+        inv = 1.0 / (0.5 * p * total_f * float(fft) ** 2)
+        for name, key in zip(names, ("acf11", "xcf", "acf22")):
+            nsec, got = read_cor(seq / name, fft)
+            assert nsec == 1, name
+            want = (lib[key][: fft // 2] * inv).astype(np.complex64)
+            assert np.array_equal(got[0].astype(np.complex64), want), name
+            _, gp = read_cor(par / name, fft)
+            assert np.max(np.abs(gp[0] - got[0])) <= 1e-5 * np.max(np.abs(got[0])), name
