@@ -497,6 +497,32 @@ fxc_status run_batch(fxc_batch* b, fxc_scan* const* scans, const uint8_t* const*
 
 }  // namespace
 
+namespace fxc {
+
+void batch_release(fxc_batch* b) {
+  if (!b) return;
+  std::lock_guard<std::mutex> lk(b->mu);
+  DeviceGuardB dg(b->device);
+  cudaEventSynchronize(b->ev_done);
+  drop_graphs(b);
+  for (auto& A : b->arena) {
+    if (A.staged) cudaEventSynchronize(A.staged);
+    cudaFree(A.d);
+    if (A.h) cudaFreeHost(A.h);
+    A.d = nullptr;
+    A.h = nullptr;
+    A.cap = 0;
+    A.hcap = 0;
+  }
+  cudaFree(b->d_part);
+  b->d_part = nullptr;
+  b->part_cap = 0;
+  engine_release(b->eng, b->charged);
+  b->charged = 0;
+}
+
+}  // namespace fxc
+
 extern "C" {
 
 fxc_status fxc_batch_create(fxc_engine* e, const fxc_batch_opts* opts, fxc_batch** out) {

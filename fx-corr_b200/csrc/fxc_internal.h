@@ -61,6 +61,10 @@ fxc_status sector_collect(fxc_scan* s, const StagedSector& ss, cudaEvent_t compu
 // Gives back a staged slot whose sector was never computed.
 void sector_release(fxc_scan* s, const StagedSector& ss);
 
+// Frees a batch's device tables and partials (and their budget charge) once
+// its last call's work is done; the next call grows them again.
+void batch_release(fxc_batch* b);
+
 // Registers (add) or forgets a batch, destroyed by fxc_engine_destroy.
 void engine_track_batch(fxc_engine* e, fxc_batch* b, bool add);
 

@@ -98,6 +98,7 @@ fxc_status run_job(fxc_server* sv, fxc_scan** sp, Job* J) {
   fxc_scan_cfg cfg = J->cfg;
   cfg.delay.geom_table = J->table.empty() ? nullptr : J->table.data();
   // admission: bind the slot's scan within the budget, or wait for memory
+  bool batch_released = false;
   for (;;) {
     fxc_status st = *sp ? fxc::scan_bind(*sp, &cfg) : fxc_scan_open(sv->eng, &cfg, sp);
     if (st != FXC_EBUSY) {
@@ -110,7 +111,17 @@ fxc_status run_job(fxc_server* sv, fxc_scan** sp, Job* J) {
       continue;
     }
     std::unique_lock<std::mutex> lk(sv->mu);
-    if (sv->running <= 1 && sv->idle_holding == 0) return st;  // nothing can free memory
+    if (sv->running <= 1 && sv->idle_holding == 0) {
+      // no other job holds memory; the batch's tables and partials (grown
+      // by earlier batches) are the last thing to give back
+      if (sv->batch && !batch_released) {
+        lk.unlock();
+        fxc::batch_release(sv->batch);
+        batch_released = true;
+        continue;
+      }
+      return st;  // nothing can free memory
+    }
     sv->pressure = true;
     sv->cv_work.notify_all();
     sv->cv_done.wait_for(lk, std::chrono::milliseconds(2));
