@@ -128,8 +128,12 @@ int main(int argc, char** argv) {
       std::printf("clock=%.17g,%.17g processes=%zu\n", s.ant1_clock_delay_s.value_or(-1),
                   s.ant2_clock_delay_s.value_or(-1), s.processes.size());
       for (const auto& p : s.processes)
-        std::printf("process epoch=%s skip=%.17g length=%s\n", p.epoch.c_str(), p.skip_sec,
-                    p.length_sec ? std::to_string(*p.length_sec).c_str() : "-");
+        std::printf("process epoch=%s skip=%.17g length=%s fft=%s bit=%s level=%s\n",
+                    p.epoch.c_str(), p.skip_sec,
+                    p.length_sec ? std::to_string(*p.length_sec).c_str() : "-",
+                    p.fft ? std::to_string(*p.fft).c_str() : "-",
+                    p.bit ? std::to_string(*p.bit).c_str() : "-",
+                    p.level ? p.level->c_str() : "-");
     } else {
       return 2;
     }

@@ -244,6 +244,7 @@ def test_xml_schedule_fields(tool, tmp_path):
   <process><epoch>2024/043 15:52:00</epoch><skip>2</skip><length>5</length><object>S2</object><stations>AB</stations></process>
   <process><epoch>2024/043 16:00:00</epoch><object>S1</object><stations>AX</stations></process>
   <process><epoch>2024/043 17:00:00</epoch><object>S1</object><stations>BA</stations></process>
+  <process><epoch>2024/043 18:00:00</epoch><fft> 16384 </fft><bit>4</bit><level>-1.5,-0.5,0.5,1.5</level><object>S1</object><stations>AB</stations></process>
 </schedule>"""
     p = tmp_path / "s.xml"
     p.write_text(xml)
@@ -256,5 +257,8 @@ def test_xml_schedule_fields(tool, tmp_path):
     assert "rot=1000000,-2000000" in out
     assert "clock=9.9999999999999995e-07,3.0000000000000001e-06" in out
     # processes without both station keys are dropped (src/xml.rs:265-270)
-    assert "processes=2" in out
-    assert "process epoch=2024/043 15:52:00 skip=2 length=5.000000" in out
+    assert "processes=3" in out  # the AX process has no station B
+    assert "process epoch=2024/043 15:52:00 skip=2 length=5.000000 fft=- bit=- level=-" in out
+    # this build's per-process extension (<fft>, <bit>, <level> inside <process>)
+    assert ("process epoch=2024/043 18:00:00 skip=0 length=- fft=16384 bit=4 "
+            "level=-1.5,-0.5,0.5,1.5") in out
