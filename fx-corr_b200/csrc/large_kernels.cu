@@ -70,25 +70,59 @@ __global__ void decode_global_kernel(const LargeParams p, uint64_t f0, uint64_t 
   }
 }
 
+// Per-station decode plan of decode_dif_kernel: for a station whose samples
+// are contiguous runs of word bits after the shuffle (1- and 2-bit stations
+// under any shuffle, wider ones unshuffled), sample slot c of a word is read
+// with one or two shifts: code = (w >> p0) & mask, or, for a 2-bit sample whose
+// two bits the shuffle separates or swaps, ((w >> p0) & 1) | ((w >> p1) & 1) << 1.
+// Bit j of slot c's code is word bit perm[c b + j] (src/utils.rs:159-171).
+struct ShiftPlan {
+  uint32_t p0[32], p1[32];
+  uint32_t split;  // bit c: slot c takes two shifts
+};
+
+__device__ __forceinline__ bool shift_decodable(const StationParams& q) {
+  return q.bits <= 2 || q.shkind == SH_IDENTITY;
+}
+
+__device__ __forceinline__ void build_shift_plan(const StationParams& q, ShiftPlan& sp, int i) {
+  const int b = q.bits, spw = 32 / b;
+  if (i >= spw) return;
+  const bool natural = q.shkind == SH_IDENTITY;
+  const uint32_t p0 = natural ? (uint32_t)(i * b) : q.perm[i * b];
+  const uint32_t p1 = b == 2 ? (natural ? (uint32_t)(i * b + 1) : q.perm[i * b + 1]) : 0u;
+  sp.p0[i] = p0;
+  sp.p1[i] = p1;
+  if (b == 2 && p1 != p0 + 1) atomicOr(&sp.split, 1u << i);
+}
+
 // Decode + shift fused with the first (radix-C, decimation in frequency)
 // step of the four-step FFT: thread (frame, m) decodes samples m + M c of both
 // stations (z = x1 + i x2, station 2 negated on odd frames as in
 // decode_global_kernel), combines them with a C-point DFT and writes row q,
 // column m twiddled by W_N^(m q) — the complex frame never goes to HBM.
+// M is a whole number of words, so the C samples of a column sit in the same
+// slot of C words: the slot's shifts are looked up once per station.
 template <int C>
 __global__ void decode_dif_kernel(const LargeParams p, uint64_t f0, uint64_t nb,
                                   float2* __restrict__ y) {
   __shared__ uint32_t lut[2048];
   __shared__ float lv[512];
+  __shared__ ShiftPlan plan[2];
   for (int i = threadIdx.x; i < 512; i += blockDim.x)
     lv[i] = p.st[i >> 8].levels[i & 255] * p.st[i >> 8].scale;
   for (int s = 0; s < 2; ++s)
-    if (p.st[s].shkind == SH_GENERIC)
+    if (p.st[s].shkind == SH_GENERIC && !shift_decodable(p.st[s]))
       for (int i = threadIdx.x; i < 1024; i += blockDim.x) lut[s * 1024 + i] = p.st[s].shlut[i];
+  if (threadIdx.x < 2) plan[threadIdx.x].split = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < 64; i += blockDim.x)
+    if (shift_decodable(p.st[i >> 5])) build_shift_plan(p.st[i >> 5], plan[i >> 5], i & 31);
   __syncthreads();
   constexpr int M = kLargeM;
   constexpr int N = C * M;
   static_assert(M == 8192, "frame / column split by shifts");
+  const bool fast[2] = {shift_decodable(p.st[0]), shift_decodable(p.st[1])};
   const uint64_t total = nb * (uint64_t)M;
   for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (uint64_t)gridDim.x * blockDim.x) {
@@ -96,18 +130,45 @@ __global__ void decode_dif_kernel(const LargeParams p, uint64_t f0, uint64_t nb,
     const int m = (int)(idx & (uint64_t)(M - 1));
     const uint64_t f = f0 + fl;
     const FrameInfo& F = p.finfo[f];
-    const uint8_t* r1 = p.st[0].raw + f * p.st[0].bpf;
-    const uint8_t* r2 = p.st[1].raw + f * p.st[1].bpf;
     const bool odd = (f & 1u) != 0;
+    float xs[2][8];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const StationParams& q = p.st[s];
+      const uint8_t* fr = q.raw + f * q.bpf;
+      const int m0 = m - (s == 0 ? F.s1 : F.s2);
+      const float* lvs = lv + 256 * s;
+      if (fast[s]) {
+        const int b = q.bits, lg = b == 1 ? 5 : (b == 2 ? 4 : (b == 4 ? 3 : 2));
+        const uint32_t spw = 32u / (uint32_t)b, mask = (1u << b) - 1u;
+        const int c = m0 & (int)(spw - 1u);
+        const uint32_t p0 = plan[s].p0[c], p1 = plan[s].p1[c];
+        const bool split = (plan[s].split >> c) & 1u;
+        const int w0 = m0 >> lg;  // floor division
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(fr);
+        const bool neg = q.lsb && (m0 & 1);  // M is even: the same parity on every row
+#pragma unroll
+        for (int r = 0; r < C; ++r) {
+          const int mr = m0 + M * r;
+          float x = 0.f;
+          if ((unsigned)mr < (unsigned)N) {
+            const uint32_t w = words[w0 + r * (M >> lg)];
+            const uint32_t code = split ? (((w >> p0) & 1u) | (((w >> p1) & 1u) << 1))
+                                        : ((w >> p0) & mask);
+            x = lvs[code];
+            if (neg) x = -x;
+          }
+          xs[s][r] = x;
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < C; ++r)
+          xs[s][r] = sample_at(fr, q.bits, q.shkind, lut + 1024 * s, lvs, q.lsb, m0 + M * r, N);
+      }
+    }
     float2 v[16];
 #pragma unroll
-    for (int c = 0; c < C; ++c) {
-      const int n = m + M * c;
-      const float a = sample_at(r1, p.st[0].bits, p.st[0].shkind, lut, lv, p.st[0].lsb, n - F.s1, N);
-      const float b = sample_at(r2, p.st[1].bits, p.st[1].shkind, lut + 1024, lv + 256,
-                                p.st[1].lsb, n - F.s2, N);
-      v[c] = make_float2(a, odd ? -b : b);
-    }
+    for (int c = 0; c < C; ++c) v[c] = make_float2(xs[0][c], odd ? -xs[1][c] : xs[1][c]);
     if constexpr (C == 2) {
       dft2<0>(v);
     } else if constexpr (C == 4) {
@@ -213,6 +274,8 @@ __global__ void acc_global_kernel(const LargeParams p, const float2* __restrict_
   double a[4] = {0, 0, 0, 0};
   const uint64_t groups = gridDim.z;
   const uint64_t g0 = (blockIdx.z * nb) / groups, g1 = ((blockIdx.z + 1) * nb) / groups;
+  // unrolled: the frames' loads go out together (the loop is latency-bound)
+#pragma unroll 4
   for (uint64_t fl = g0; fl < g1; ++fl) {
     const float2* Zf = Y + fl * (uint64_t)N;
     const FrameInfo& F = p.finfo[f0 + fl];

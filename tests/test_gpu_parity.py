@@ -383,6 +383,13 @@ LARGE_CASES = [
     dict(fft=32768, band=(-64, 64, 16384, 0), grid=1, bits1=4, bits2=4),
     dict(fft=65536, band=(0, 0, 32768, 0), grid=0, bits1=1, bits2=2,
          products=oracle.PROD_ACF | oracle.PROD_ACF_OVERLAP_ONLY | oracle.PROD_XCF),
+    # the four-step decode's shift plans: shuffled 1- and 2-bit stations (bits
+    # kept together, reordered, split or swapped), and the generic 8/4-bit path
+    dict(fft=32768, band=(64, 0, 16320, 64), grid=0, shuffle="generic", lsb2=True),
+    dict(fft=32768, band=(0, 0, 16384, 0), grid=1, bits1=1, bits2=2, shuffle="pairswap",
+         lsb1=True),
+    dict(fft=16384, band=(5, 0, 8187, 5), grid=1, shuffle="sample2"),
+    dict(fft=65536, band=(-32, 32, 32768, 0), grid=0, bits1=8, bits2=4, shuffle="generic"),
 ]
 
 
