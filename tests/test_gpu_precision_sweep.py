@@ -1,4 +1,4 @@
-"""Precision sweep (BASELINE config 3 shapes): bit depths 1/2/4/8 x FFT
+"""Precision sweep: bit depths 1/2/4/8 x FFT
 1024/4096/16384/65536 at 512 Msps, correlated noise at rho = 0.01 plus a
 -30 dB tone at a seeded channel; the FP32 GPU path against the FP64 oracle,
 amplitude and phase error per bin.  Each case runs a bounded sample of the
