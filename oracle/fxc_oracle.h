@@ -126,6 +126,21 @@ void orc_normalize(uint32_t fft, uint64_t nf, double level_power, const double* 
 /* main.rs:378-387 */
 double orc_level_power(const double* levels, uint32_t n);
 
+/* Test data (synth.c, not a restatement): nsamp samples per station of
+ * quantised Gaussian noise (unit variance times `gain`, nearest of the
+ * nlevels = 2^bits levels) sharing a common component at correlation rho,
+ * station 2's copy `lag` samples late, plus tone_amp * cos(2 pi tone_cyc n +
+ * tone_phase) at both stations when tone_amp != 0, odd samples of an LSB station negated,
+ * packed LSB-first into little-endian words with word bit p moved to bit
+ * shuffle_out[p].  nsamp must fill whole words.  Returns 0, or -1 on bad
+ * arguments.  The output does not depend on nthreads. */
+int orc_synth_pack_pair(uint64_t seed, uint64_t nsamp, double rho, uint32_t lag,
+                        double tone_amp, double tone_cyc, double tone_phase, uint32_t bits,
+                        const double* levels, uint32_t nlevels, double gain,
+                        const uint8_t shuffle_out1[32], int32_t lsb1,
+                        const uint8_t shuffle_out2[32], int32_t lsb2, uint8_t* out1,
+                        uint8_t* out2, int32_t nthreads);
+
 #ifdef __cplusplus
 }
 #endif

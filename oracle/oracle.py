@@ -45,9 +45,9 @@ DEFAULT_SHUFFLE_EXT = list(range(31, -1, -1))
 
 def build(force: bool = False) -> Path:
     """Compile the C restatement into oracle/lib/libfxc_oracle.so."""
-    src = HERE / "fxc_oracle.c"
+    srcs = [HERE / "fxc_oracle.c", HERE / "synth.c"]
     if LIB_PATH.exists() and not force and LIB_PATH.stat().st_mtime >= max(
-        src.stat().st_mtime, (HERE / "fxc_oracle.h").stat().st_mtime
+        [x.stat().st_mtime for x in srcs] + [(HERE / "fxc_oracle.h").stat().st_mtime]
     ):
         return LIB_PATH
     LIB_DIR.mkdir(exist_ok=True)
@@ -55,7 +55,7 @@ def build(force: bool = False) -> Path:
     cmd = [
         "gcc", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fno-math-errno",
         "-fopenmp", "-fPIC", "-shared", "-std=c11", "-D_GNU_SOURCE",
-        "-o", str(tmp), str(src), "-lm",
+        "-o", str(tmp), *map(str, srcs), "-lm",
     ]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB_PATH)
@@ -138,6 +138,11 @@ def lib():
         L.orc_normalize.argtypes = [C.c_uint32, C.c_uint64, C.c_double, f64p, f64p, f32p]
         L.orc_level_power.argtypes = [f64p, C.c_uint32]
         L.orc_level_power.restype = C.c_double
+        L.orc_synth_pack_pair.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_uint32,
+                                          C.c_double, C.c_double, C.c_double,
+                                          C.c_uint32, f64p, C.c_uint32, C.c_double, u8p,
+                                          C.c_int32, u8p, C.c_int32, u8p, u8p, C.c_int32]
+        L.orc_synth_pack_pair.restype = C.c_int
         _lib = L
     return _lib
 
@@ -497,6 +502,36 @@ def fp64_sector_corr(scan: Scan, raw1, raw2, nf: int, first_frame: int = 0, chun
     return dict(acf11=acc11, acf22=acc22, xcf=acc12, failed=0)
 
 
+def fp64_sector_corr_parallel(scan: Scan, raw1, raw2, nf: int, first_frame: int = 0,
+                              workers: int = 0, pieces_per_worker: int = 4):
+    """fp64_sector_corr over contiguous frame ranges in worker processes,
+    summed in range order: the FP64 oracle for sectors of 1e9 samples.  The
+    pool uses the spawn start method, which is safe in a process that has
+    already initialised CUDA (a forked child of such a process can hang)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    workers = workers or os.cpu_count() or 1
+    npieces = max(1, min(nf, workers * pieces_per_worker))
+    bounds = [nf * k // npieces for k in range(npieces + 1)]
+    b1, b2 = scan.bpf(scan.bits1), scan.bpf(scan.bits2)
+    r1 = np.asarray(raw1, np.uint8)
+    r2 = np.asarray(raw2, np.uint8)
+    total = None
+    with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+        futs = [ex.submit(fp64_sector_corr, scan, r1[f0 * b1:f1 * b1], r2[f0 * b2:f1 * b2],
+                          f1 - f0, first_frame + f0)
+                for f0, f1 in zip(bounds[:-1], bounds[1:]) if f1 > f0]
+        for f in futs:
+            part = f.result()
+            if total is None:
+                total = part
+            else:
+                for k in ("acf11", "acf22", "xcf"):
+                    total[k] = total[k] + part[k]
+    return total
+
+
 def fp64_sector_phased(scan: Scan, raw1, raw2, nf: int, first_frame: int = 0, chunk: int = 256):
     """FP64 oracle for the phased power of one sector (main.rs:2222-2365),
     plus the float64 time series that the .raw output quantises."""
@@ -634,6 +669,37 @@ def encode_station(x: np.ndarray, bits: int, levels, shuffle, lsb: bool, gain=No
         y = y.copy()
         y[1::2] *= -1
     return pack_codes(quantise_codes(y, levels), bits, shuffle)
+
+
+def synth_packed_pair(n_samples: int, seed: int, bits: int, levels, shuffle1, lsb1: bool,
+                      shuffle2, lsb2: bool, rho: float = 0.05, lag: int = 7, gain=None,
+                      nthreads: int = 0, tone_bin=None, tone_db: float = -30.0, fft: int = 1024):
+    """Both stations' packed .raw bytes of seeded quantised Gaussian noise
+    (common component at rho, station 2 `lag` whole samples late; optionally
+    a tone at FFT bin `tone_bin` of an `fft`-point frame, `tone_db` below the
+    noise, at both stations, as synth_station_pair adds it), written by
+    the C generator in synth.c: fast enough for full-size sectors (1e9
+    samples per station in seconds), identical for any thread count.  The
+    shuffles are the stations' internal maps, applied inversely as the
+    encoder above does."""
+    g = level_gain(bits) if gain is None else gain
+    lv = np.ascontiguousarray(levels, np.float64)
+    s1 = np.ascontiguousarray(shuffle1, np.uint8)
+    s2 = np.ascontiguousarray(shuffle2, np.uint8)
+    nb = n_samples * bits // 8
+    o1, o2 = np.empty(nb, np.uint8), np.empty(nb, np.uint8)
+    nt = nthreads or os.cpu_count() or 1
+    amp = 0.0 if tone_bin is None else math.sqrt(2.0) * 10 ** (tone_db / 20.0)
+    cyc = 0.0 if tone_bin is None else tone_bin / fft
+    ph = 0.0 if tone_bin is None else float(np.random.Generator(np.random.PCG64(seed)).uniform(
+        0, 2 * np.pi))
+    rc = lib().orc_synth_pack_pair(seed, n_samples, rho, lag, amp, cyc, ph, bits,
+                                   _p(lv, C.c_double), lv.size,
+                                   g, _p(s1, C.c_uint8), int(lsb1), _p(s2, C.c_uint8), int(lsb2),
+                                   _p(o1, C.c_uint8), _p(o2, C.c_uint8), nt)
+    if rc != 0:
+        raise ValueError("orc_synth_pack_pair: bad arguments")
+    return o1, o2
 
 
 def random_shuffle(seed: int, avoid_special: bool = True):

@@ -208,3 +208,35 @@ def test_pure_delay_xcf_recovers_lag(oracle_lib):
     assert abs(slope2 * n / (2 * np.pi)) < 0.05
     f = oracle.fp64_sector_corr(scan2, r1, r2, nf)
     assert np.abs(np.angle(res2["xcf"][k] * np.conj(f["xcf"][k]))).max() < 1e-4
+
+
+def test_fp64_parallel_matches_serial(oracle_lib):
+    """The process-pool FP64 oracle used for 1e9-sample sectors sums the same
+    per-frame products as the serial one (to FP64 rounding)."""
+    from _cases import make_scan
+
+    scan = make_scan(fft=1024, fs=512e6, shuffle="generic", lsb1=True, band=(8, 0, 504, 8),
+                     delay=dict(net_d1_base=3.3e-7, total_rate1_base=2.1e-6, lo1_hz=8.4e9,
+                                lo2_hz=8.4e9))
+    nf = 300
+    r1, r2 = oracle_lib.synth_packed_pair(nf * 1024, 4, 2, scan.levels1, scan.shuffle1, True,
+                                          scan.shuffle2, False, rho=0.1, tone_bin=77, fft=1024)
+    a = oracle_lib.fp64_sector_corr(scan, r1, r2, nf, first_frame=9)
+    b = oracle_lib.fp64_sector_corr_parallel(scan, r1, r2, nf, first_frame=9, workers=2)
+    for k in ("acf11", "acf22", "xcf"):
+        assert np.allclose(a[k], b[k], rtol=1e-12, atol=1e-9 * np.abs(a[k]).max()), k
+
+
+def test_synth_packed_pair_is_thread_count_independent(oracle_lib):
+    lv = [-3.0, -1.0, 1.0, 3.0]
+    sh = oracle_lib.random_shuffle(8)
+    a = oracle_lib.synth_packed_pair(1 << 16, 11, 2, lv, sh, True, list(range(32)), False,
+                                     tone_bin=5, fft=256, nthreads=1)
+    b = oracle_lib.synth_packed_pair(1 << 16, 11, 2, lv, sh, True, list(range(32)), False,
+                                     tone_bin=5, fft=256, nthreads=3)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    # the common component: station 2 lags by 7 samples
+    x1 = oracle_lib.c_decode(a[0], 1 << 16, 2, sh, lv, True)
+    x2 = oracle_lib.c_decode(a[1], 1 << 16, 2, list(range(32)), lv, False)
+    c = [float(np.mean(x1[:len(x1) - L] * x2[L:])) for L in (6, 7, 8)]
+    assert c[1] > 3 * max(abs(c[0]), abs(c[2]))
