@@ -43,6 +43,7 @@ LEVELS = [-3.0, -1.0, 1.0, 3.0]
 OBS_MHZ = 8400.0
 ROT1_HZ, ROT2_HZ = 0.0, 16e6
 RHO = 0.05
+METRIC = "Gsample/s (2-bit, FFT 8192)"
 WORKLOAD = ("full-rate plain scan: 1024 Msps, 2-bit, FFT 8192, 10 s (10 sectors x 125000 frame "
             "pairs), generic shuffle, ant1 LSB / ant2 USB, 16 MHz band offset, ACFx2+XCF")
 
@@ -55,13 +56,18 @@ def shuffle_internal(seed: int):
             return p
 
 
-def scan_config(fxc):
+PROD_ACF, PROD_XCF = 1, 2  # product bits (same values in fxc and the oracle)
+
+
+def scan_fields(band_alignment):
     """Resolve the scan the way run_once does (src/main.rs:1186-1212,
-    1317-1328, 1618-1673) for the synthetic schedule above."""
+    1317-1328, 1618-1673) for the synthetic schedule above.  Returns the
+    fields shared by fxc.ScanConfig and oracle.Scan; `band_alignment` is
+    either's restatement of compute_band_alignment (src/main.rs:360-372)."""
     bw = FS / 2e6
     c1 = OBS_MHZ + ROT1_HZ / 1e6 + 0.5 * bw
     c2 = OBS_MHZ + ROT2_HZ / 1e6 + 0.5 * bw
-    band = fxc.band_alignment(N, FS, c1, c2, bw, bw)
+    band = band_alignment(N, FS, c1, c2, bw, bw)
     grid = 0 if abs(ROT1_HZ) <= abs(ROT2_HZ) else 1
     df = FS / N
     rot_residual = (ROT1_HZ - ROT2_HZ) - band[0] * df
@@ -79,10 +85,32 @@ def scan_config(fxc):
     delay = dict(time_offset_s=0.0, delay_user_samples=user, extra_delay_rate_sps=extra_rate,
                  d_seek=d_seek, lo1_hz=(OBS_MHZ + ROT1_HZ / 1e6) * 1e6,
                  lo2_hz=(OBS_MHZ + ROT2_HZ / 1e6) * 1e6)
-    return fxc.ScanConfig(fft=N, fs=FS, bits1=BITS, bits2=BITS, levels1=LEVELS, levels2=LEVELS,
-                          shuffle1=shuffle_internal(101), shuffle2=shuffle_internal(102),
-                          lsb1=True, lsb2=False, band=tuple(band), grid=grid,
-                          products=fxc.PROD_ACF | fxc.PROD_XCF, delay=delay, geom_table=table)
+    return dict(fft=N, fs=FS, bits1=BITS, bits2=BITS, levels1=LEVELS, levels2=LEVELS,
+                shuffle1=shuffle_internal(101), shuffle2=shuffle_internal(102),
+                lsb1=True, lsb2=False, band=tuple(band), grid=grid,
+                products=PROD_ACF | PROD_XCF, delay=delay, geom_table=table)
+
+
+def scan_config(fxc):
+    return fxc.ScanConfig(**scan_fields(fxc.band_alignment))
+
+
+def import_oracle():
+    """The checker and CPU restatement under oracle/ (the bench's CPU legs
+    only)."""
+    p = str(ROOT / "oracle")
+    if p not in sys.path:
+        sys.path.insert(0, p)
+    import oracle
+
+    return oracle
+
+
+def oracle_scan():
+    """The same scan for the CPU restatement, resolved with the oracle's own
+    band alignment (no product code involved)."""
+    oracle = import_oracle()
+    return oracle.Scan(**scan_fields(oracle.c_band_alignment))
 
 
 def gen_station_pair_gpu(torch, nsamp, seed, cfg, lag=7):
@@ -203,45 +231,6 @@ def flops_per_station_sample(n):
 
 # -------------------------------------------------------------- CPU legs
 
-def cpu_sample(cfg_o, get_sector, nsec, nfs, target_s=10.0, threads=None):
-    """Times the oracle port (OpenMP, all host threads unless `threads`)
-    sector by sector over the scan until about target_s seconds of CPU work;
-    returns (Gsample/s, frames, threads, seconds)."""
-    import oracle
-
-    oracle.build()
-    threads = threads or os.cpu_count() or 1
-    frames, spent = 0, 0.0
-    for i in range(nsec):
-        r1, r2 = get_sector(i)
-        t0 = time.perf_counter()
-        oracle.c_sector_corr(cfg_o, r1, r2, nfs, i * nfs, threads)
-        spent += time.perf_counter() - t0
-        frames += nfs
-        if spent >= target_s:
-            break
-    return 2 * frames * N / spent / 1e9, frames, threads, spent
-
-
-def to_oracle_scan(cfg):
-    import dataclasses
-
-    import oracle
-
-    d = dataclasses.asdict(cfg)
-    d["geom_table"] = cfg.geom_table
-    return oracle.Scan(**d)
-
-
-def cpu_inputs_numpy(cfg, nf):
-    import oracle
-
-    x1, x2 = oracle.synth_station_pair(nf * N, 7, rho=RHO, delay_samples=7.0)
-    r1 = oracle.encode_station(x1, BITS, LEVELS, cfg.shuffle1, cfg.lsb1)
-    r2 = oracle.encode_station(x2, BITS, LEVELS, cfg.shuffle2, cfg.lsb2)
-    return r1, r2
-
-
 def replica_throughput(dist, samples, ms, device):
     """Whole-job throughput of independent replicas (the path shards by scan
     or sector with no data-path collective): every rank's samples over the
@@ -259,54 +248,165 @@ def replica_throughput(dist, samples, ms, device):
     return samples / (ms * 1e-3) / 1e9, ms
 
 
-def run_reference(args, rank, world):
-    """--impl reference: the CPU restatement of the reference path on this
-    box's host cores, K bounded-sample steps."""
-    if rank != 0:
-        return 0
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import fxc
-
-    cfg = scan_config(fxc)
-    cfg_o = to_oracle_scan(cfg)
-    import oracle
-
+def reference_line(steps, warmup, world, sectors=SECTORS, nfs=NF_SECTOR, threads=None):
+    """The reference arm: the CPU restatement of the reference's rayon path
+    (oracle/fxc_oracle.c, OpenMP over all host threads) on the full workload,
+    every step correlating all `sectors` x `nfs` frame pairs of the scan.
+    Imports the oracle only, never the product package.  Each sector
+    correlates the same seeded 1-s input bytes (generated once by the
+    oracle's C generator) with its own delay model (frames i*nfs onwards);
+    the restatement's cost does not depend on the sample values."""
+    oracle = import_oracle()
     oracle.build()
-    threads = os.cpu_count() or 1
-    probe_nf = 512
-    r1, r2 = cpu_inputs_numpy(cfg, probe_nf)
+    scan = oracle_scan()
+    threads = threads or os.cpu_count() or 1
+    r1, r2 = oracle.synth_packed_pair(nfs * N, 1000, BITS, LEVELS, scan.shuffle1, scan.lsb1,
+                                      scan.shuffle2, scan.lsb2, rho=RHO, lag=7, nthreads=threads)
+
+    def step():
+        for i in range(sectors):
+            out = oracle.c_sector_corr(scan, r1, r2, nfs, i * nfs, threads)
+            if out["failed"]:
+                raise RuntimeError("restatement reported failed frames")
+
+    for _ in range(warmup):
+        step()
     t0 = time.perf_counter()
-    oracle.c_sector_corr(cfg_o, r1, r2, probe_nf, 0, threads)
-    per_frame = (time.perf_counter() - t0) / probe_nf
-    # each step is a bounded sample sized so that warmup + steps take ~2 minutes
-    budget = 120.0 / max(1, args.steps + args.warmup)
-    nf = int(max(256, min(NF_SECTOR, budget / max(per_frame, 1e-7))))
-    r1, r2 = cpu_inputs_numpy(cfg, nf)
-    for _ in range(args.warmup):
-        oracle.c_sector_corr(cfg_o, r1, r2, nf, 0, threads)
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        oracle.c_sector_corr(cfg_o, r1, r2, nf, k * nf, threads)
-    dt = (time.perf_counter() - t0) / args.steps
-    value = 2 * nf * N / dt / 1e9
-    sample = f"{nf} frame pairs of the workload per step (of 1250000 per 10-s scan)"
-    line = {
-        "impl": "reference", "metric": "Gsample/s (2-bit, FFT 8192)", "value": value,
-        "unit": "Gsample/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+    for _ in range(steps):
+        step()
+    dt = (time.perf_counter() - t0) / steps
+    value = 2 * sectors * nfs * N / dt / 1e9
+    full = sectors == SECTORS and nfs == NF_SECTOR
+    sample = (f"the whole scan per step: {sectors} sectors x {nfs} frame pairs (each sector the "
+              f"same seeded input bytes with its own delay model)")
+    return {
+        "impl": "reference", "metric": METRIC, "value": value,
+        "unit": "Gsample/s", "n_gpus": world, "steps": steps, "warmup": warmup,
         "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, quantised Gaussian)",
-        "config": {"workload": WORKLOAD, "fft": N, "fs_hz": FS, "bits": BITS,
-                   "sample": sample},
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded quantised Gaussian, "
+        "rho=0.05, oracle C generator)",
+        "config": {"workload": WORKLOAD if full else
+                   f"reduced case ({sectors} x {nfs} frame pairs) of: {WORKLOAD}",
+                   "fft": N, "fs_hz": FS, "bits": BITS, "scan_s": SCAN_S,
+                   "sectors": sectors, "frames_per_sector": nfs},
         "cpu_baseline": {"value": value, "unit": "Gsample/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "Gsample/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+
+
+def run_reference(args, rank, world):
+    """--impl reference: rank 0 times the CPU restatement on this box's host
+    cores; the other ranks exit without work."""
+    if rank != 0:
+        return 0
+    line = reference_line(args.steps, args.warmup, world, args.sectors, args.frames_per_sector)
     print(json.dumps(line), flush=True)
     return 0
 
 
 # ------------------------------------------------------------------ main
+
+def cpu_parity_leg(torch, scan, sec1, sec2, accs, nfs, slice_frames=1000):
+    """The CPU restatement of the reference path (oracle/fxc_oracle.c,
+    OpenMP over all host threads) on every sector of the measured scan, the
+    same bytes the GPU correlated: its time is the cpu_baseline, and its
+    accumulators check the GPU's (accs[i], left by the timed steps) at full
+    size.  On the first `slice_frames` frames of each sector the GPU, the
+    restatement and the FP64 oracle are compared as well, stating the
+    restatement's own drift from FP64 beside the GPU's error."""
+    oracle = import_oracle()
+    sys.path.insert(0, str(ROOT / "tests"))
+    from _cases import spectral_errors, xcf_drift_bound, xcf_floor
+
+    oracle.build()
+    cfg_o = oracle_scan()
+    threads = os.cpu_count() or 1
+    h = cfg_o.h
+    sb, a1s, a1e, a2s = cfg_o.band
+    bound = xcf_drift_bound(a1e - a1s)
+    worst = {}
+
+    def upd(key, errs, names):
+        d = worst.setdefault(key, {})
+        for nm, v in zip(names, errs):
+            d[nm] = max(d.get(nm, 0.0), float(v))
+
+    def split(a):
+        return dict(acf11=a[:h], acf22=a[h:2 * h], xcf=a[2 * h:4 * h].view(np.complex128))
+
+    names = ("rel_amp", "phase_rad", "abs_over_peak")
+    spent, frames = 0.0, 0
+    acc_s = torch.empty(5 * h, dtype=torch.float64, device="cuda")
+    bpf = cfg_o.bpf(BITS)
+    for i in range(len(sec1)):
+        r1, r2 = sec1[i].cpu().numpy(), sec2[i].cpu().numpy()
+        t0 = time.perf_counter()
+        c = oracle.c_sector_corr(cfg_o, r1, r2, nfs, i * nfs, threads)
+        spent += time.perf_counter() - t0
+        frames += nfs
+        g = split(accs[i].cpu().numpy())
+        for k in ("acf11", "acf22"):
+            upd("gpu_vs_port_" + k, spectral_errors(g[k], c[k]), names)
+        upd("gpu_vs_port_xcf", spectral_errors(g["xcf"], c["xcf"], xcf_floor(c, nfs)), names)
+        # slice against FP64
+        m = min(slice_frames, nfs)
+        scan.run_device(sec1[i][:m * bpf], sec2[i][:m * bpf], m, i * nfs, acc_s)
+        gs = split(acc_s.cpu().numpy())
+        f = oracle.fp64_sector_corr(cfg_o, r1[:m * bpf], r2[:m * bpf], m, i * nfs)
+        cs = oracle.c_sector_corr(cfg_o, r1[:m * bpf], r2[:m * bpf], m, i * nfs, threads)
+        fl = xcf_floor(f, m)
+        for who, x in (("gpu", gs), ("port", cs)):
+            for k in ("acf11", "acf22"):
+                upd(f"{who}_vs_fp64_{k}", spectral_errors(x[k], f[k]), names)
+            upd(f"{who}_vs_fp64_xcf", spectral_errors(x["xcf"], f["xcf"], fl), names)
+    scan.check()
+    tol_amp, tol_ph = 1e-5, 1e-4
+    ok_fp64 = all(worst[f"gpu_vs_fp64_{k}"]["rel_amp"] <= tol_amp and
+                  worst[f"gpu_vs_fp64_{k}"]["phase_rad"] <= tol_ph and
+                  worst[f"gpu_vs_fp64_{k}"]["abs_over_peak"] <= tol_amp
+                  for k in ("acf11", "acf22", "xcf"))
+    ok_port = all(worst[f"gpu_vs_port_{k}"]["rel_amp"] <= tol_amp for k in ("acf11", "acf22")) \
+        and worst["gpu_vs_port_xcf"]["rel_amp"] <= bound["rel_amp"] \
+        and worst["gpu_vs_port_xcf"]["phase_rad"] <= bound["phase_rad"]
+    parity = {
+        "full_size": {"against": "C restatement of the reference path, same bytes",
+                      "sectors": len(sec1), "frame_pairs_compared": frames,
+                      **{k[len("gpu_vs_port_"):]: v for k, v in worst.items()
+                         if k.startswith("gpu_vs_port_")},
+                      "tolerance": {"acf_rel_amp": tol_amp, "xcf": bound,
+                                    "xcf_note": "the restatement's f32 phase-ramp recurrence "
+                                                "drift (ov * 2^-23) plus the GPU's FP64 "
+                                                "tolerance"},
+                      "pass": bool(ok_port)},
+        "fp64_slices": {"frame_pairs_compared": len(sec1) * min(slice_frames, nfs),
+                        "slices": f"first {min(slice_frames, nfs)} frame pairs of each sector",
+                        "gpu": {k[len("gpu_vs_fp64_"):]: v for k, v in worst.items()
+                                if k.startswith("gpu_vs_fp64_")},
+                        "reference_restatement": {k[len("port_vs_fp64_"):]: v
+                                                  for k, v in worst.items()
+                                                  if k.startswith("port_vs_fp64_")},
+                        "tolerance": {"rel_amp": tol_amp, "phase_rad": tol_ph},
+                        "pass": bool(ok_fp64)},
+        "metrics": "per-bin relative amplitude against max(|ref|, floor), phase on bins at or "
+                   "above the floor, largest complex error over the peak (tests/_cases.py)",
+    }
+    cpu = {"value": 2 * frames * N / spent / 1e9, "unit": "Gsample/s", "cores": threads,
+           "kind": "port",
+           "sample": f"the whole scan, {len(sec1)} sectors x {nfs} frame pairs ({spent:.1f} s of "
+                     f"CPU work, C restatement, OpenMP over all host threads)"}
+    # the reference's own default pool: logical cores - 2 (src/main.rs:920-924)
+    thr_d = max(1, threads - 2)
+    r1, r2 = sec1[0].cpu().numpy(), sec2[0].cpu().numpy()
+    t0 = time.perf_counter()
+    oracle.c_sector_corr(cfg_o, r1, r2, nfs, 0, thr_d)
+    dt = time.perf_counter() - t0
+    cpu["at_reference_default_threads"] = {
+        "value": 2 * nfs * N / dt / 1e9, "threads": thr_d,
+        "sample": f"sector 0, {nfs} frame pairs ({dt:.1f} s of CPU work)"}
+    return cpu, parity
+
 
 def serve_jobs(n_jobs, load, seed=5150):
     """Long jobs: seeded Poisson stream of 0.1-5 s chunks at 256-1024 Msps,
@@ -723,27 +823,13 @@ def main():
                 "algorithmic_bytes_per_launch": bytes_launch},
     }
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        sys.path.insert(0, str(ROOT / "oracle"))
-        cfg_o = to_oracle_scan(cfg)
-        v, nf_cpu, thr, dt = cpu_sample(
-            cfg_o, lambda i: (sec1[i].cpu().numpy(), sec2[i].cpu().numpy()), SECTORS_, NFS)
-        cpu = {"value": v, "unit": "Gsample/s", "cores": thr, "kind": "port",
-               "sample": f"first {nf_cpu} frame pairs of the scan ({dt:.1f} s of CPU work, "
-                         f"C restatement, OpenMP over all host threads)"}
-        # the reference's own default pool: logical cores - 2 (src/main.rs:920-924)
-        thr_d = max(1, (os.cpu_count() or 1) - 2)
-        v_d, nf_d, _, dt_d = cpu_sample(
-            cfg_o, lambda i: (sec1[i].cpu().numpy(), sec2[i].cpu().numpy()), SECTORS_, NFS,
-            target_s=3.0, threads=thr_d)
-        cpu["at_reference_default_threads"] = {
-            "value": v_d, "threads": thr_d,
-            "sample": f"first {nf_d} frame pairs ({dt_d:.1f} s of CPU work)"}
+        cpu, parity = cpu_parity_leg(torch, scan, sec1, sec2, accs, NFS)
 
     if rank == 0:
         line = {
-            "metric": "Gsample/s (2-bit, FFT 8192)", "value": value, "unit": "Gsample/s",
+            "metric": METRIC, "value": value, "unit": "Gsample/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded quantised Gaussian, rho=0.05, generated on device)",
@@ -755,6 +841,7 @@ def main():
                        "l2": "inputs larger than L2 (512 MB per sector, 5.12 GB per step)"},
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "parity": parity,
             "e2e": e2e,
             "batched": batched,
             "serving": serve,

@@ -129,3 +129,15 @@ def assert_sector_close(got, ref, scan, what, nf=None, ref_acf=None):
         fl = xcf_floor(ref_acf if ref_acf is not None else ref, nf) if nf else None
         out["xcf"] = assert_spectra_close(got["xcf"], ref["xcf"], what + " xcf", floor=fl)
     return out
+
+
+def xcf_drift_bound(ov):
+    """How far the reference's XCF may sit from the exact product: its phase
+    ramp is the f32 recurrence ph *= step over the ov overlap bins
+    (src/main.rs:2513-2527, src/utils.rs:115-117), so after k bins the ramp's
+    relative magnitude and its angle each carry up to k roundings of about
+    2^-24, plus the rounding of step itself: at most ov * 2^-23 in both.  The
+    GPU evaluates the ramp per bin and tracks FP64 within REL_AMP_TOL /
+    PHASE_TOL, so the GPU against the f32 restatement is bounded by the sum."""
+    d = ov * 2.0 ** -23
+    return {"rel_amp": REL_AMP_TOL + d, "phase_rad": PHASE_TOL + d}
