@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -23,6 +24,9 @@ using namespace fxc;
 namespace {
 
 thread_local std::string g_err;
+
+// failure injection (fxc_debug_inject_wait_timeout)
+std::atomic<uint32_t> g_dbg_polls{0}, g_dbg_flags{0};
 
 fxc_status fail(fxc_status s, const char* fmt, ...) {
   char buf[512];
@@ -231,6 +235,7 @@ CorrParams corr_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2, 
   p.partials = s->d_partials;
   p.finfo = s->d_finfo;
   p.err = s->d_err;
+  internal_debug_settings(&p.wait_polls, &p.debug_flags);
   return p;
 }
 
@@ -945,8 +950,12 @@ fxc_status fxc_scan_check(fxc_scan* s) {
   uint32_t err = 0;
   CK(cudaMemcpy(&err, s->d_err, 4, cudaMemcpyDeviceToHost));
   CK(cudaMemset(s->d_err, 0, 4));
-  if (err & ERR_WAIT_TIMEOUT) return fail(FXC_ETIMEDOUT, "a bounded device-side wait gave up");
-  if (err) return fail(FXC_EDEVICE, "kernel error word 0x%x", err);
+  return internal_device_error(err);
+}
+
+fxc_status fxc_debug_inject_wait_timeout(uint32_t wait_polls, int32_t withhold_copies) {
+  g_dbg_polls.store(wait_polls);
+  g_dbg_flags.store(withhold_copies ? DBG_WITHHOLD_COPIES : 0u);
   return FXC_OK;
 }
 
@@ -1005,6 +1014,12 @@ fxc_status fxc_decode_device(fxc_scan* s, const uint8_t* d_raw1, const uint8_t* 
   CorrParams p = corr_params(s, d_raw1, d_raw2, nf, first_frame);
   p.out_a = d_x1;
   p.out_b = d_x2;
+  if (s->n == 8192) {
+    // the FFT-8192 correlation kernel's decode path (fold_inputs)
+    const int grid = (int)std::min<uint64_t>(nf, (uint64_t)s->eng->sm_count * 4);
+    CK(launch_fold_decode(p, grid, (cudaStream_t)stream));
+    return FXC_OK;
+  }
   CK(launch_corr(s->n, MODE_DECODE, p, corr_grid(s, nf), (cudaStream_t)stream));
   return FXC_OK;
 }
@@ -1098,8 +1113,7 @@ fxc_status fxc_sector_wait(fxc_scan* s, uint64_t sector_id, int32_t timeout_ms,
   }
   if (err) {
     cudaMemsetAsync(s->d_err, 0, 4, s->stream);
-    if (err & ERR_WAIT_TIMEOUT) return fail(FXC_ETIMEDOUT, "a bounded device-side wait gave up");
-    return fail(FXC_EDEVICE, "kernel error word 0x%x", err);
+    return internal_device_error(err);
   }
   return FXC_OK;
 }
@@ -1115,6 +1129,28 @@ fxc_status fxc_host_alloc(uint64_t bytes, void** out) {
 
 fxc_status fxc_host_free(void* p) {
   if (p) CK(cudaFreeHost(p));
+  return FXC_OK;
+}
+
+fxc_status fxc_host_register(void* p, uint64_t bytes) {
+  if (!p || !bytes) return fail(FXC_EINVAL, "fxc_host_register: NULL or empty buffer");
+  const cudaError_t e = cudaHostRegister(p, bytes, cudaHostRegisterDefault);
+  if (e == cudaErrorHostMemoryAlreadyRegistered) {
+    cudaGetLastError();  // not sticky; the buffer is page-locked already
+    return FXC_OK;
+  }
+  if (e != cudaSuccess) return fail(FXC_ECUDA, "cudaHostRegister: %s", cudaGetErrorString(e));
+  return FXC_OK;
+}
+
+fxc_status fxc_host_unregister(void* p) {
+  if (!p) return fail(FXC_EINVAL, "fxc_host_unregister: NULL buffer");
+  const cudaError_t e = cudaHostUnregister(p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(e == cudaErrorHostMemoryNotRegistered ? FXC_EINVAL : FXC_ECUDA,
+                "cudaHostUnregister: %s", cudaGetErrorString(e));
+  }
   return FXC_OK;
 }
 
@@ -1193,6 +1229,17 @@ fxc_status fxc_normalize(uint32_t fft, uint64_t nf, double level_power, const do
 namespace fxc {
 
 fxc_status internal_fail(fxc_status s, const char* msg) { return fail(s, "%s", msg); }
+
+void internal_debug_settings(uint32_t* wait_polls, uint32_t* debug_flags) {
+  *wait_polls = g_dbg_polls.load();
+  *debug_flags = g_dbg_flags.load();
+}
+
+fxc_status internal_device_error(uint32_t err) {
+  if (err & ERR_WAIT_TIMEOUT) return fail(FXC_ETIMEDOUT, "a bounded device-side wait gave up");
+  if (err) return fail(FXC_EDEVICE, "kernel error word 0x%x", err);
+  return FXC_OK;
+}
 
 int engine_sm_count(const fxc_engine* e) { return e->sm_count; }
 int engine_device(const fxc_engine* e) { return e->device; }

@@ -162,6 +162,53 @@ __device__ __forceinline__ void fold_station(int bits, bool split, const uint32_
 }
 
 
+// The scan's decode tables in shared memory (primary station first): level
+// tables with their negated copies, the rotate amounts of every sample slot,
+// and the byte LUTs of 4- and 8-bit generic shuffles.  Needs a barrier before
+// use.
+__device__ __forceinline__ void fold_build_tables(const StationParams& sp, const StationParams& ss,
+                                                  bool preP, bool preS, uint8_t* smem, int tid) {
+  float* lv = reinterpret_cast<float*>(smem);
+  uint32_t* pos = reinterpret_cast<uint32_t*>(smem + kOffPos);
+  uint32_t* lut = reinterpret_cast<uint32_t*>(smem + kOffLut);
+  for (int i = tid; i < 1024; i += kT) {
+    // per station: 2^b levels, then their negations (the two sign groups of a
+    // warp's table loads fall in different banks)
+    const StationParams& q = (i < 512) ? sp : ss;
+    const int n = 1 << q.bits, c2 = i & 511;
+    const float x = c2 < 2 * n ? q.levels[c2 & (n - 1)] * q.scale : 0.0f;
+    lv[i] = c2 >= n ? -x : x;
+  }
+  for (int i = tid; i < 64; i += kT) {
+    // rotate amounts of sample slot c: bit j of the sample is word bit p_j
+    const int k = i >> 5, cc = i & 31;
+    const StationParams& q = k ? ss : sp;
+    const int b = q.bits;
+    const bool natural = (k ? preS : preP) || q.shkind == SH_IDENTITY;
+    uint32_t r = 0;
+    if (cc * b < 32) {
+      const int p0 = natural ? cc * b : q.perm[cc * b];
+      const int p1 = b >= 2 ? (natural ? cc * b + 1 : q.perm[cc * b + 1]) : 0;
+      r = (uint32_t)((p0 - 2) & 31) | ((uint32_t)((p1 - 3) & 31) << 8);
+    }
+    pos[i] = r;
+  }
+  for (int k = 0; k < 2; ++k) {
+    const StationParams& q = k ? ss : sp;
+    if ((k ? preS : preP) && q.shkind == SH_GENERIC)
+      for (int i = tid; i < 1024; i += kT) lut[k * 1024 + i] = q.shlut[i];
+  }
+}
+
+// A 2-bit shuffle keeps every sample's two bits adjacent and in order, or it
+// splits them (two rotates per sample).
+__device__ __forceinline__ bool fold_split2(const StationParams& q) {
+  if (q.bits != 2 || q.shkind == SH_IDENTITY) return false;
+  for (int cc = 0; cc < 16; ++cc)
+    if (q.perm[2 * cc + 1] != q.perm[2 * cc] + 1 || (q.perm[2 * cc] & 1)) return true;
+  return false;
+}
+
 // Per-CTA state of the fold kernels that does not depend on the scan: the
 // twiddle power chains, the two-row DIF twiddle bases, and the number of
 // staging iterations consumed so far (it sets the mbarrier slot and phase, so
@@ -171,6 +218,7 @@ struct FoldCta {
   Twiddles<kN> tw;
   float2 dtw0, dtw1, wb1;
   uint32_t seq;
+  uint32_t polls;  // bounded-wait limit of the last span (the drain uses it)
 };
 
 template <int ROWS>
@@ -200,14 +248,16 @@ __device__ __forceinline__ void fold_cta_init(uint8_t* smem, FoldCta<ROWS>& c) {
     c.wb1 = make_float2((float)cs, (float)sn);
   }
   c.seq = 0;
+  c.polls = kWaitPolls;
 }
 
 // Never leave a bulk copy in flight into a finished CTA's shared memory.
-__device__ __forceinline__ void fold_cta_drain(uint8_t* smem) {
+template <int ROWS>
+__device__ __forceinline__ void fold_cta_drain(uint8_t* smem, const FoldCta<ROWS>& c) {
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
   const int* flag = reinterpret_cast<const int*>(smem + kOffFlag);
   if (threadIdx.x == 0 && *flag) {
-    for (int s = 0; s < kStages; ++s) mbar_wait(&bars[s], 0, kWaitPolls);
+    for (int s = 0; s < kStages; ++s) mbar_wait(&bars[s], 0, c.polls);
   }
 }
 
@@ -250,12 +300,16 @@ __device__ __forceinline__ bool fold_span(const CorrParams& p, int row, uint64_t
   const uint8_t* rawP = sp.raw;
   const uint8_t* rawS = ss.raw;
   const FrameInfo* gfi = p.finfo;
+  const uint32_t polls = p.wait_polls ? p.wait_polls : kWaitPolls;
+  const bool withhold = (p.debug_flags & DBG_WITHHOLD_COPIES) != 0;
+  c.polls = polls;
 
   // slot: [FrameInfo][primary frame][secondary frame]
   auto issue = [&](uint64_t it) {
     const int slot = (int)((seq0 + (uint32_t)(it - it0)) % kStages);
     uint8_t* dst = stage + slot * L.stage_stride;
     mbar_expect_tx(&bars[slot], kFiBytes + bpfP + bpfS);
+    if (withhold) return;  // failure injection: the wait below runs out
     bulk_g2s(dst, gfi + it, kFiBytes, &bars[slot]);
     bulk_g2s(dst + kFiBytes, rawP + it * bpfP, bpfP, &bars[slot]);
     bulk_g2s(dst + kFiBytes + bpfP, rawS + it * bpfS, bpfS, &bars[slot]);
@@ -269,41 +323,8 @@ __device__ __forceinline__ bool fold_span(const CorrParams& p, int row, uint64_t
     for (uint64_t it = it0; it < it1 && it < it0 + kStages; ++it) issue(it);
   }
   // ---- constant tables of this scan
-  for (int i = tid; i < 1024; i += kT) {
-    // per station: 2^b levels, then their negations (the two sign groups of a
-    // warp's table loads fall in different banks)
-    const StationParams& q = (i < 512) ? sp : ss;
-    const int n = 1 << q.bits, c2 = i & 511;
-    const float x = c2 < 2 * n ? q.levels[c2 & (n - 1)] * q.scale : 0.0f;
-    lv[i] = c2 >= n ? -x : x;
-  }
-  for (int i = tid; i < 64; i += kT) {
-    // rotate amounts of sample slot c: bit j of the sample is word bit p_j
-    const int k = i >> 5, cc = i & 31;
-    const StationParams& q = k ? ss : sp;
-    const int b = q.bits;
-    const bool natural = (k ? preS : preP) || q.shkind == SH_IDENTITY;
-    uint32_t r = 0;
-    if (cc * b < 32) {
-      const int p0 = natural ? cc * b : q.perm[cc * b];
-      const int p1 = b >= 2 ? (natural ? cc * b + 1 : q.perm[cc * b + 1]) : 0;
-      r = (uint32_t)((p0 - 2) & 31) | ((uint32_t)((p1 - 3) & 31) << 8);
-    }
-    pos[i] = r;
-  }
-  for (int k = 0; k < 2; ++k) {
-    const StationParams& q = k ? ss : sp;
-    if ((k ? preS : preP) && q.shkind == SH_GENERIC)
-      for (int i = tid; i < 1024; i += kT) lut[k * 1024 + i] = q.shlut[i];
-  }
-  // a 2-bit shuffle keeps every sample's two bits adjacent and in order, or not
-  auto split2 = [](const StationParams& q) {
-    if (q.bits != 2 || q.shkind == SH_IDENTITY) return false;
-    for (int cc = 0; cc < 16; ++cc)
-      if (q.perm[2 * cc + 1] != q.perm[2 * cc] + 1 || (q.perm[2 * cc] & 1)) return true;
-    return false;
-  };
-  const bool splitP = split2(sp), splitS = split2(ss);
+  fold_build_tables(sp, ss, preP, preS, smem, tid);
+  const bool splitP = fold_split2(sp), splitS = fold_split2(ss);
   const float2 dtw0 = c.dtw0, dtw1 = c.dtw1, wb1 = c.wb1;
   __syncthreads();
 
@@ -357,7 +378,7 @@ __device__ __forceinline__ bool fold_span(const CorrParams& p, int row, uint64_t
     const int slot = (int)(q_it % kStages);
     const uint32_t parity = (q_it / kStages) & 1u;
     const int fb = (int)(q_it & 1u);
-    if (!mbar_wait(&bars[slot], parity, kWaitPolls)) {
+    if (!mbar_wait(&bars[slot], parity, polls)) {
       atomicOr(flag, 1);
       atomicOr(err, ERR_WAIT_TIMEOUT);
     }
@@ -411,8 +432,10 @@ __device__ __forceinline__ bool fold_span(const CorrParams& p, int row, uint64_t
     }
     const float2* Y = fft_rest<kN, true>(bufA, bufB, tid, tw);
     // fft_rest opened with a barrier after the first pass: the staging slot
-    // is consumed, refill it with iteration it + kStages
-    if (tid == 0 && it + kStages < it1) {
+    // is consumed, refill it with iteration it + kStages.  Not after a wait
+    // gave up (every thread's timeout was flagged before that barrier): the
+    // slot's phase never completed, and the CTA stops below.
+    if (tid == 0 && it + kStages < it1 && !*flag) {
       fence_proxy_async();
       issue(it + kStages);
     }
@@ -545,7 +568,7 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_kernel(const CorrParams p, in
   const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
   const uint64_t it1 = ((blockIdx.x + 1) * iters) / gridDim.x;
   fold_span<ROWS>(p, row, it0, it1, p.partials + (size_t)blockIdx.x * 4 * HF, smem, L, c);
-  fold_cta_drain(smem);
+  fold_cta_drain(smem, c);
 }
 
 // Batched: a persistent grid takes the items of batch group `grp` by ticket;
@@ -572,7 +595,69 @@ __global__ void __launch_bounds__(kT, 1) corr_fold_batch_kernel(const BatchArgs 
                          c))
       break;
   }
-  fold_cta_drain(smem);
+  fold_cta_drain(smem, c);
+}
+
+// The decode + integer shift of the FFT-8192 correlation kernel on its own
+// (the stage entry point fxc_decode_device): every frame's words go through
+// the same tables and fold_inputs path as in fold_span, and the 16 inputs a
+// thread would feed its first radix-16 pass, x[t + 512 r - shift], are
+// written out (level scale undone exactly) instead of transformed.
+__global__ void __launch_bounds__(kT) fold_decode_kernel(const CorrParams p) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const int tid = threadIdx.x;
+  const bool g0 = p.grid == 0;
+  const StationParams& sp = p.st[g0 ? 0 : 1];
+  const StationParams& ss = p.st[g0 ? 1 : 0];
+  const bool preP = sp.bits > 2 && sp.shkind != SH_IDENTITY;
+  const bool preS = ss.bits > 2 && ss.shkind != SH_IDENTITY;
+  uint32_t* pos = reinterpret_cast<uint32_t*>(smem + kOffPos);
+  uint32_t* lut = reinterpret_cast<uint32_t*>(smem + kOffLut);
+  uint32_t* wP = reinterpret_cast<uint32_t*>(smem + kOffA);
+  uint32_t* wS = wP + sp.bpf / 4;
+  fold_build_tables(sp, ss, preP, preS, smem, tid);
+  const bool splitP = fold_split2(sp), splitS = fold_split2(ss);
+  const int lsbP = sp.lsb ? 1 : 0, lsbS = ss.lsb ? 1 : 0;
+  const int bitsP = sp.bits, bitsS = ss.bits;
+  float* outP = g0 ? p.out_a : p.out_b;
+  float* outS = g0 ? p.out_b : p.out_a;
+  const float uP = 1.0f / sp.scale, uS = 1.0f / ss.scale;  // powers of two: exact
+  for (uint64_t f = blockIdx.x; f < p.nf; f += gridDim.x) {
+    __syncthreads();  // tables built / previous frame's words consumed
+    const uint4* gP = reinterpret_cast<const uint4*>(sp.raw + f * sp.bpf);
+    const uint4* gS = reinterpret_cast<const uint4*>(ss.raw + f * ss.bpf);
+    for (uint32_t i = tid; i < sp.bpf / 16; i += kT) reinterpret_cast<uint4*>(wP)[i] = gP[i];
+    for (uint32_t i = tid; i < ss.bpf / 16; i += kT) reinterpret_cast<uint4*>(wS)[i] = gS[i];
+    __syncthreads();
+    if (preP || preS) {
+      preshuffle_slot(wP, sp.bpf / 4, preP ? sp.shkind : SH_IDENTITY, lut, wS, ss.bpf / 4,
+                      preS ? ss.shkind : SH_IDENTITY, lut + 1024, tid, kT);
+      __syncthreads();
+    }
+    const FrameInfo fi = p.finfo[f];
+    const int sP = g0 ? fi.s1 : fi.s2, sS = g0 ? fi.s2 : fi.s1;
+    const int mP = tid - sP, mS = tid - sS;
+    const int cP = mP & ((32 / bitsP) - 1), cS = mS & ((32 / bitsS) - 1);
+    const uint32_t tbP = (uint32_t)((mP & lsbP) << (bitsP + 2));
+    const uint32_t tbS = 2048u + (uint32_t)((mS & lsbS) << (bitsS + 2));
+    float2 v[16];
+    fold_station<false, 1>(bitsP, splitP, wP, smem, sP, pos[cP], tbP, v, tid, false);
+    fold_station<true, 1>(bitsS, splitS, wS, smem, sS, pos[32 + cS], tbS, v, tid, false);
+    float* oP = outP + f * kN + tid;
+    float* oS = outS + f * kN + tid;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      oP[r * kT] = v[r].x * uP;
+      oS[r * kT] = v[r].y * uS;
+    }
+  }
+}
+
+cudaError_t launch_fold_decode(const CorrParams& p, int grid, cudaStream_t stream) {
+  // tables, then both stations' words of one frame (8-bit stations at most)
+  const uint32_t smem = kOffA + 2u * kN;
+  fold_decode_kernel<<<grid, kT, smem, stream>>>(p);
+  return cudaGetLastError();
 }
 
 uint32_t fold_smem_bytes(uint32_t stage_bytes) { return fold_layout(stage_bytes).total; }

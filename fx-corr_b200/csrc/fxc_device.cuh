@@ -678,7 +678,10 @@ __device__ __forceinline__ uint32_t nearest_level(float x, const float* __restri
 // ------------------------------------------------------ staging layout
 
 constexpr int kStages = 2;
-constexpr uint32_t kWaitPolls = 1u << 26;  // bounded mbarrier wait
+// Bounded mbarrier wait: an unsatisfied try_wait returns after about 3.3 us
+// on B200 (measured with the failure-injection hook), so 2^19 polls give up
+// after about 1.7 s, three orders of magnitude above any staging copy.
+constexpr uint32_t kWaitPolls = 1u << 19;
 constexpr uint32_t kFiBytes = sizeof(FrameInfo);
 
 struct SmemLayout {

@@ -12,6 +12,13 @@ namespace fxc {
 // Records msg as the calling thread's last error and returns s.
 fxc_status internal_fail(fxc_status s, const char* msg);
 
+// The failure-injection settings of fxc_debug_inject_wait_timeout, copied into
+// the kernel parameters of every correlation launch (0, 0 in normal use).
+void internal_debug_settings(uint32_t* wait_polls, uint32_t* debug_flags);
+
+// Maps a device error word (ERR_*) to a status and message; FXC_OK for 0.
+fxc_status internal_device_error(uint32_t err);
+
 // Validates c and fills the host copies of the decode tables: byte LUTs of
 // both shuffles, f32 levels, the per-station exact level scales and shuffle kinds.
 fxc_status internal_prepare_tables(const fxc_scan_cfg* c, uint32_t* lut2048, float* lv512,

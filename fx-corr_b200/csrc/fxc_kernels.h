@@ -24,7 +24,14 @@ struct CorrParams {
   float* out_a;          // MODE_SPECTRA: S1 [nf][H] complex; MODE_DECODE: x1 [nf][N]
   float* out_b;          // S2 / x2
   uint32_t* err;         // device error word (ERR_*)
+  uint32_t wait_polls;   // polls before a staging wait gives up (0: kWaitPolls)
+  uint32_t debug_flags;  // DBG_* (failure-injection test hook; 0 in normal use)
 };
+
+// Failure injection for the tests of the bounded waits: the staging copies
+// of the fold kernels are announced on their mbarriers but never issued, so
+// every wait runs out after wait_polls polls with nothing in flight.
+enum : uint32_t { DBG_WITHHOLD_COPIES = 1u };
 
 // Layout-compatible with fxc_frame_delay in include/fxc.h.
 struct fxc_frame_delay_dev {
@@ -60,6 +67,9 @@ int corr_ctas_per_sm(uint32_t n);
 cudaError_t launch_corr(uint32_t n, int mode, const CorrParams& p, int grid, cudaStream_t s);
 // FFT-8192 correlation (MODE_CORR), one frame pair per CTA iteration (corr_fold.cu)
 cudaError_t launch_corr_fold(const CorrParams& p, int grid, cudaStream_t s);
+// FFT-8192 decode + integer shift through the correlation kernel's own decode
+// path (fold_inputs), written out as f32 samples (MODE_DECODE semantics)
+cudaError_t launch_fold_decode(const CorrParams& p, int grid, cudaStream_t s);
 // FFT-16384 correlation as two 8192-point rows (corr_fold.cu); needs an even
 // band shift (a row holds the bins of one parity)
 bool corr_fold2_supported(const CorrParams& p);

@@ -17,6 +17,11 @@
 // read and the error word is cleared per call, so results never depend on
 // earlier calls, but calls whose work overlaps on the GPU (different streams,
 // or different host threads, on one device) race on the array.
+//
+// A bounded device-side wait that gives up sets the array's error word; the
+// call then fills its output block with NaN (a last small kernel on the same
+// stream), and fxc_sector_noalloc_check reads the word back, without
+// allocating, as FXC_ETIMEDOUT / FXC_EDEVICE.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -47,6 +52,47 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 std::mutex g_mu;
 void* g_scratch_addr[64] = {};  // device address of the array, per device ordinal
+
+// Device address of the array on device `dev` (looked up once per device).
+fxc_status scratch_base(int dev, unsigned char** base) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      char msg[256];
+      snprintf(msg, sizeof msg, "cudaGetSymbolAddress of the scratch array failed: %s",
+               cudaGetErrorString(e));
+      return internal_fail(FXC_ECUDA, msg);
+    }
+    g_scratch_addr[dev] = p;
+  }
+  *base = static_cast<unsigned char*>(g_scratch_addr[dev]);
+  return FXC_OK;
+}
+
+// The current device, and that `stream` (NULL: the default stream) belongs to it.
+fxc_status current_device(void* stream, int* dev) {
+  if (cudaGetDevice(dev) != cudaSuccess || *dev < 0 || *dev >= 64)
+    return internal_fail(FXC_ECUDA, "no current CUDA device");
+  if (stream) {
+    int sd = -1;
+    if (cudaStreamGetDevice((cudaStream_t)stream, &sd) != cudaSuccess)
+      return internal_fail(FXC_EINVAL, "stream is not a valid CUDA stream");
+    if (sd != *dev)
+      return internal_fail(FXC_EINVAL,
+                           "stream belongs to another device than the current one; make the "
+                           "stream's device current before the call");
+  }
+  return FXC_OK;
+}
+
+// After the reduction: a call whose bounded wait gave up leaves NaN in every
+// output value instead of short sums.
+__global__ void noalloc_poison_kernel(const uint32_t* err, double* acc, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && *err != 0u) acc[i] = __longlong_as_double(0x7ff8000000000000ll);
+}
 
 }  // namespace
 
@@ -88,24 +134,11 @@ extern "C" fxc_status fxc_sector_run_device_noalloc(const fxc_scan_cfg* cfg,
   }
 
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
-    return internal_fail(FXC_ECUDA, "no current CUDA device");
+  st = current_device(stream, &dev);
+  if (st != FXC_OK) return st;
   unsigned char* base = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_addr[dev]) {
-      void* p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess) {
-        char msg[256];
-        snprintf(msg, sizeof msg, "cudaGetSymbolAddress of the scratch array failed: %s",
-                 cudaGetErrorString(e));
-        return internal_fail(FXC_ECUDA, msg);
-      }
-      g_scratch_addr[dev] = p;
-    }
-    base = static_cast<unsigned char*>(g_scratch_addr[dev]);
-  }
+  st = scratch_base(dev, &base);
+  if (st != FXC_OK) return st;
   FrameInfo* rec = reinterpret_cast<FrameInfo*>(base);
   uint32_t* d_lut = reinterpret_cast<uint32_t*>(base + kOffLut);
   float* d_lv = reinterpret_cast<float*>(base + kOffLevels);
@@ -184,6 +217,7 @@ extern "C" fxc_status fxc_sector_run_device_noalloc(const fxc_scan_cfg* cfg,
   p.partials = part;
   p.finfo = rec;
   p.err = d_err;
+  internal_debug_settings(&p.wait_polls, &p.debug_flags);
   int sms = 0;
   NA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t iters = (nf + fpc - 1) / fpc;
@@ -194,6 +228,22 @@ extern "C" fxc_status fxc_sector_run_device_noalloc(const fxc_scan_cfg* cfg,
   const double u1 = 1.0 / scale[0], u2 = 1.0 / scale[1];
   NA_CK(launch_reduce(part, (int)grid, (int)h, 0.25 * u1 * u1, 0.25 * u2 * u2, 0.25 * u1 * u2,
                       d_acc, s));
+  noalloc_poison_kernel<<<(5 * h + 255) / 256, 256, 0, s>>>(d_err, d_acc, 5 * h);
+  NA_CK(cudaGetLastError());
 #undef NA_CK
   return FXC_OK;
+}
+
+extern "C" fxc_status fxc_sector_noalloc_check(void* stream) {
+  int dev = 0;
+  fxc_status st = current_device(stream, &dev);
+  if (st != FXC_OK) return st;
+  unsigned char* base = nullptr;
+  st = scratch_base(dev, &base);
+  if (st != FXC_OK) return st;
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  uint32_t err = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&err, base + kOffErr, sizeof err, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return internal_fail(FXC_ECUDA, cudaGetErrorString(e));
+  return internal_device_error(err);
 }

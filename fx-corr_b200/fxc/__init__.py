@@ -37,7 +37,8 @@ EXPORTS = [
     "fxc_server_create", "fxc_server_submit", "fxc_server_wait", "fxc_server_destroy",
     "fxc_host_alloc", "fxc_host_free", "fxc_batch_create", "fxc_batch_destroy",
     "fxc_batch_run_device", "fxc_batch_autotune", "fxc_batch_shape", "fxc_batch_launches",
-    "fxc_batch_set_shape",
+    "fxc_batch_set_shape", "fxc_sector_noalloc_check", "fxc_debug_inject_wait_timeout",
+    "fxc_host_register", "fxc_host_unregister",
 ]
 NOALLOC_MAX_FRAMES = 32768
 
@@ -162,6 +163,8 @@ def lib():
         "fxc_scan_set_profiling": ([vp, C.c_int32], st),
         "fxc_sector_run_device_noalloc": ([C.POINTER(ScanCfgC), vp, vp, C.c_uint64, C.c_uint64,
                                            vp, vp], st),
+        "fxc_sector_noalloc_check": ([vp], st),
+        "fxc_debug_inject_wait_timeout": ([C.c_uint32, C.c_int32], st),
         "fxc_scan_profile": ([vp, f64p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_int32],
                              st),
         "fxc_server_create": ([vp, C.POINTER(ServerOpts), C.POINTER(vp)], st),
@@ -170,6 +173,8 @@ def lib():
         "fxc_server_destroy": ([vp], st),
         "fxc_host_alloc": ([C.c_uint64, C.POINTER(vp)], st),
         "fxc_host_free": ([vp], st),
+        "fxc_host_register": ([vp, C.c_uint64], st),
+        "fxc_host_unregister": ([vp], st),
         "fxc_batch_create": ([vp, C.POINTER(BatchOpts), C.POINTER(vp)], st),
         "fxc_batch_destroy": ([vp], st),
         "fxc_batch_run_device": ([vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
@@ -590,6 +595,30 @@ def sector_run_device_noalloc(cfg: ScanConfig, d_raw1, d_raw2, nf: int, first_fr
     c = cfg.to_c()
     check(lib().fxc_sector_run_device_noalloc(C.byref(c), _ptr(d_raw1), _ptr(d_raw2), nf,
                                               first_frame, _ptr(d_acc), _stream(stream)))
+
+
+def host_register(buf: np.ndarray):
+    """fxc_host_register: page-lock a caller-owned numpy buffer in place."""
+    check(lib().fxc_host_register(buf.ctypes.data, buf.nbytes))
+
+
+def host_unregister(buf: np.ndarray):
+    check(lib().fxc_host_unregister(buf.ctypes.data))
+
+
+def sector_noalloc_check(stream=None):
+    """fxc_sector_noalloc_check: synchronises `stream` and raises FxcError
+    (FXC_ETIMEDOUT, FXC_EDEVICE) when the last allocation-free call on the
+    current device reported a kernel error."""
+    check(lib().fxc_sector_noalloc_check(_stream(stream)))
+
+
+def debug_inject_wait_timeout(wait_polls: int = 0, withhold_copies: bool = False):
+    """Failure-injection test hook (fxc_debug_inject_wait_timeout): bound the
+    correlation kernels' staging waits to `wait_polls` polls and, with
+    `withhold_copies`, let them run out with no copy in flight.  (0, False)
+    restores normal operation."""
+    check(lib().fxc_debug_inject_wait_timeout(wait_polls, int(bool(withhold_copies))))
 
 
 def probe_fp32_peak(device: int = 0) -> float:

@@ -167,6 +167,18 @@ FXC_API fxc_status fxc_sector_run_device(fxc_scan* s, const uint8_t* d_raw1, con
  * FXC_OK when no kernel reported an error.  Synchronises the scan's work. */
 FXC_API fxc_status fxc_scan_check(fxc_scan* s);
 
+/* Failure-injection test hook, no reference counterpart (the reference has
+ * no device-side waits).  Process-wide, for the correlation launches that
+ * follow: wait_polls > 0 bounds every staging wait of the FFT-8192 / 16384
+ * correlation kernels to that many mbarrier polls (0 restores the built-in
+ * limit); withhold_copies != 0 makes those kernels announce their staging
+ * copies without issuing them, so that each CTA's first wait runs out with
+ * no copy in flight, the kernel sets its error word and stops, and
+ * fxc_scan_check / fxc_sector_wait / fxc_sector_noalloc_check report
+ * FXC_ETIMEDOUT while the CUDA context stays usable.  Not for production
+ * use; (0, 0) is the normal setting. */
+FXC_API fxc_status fxc_debug_inject_wait_timeout(uint32_t wait_polls, int32_t withhold_copies);
+
 /* Kernel timing: when enabled, every correlation-kernel launch of this scan
  * is bracketed by CUDA events on its launch stream.  fxc_scan_profile sums
  * their elapsed device time (synchronising on the last event) and reports the
@@ -190,10 +202,18 @@ FXC_API fxc_status fxc_scan_profile(fxc_scan* s, double* kernel_ms, uint64_t* ke
  * <= 8192, nf <= FXC_NOALLOC_MAX_FRAMES per call (add the results of several
  * calls for a longer sector), geometric table <= FXC_NOALLOC_MAX_GEOM entries;
  * larger requests fail with FXC_EINVAL / FXC_EUNSUPPORTED.  Runs on the
- * current device, enqueued on `stream`.  The first call on each device looks
- * up the array's device address, so make that first call before any stream
- * capture.  All calls share the array: calls whose work overlaps on one GPU
- * (other streams or host threads) race and must be serialised by the caller. */
+ * current device, enqueued on `stream`, which must belong to that device
+ * (FXC_EINVAL otherwise).  The first call on each device looks up the array's
+ * device address, so make that first call before any stream capture.  All
+ * calls share the array: calls whose work overlaps on one GPU (other streams
+ * or host threads) race and must be serialised by the caller.
+ *
+ * Errors inside the kernels: when a bounded device-side wait gives up, the
+ * call fills d_acc with NaN; fxc_sector_noalloc_check(stream) then
+ * synchronises `stream` and returns FXC_ETIMEDOUT (FXC_EDEVICE for another
+ * kernel error, FXC_OK when the last call on this device completed cleanly),
+ * again without allocating.  Check before the next call on the device, which
+ * clears the error word. */
 #define FXC_NOALLOC_MAX_FRAMES 32768
 #define FXC_NOALLOC_MAX_GEOM 4096
 #define FXC_NOALLOC_SCRATCH_MIB 24
@@ -201,6 +221,7 @@ FXC_API fxc_status fxc_sector_run_device_noalloc(const fxc_scan_cfg* cfg, const 
                                                  const uint8_t* d_raw2, uint64_t nf,
                                                  uint64_t first_frame, double* d_acc,
                                                  void* stream);
+FXC_API fxc_status fxc_sector_noalloc_check(void* stream);
 
 /* ---- serving loop -------------------------------------------------------
  * No reference counterpart: the reference correlates one scan per process
@@ -316,6 +337,16 @@ FXC_API uint64_t fxc_batch_launches(fxc_batch* b);
  * it overlap device work. */
 FXC_API fxc_status fxc_host_alloc(uint64_t bytes, void** out);
 FXC_API fxc_status fxc_host_free(void* p);
+/* Page-locks a caller-owned host buffer in place, so that a reader that owns
+ * its sector buffers (the reference's Vec<u8> per station, filled by the
+ * reader thread, src/main.rs:2133-2147) passes them to fxc_sector_submit
+ * without a staging copy and the host-to-device copies overlap device work.
+ * The buffer must stay allocated until fxc_host_unregister; registering
+ * costs a page-table walk, so register long-lived buffers once.  A buffer
+ * that is already registered (or page-locked by fxc_host_alloc) is
+ * accepted as is. */
+FXC_API fxc_status fxc_host_register(void* p, uint64_t bytes);
+FXC_API fxc_status fxc_host_unregister(void* p);
 
 /* Stage entry points, for parity tests of the individual steps. */
 /* Per-frame delay model on the device (src/main.rs:184-241). */
