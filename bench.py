@@ -571,8 +571,9 @@ def serve_leg(fxc, torch, eng, jobs, slots, batch, plain_jobs=None, label="", mi
                       j["sector_frames"], out.ctypes.data, None)
         prepared.append((jc, out))
 
-    def run_served(paced):
-        n = len(jobs)
+    def run_served(paced, server=None, count=None):
+        server = server or sv
+        n = len(jobs) if count is None else count
         ids = [C.c_uint64() for _ in range(n)]
         stats = [fxc.JobStats() for _ in range(n)]
         ready = [threading.Event() for _ in range(n)]
@@ -585,7 +586,7 @@ def serve_leg(fxc, torch, eng, jobs, slots, batch, plain_jobs=None, label="", mi
                     dt = t0 + jobs[k]["arrival"] - time.perf_counter()
                     if dt > 0:
                         time.sleep(dt)
-                rc = L.fxc_server_submit(sv.h, C.byref(prepared[k][0]), C.byref(ids[k]))
+                rc = L.fxc_server_submit(server.h, C.byref(prepared[k][0]), C.byref(ids[k]))
                 if rc != 0:
                     err.append((k, rc, L.fxc_last_error().decode()))
                 ready[k].set()
@@ -595,7 +596,7 @@ def serve_leg(fxc, torch, eng, jobs, slots, batch, plain_jobs=None, label="", mi
         for k in range(n):  # waits run beside the submissions
             ready[k].wait()
             if not err:
-                rc = L.fxc_server_wait(sv.h, ids[k].value, -1, C.byref(stats[k]))
+                rc = L.fxc_server_wait(server.h, ids[k].value, -1, C.byref(stats[k]))
                 if rc != 0:
                     err.append((k, rc, L.fxc_last_error().decode()))
         th.join()
@@ -618,6 +619,16 @@ def serve_leg(fxc, torch, eng, jobs, slots, batch, plain_jobs=None, label="", mi
         p_lat, p_wall = run_plain(True)
     finally:
         sv.close()
+    # the second plain baseline: one job at a time through one long-lived scan
+    # that is rebound to each job (a one-slot server without batching: no
+    # per-job allocation, the job loop runs in the server's C++ worker)
+    pp = fxc.Server(eng, slots=1, batch=False)
+    try:
+        run_served(False, pp, np_jobs)
+        q_sat_wall = statistics.median(run_served(False, pp, np_jobs)[1] for _ in range(3))
+        q_lat, q_wall = run_served(True, pp, np_jobs)
+    finally:
+        pp.close()
     tot = float(sum(samples))
     tot_plain = float(sum(samples[:np_jobs]))
 
@@ -625,6 +636,7 @@ def serve_leg(fxc, torch, eng, jobs, slots, batch, plain_jobs=None, label="", mi
         return float(np.percentile(np.asarray(v) * 1e3, q))
 
     s_jps, p_jps = len(jobs) / s_sat_wall, np_jobs / p_sat_wall
+    q_jps = np_jobs / q_sat_wall
     return {
         "workload": label, "jobs": len(jobs), "plain_jobs": np_jobs, "slots": slots,
         "batched": bool(batch), "job_mix": mix,
@@ -636,12 +648,21 @@ def serve_leg(fxc, torch, eng, jobs, slots, batch, plain_jobs=None, label="", mi
         "plain": {"p50_ms": pct(p_lat, 50), "p99_ms": pct(p_lat, 99),
                   "gsample_s": tot_plain / p_wall / 1e9,
                   "saturated_jobs_per_s": p_jps,
-                  "saturated_gsample_s": tot_plain / p_sat_wall / 1e9},
+                  "saturated_gsample_s": tot_plain / p_sat_wall / 1e9,
+                  "path": "per job: fxc_scan_open, per-sector synchronous fxc_sector_submit/wait, "
+                          "fxc_scan_close (Python loop)"},
+        "plain_persistent": {"p50_ms": pct(q_lat, 50), "p99_ms": pct(q_lat, 99),
+                             "gsample_s": tot_plain / q_wall / 1e9,
+                             "saturated_jobs_per_s": q_jps,
+                             "saturated_gsample_s": tot_plain / q_sat_wall / 1e9,
+                             "path": "one long-lived scan rebound to each job in turn (one-slot "
+                                     "server, no batching): no per-job allocation, job loop in "
+                                     "C++"},
         "saturated_job_throughput_ratio": s_jps / p_jps,
+        "saturated_job_throughput_ratio_vs_persistent": s_jps / q_jps,
         "saturated_runs": "median of 3 per path",
-        "path": "fxc_server_submit/fxc_server_wait%s vs fxc_scan_open + per-sector synchronous "
-                "fxc_sector_submit/wait + fxc_scan_close" % (
-                    " (batched: fxc_batch_run_device in CUDA graphs, autotuned)" if batch else ""),
+        "path": "fxc_server_submit/fxc_server_wait%s" % (
+            " (batched: fxc_batch_run_device in CUDA graphs, autotuned)" if batch else ""),
     }
 
 
@@ -788,17 +809,21 @@ def main():
                 return {"error": f"{type(e).__name__}: {e}"}
 
         serve = {
-            # the headline's served vs plain: short 2-bit FFT-8192 jobs, batched server
+            # the headline's served vs plain: the long-job stream of the serving
+            # workload (0.1-5 s chunks, FFT 1024-16384, 2x real time offered)
+            "headline": "long",
+            "long": guarded(lambda: serve_leg(
+                fxc, torch, eng, serve_jobs(args.serve_jobs, 2.0), slots=4, batch=True,
+                label="serving workload: long jobs, mixed FFT",
+                mix="Poisson arrivals at 2x real time; 0.1-5 s at 256/512/1024 Msps, 2-bit, "
+                    "FFT 1024-16384, random delays/rates, 1-s dumps, pinned host buffers")),
+            # a second figure: short 2-bit FFT-8192 jobs, where per-job set-up
+            # dominates the plain path
             "short": guarded(lambda: serve_leg(
                 fxc, torch, eng, short_jobs(args.serve_short_jobs, rate=4000.0), slots=32,
                 batch=True, plain_jobs=200, label="short jobs, FFT 8192",
                 mix="Poisson arrivals at 4000 jobs/s; 1-16 ms at 1024 Msps (125-2000 frame "
                     "pairs), 2-bit, FFT 8192, random delays/rates, one dump, pinned host buffers")),
-            "long": guarded(lambda: serve_leg(
-                fxc, torch, eng, serve_jobs(args.serve_jobs, 2.0), slots=4, batch=True,
-                label="long jobs, mixed FFT",
-                mix="Poisson arrivals at 2x real time; 0.1-5 s at 256/512/1024 Msps, 2-bit, "
-                    "FFT 1024-16384, random delays/rates, 1-s dumps, pinned host buffers")),
         }
 
     # ---- roofline of the dominant kernel (correlation kernel, one sector per launch)

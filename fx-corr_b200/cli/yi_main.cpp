@@ -65,6 +65,29 @@ struct Fail : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 
+// An error the reference raises as std::io::Error::other(String): its main
+// prints the Debug form `Custom { kind: Other, error: "..." }`.
+struct IoFail : Fail {
+  using Fail::Fail;
+};
+
+// A string's Debug form: quoted, with quotes and backslashes escaped.
+std::string debug_quoted(const std::string& m) {
+  std::string q = "\"";
+  for (char c : m) {
+    if (c == '"' || c == '\\') q += '\\';
+    if (c == '\n') {
+      q += "\\n";
+      continue;
+    }
+    q += c;
+  }
+  return q + "\"";
+}
+
+// std::io::Error's Display of an OS error: "<strerror> (os error <n>)".
+std::string os_error(int e) { return std::string(std::strerror(e)) + " (os error " + std::to_string(e) + ")"; }
+
 // ------------------------------------------------------------------ logging
 // println! of the reference, optionally teed to ./stdout/stdout_<tag>.log
 // (main.rs:36-108, yi-corr only).
@@ -186,11 +209,13 @@ void ck(fxc_status s, const char* what) {
 // of short reads (main.rs:445-503, 1578-1616).
 class RawReader {
  public:
-  RawReader(const std::string& path, uint64_t start_byte) : path_(path) {
+  // label: "ant1" / "ant2", for the reference's read-error message
+  RawReader(const std::string& path, uint64_t start_byte, const char* label)
+      : path_(path), label_(label) {
     f_ = std::fopen(path.c_str(), "rb");
-    if (!f_) throw Fail("failed to open/seek " + path + ": " + std::strerror(errno));
+    if (!f_) throw Fail("failed to open/seek " + path + ": " + os_error(errno));
     if (fseeko(f_, (off_t)start_byte, SEEK_SET) != 0)
-      throw Fail("failed to open/seek " + path + ": " + std::strerror(errno));
+      throw Fail("failed to open/seek " + path + ": " + os_error(errno));
 #ifdef POSIX_FADV_SEQUENTIAL
     posix_fadvise(fileno(f_), 0, 0, POSIX_FADV_SEQUENTIAL);
     posix_fadvise(fileno(f_), 0, 0, POSIX_FADV_WILLNEED);
@@ -199,12 +224,22 @@ class RawReader {
   ~RawReader() {
     if (f_) std::fclose(f_);
   }
+  RawReader(const RawReader&) = delete;
+  RawReader& operator=(const RawReader&) = delete;
+  // read_with_padding (main.rs:445-456): a short read leaves the tail zero
   void read_padded(uint8_t* out, size_t n) {
     size_t got = 0;
     while (got < n) {
+      errno = 0;
       const size_t r = std::fread(out + got, 1, n - got, f_);
       if (r == 0) {
-        if (std::ferror(f_)) throw Fail("failed reading " + path_);
+        if (std::ferror(f_)) {
+          if (errno == EINTR) {
+            std::clearerr(f_);
+            continue;
+          }
+          throw Fail(std::string("failed reading ") + label_ + " input: " + os_error(errno));
+        }
         break;
       }
       got += r;
@@ -214,8 +249,20 @@ class RawReader {
 
  private:
   std::string path_;
+  const char* label_;
   FILE* f_ = nullptr;
 };
+
+// Opens a station's reader; a failure is reported as the reference's reader
+// thread reports it through its channel (main.rs:2110-2127, 2196-2210).
+std::unique_ptr<RawReader> open_reader(const std::string& path, uint64_t start_byte,
+                                       const char* label) {
+  try {
+    return std::make_unique<RawReader>(path, start_byte, label);
+  } catch (const std::exception& e) {
+    throw IoFail(std::string("synth reader error: ") + e.what());
+  }
+}
 
 // One sector's packed bytes of both stations in page-locked memory.
 struct SectorBuf {
@@ -231,7 +278,8 @@ class SectorReader {
  public:
   SectorReader(const std::string& p1, uint64_t s1, const std::string& p2, uint64_t s2,
                std::vector<uint64_t> counts, uint64_t bpf1, uint64_t bpf2, int depth)
-      : r1_(p1, s1), r2_(p2, s2), counts_(std::move(counts)), bpf1_(bpf1), bpf2_(bpf2) {
+      : r1_(open_reader(p1, s1, "ant1")), r2_(open_reader(p2, s2, "ant2")),
+        counts_(std::move(counts)), bpf1_(bpf1), bpf2_(bpf2) {
     uint64_t mx = 0;
     for (uint64_t c : counts_) mx = std::max(mx, c);
     for (int k = 0; k < depth; ++k) {
@@ -261,7 +309,7 @@ class SectorReader {
   SectorBuf* next() {
     std::unique_lock<std::mutex> lk(mu_);
     cv_.wait(lk, [&] { return !ready_.empty() || done_ || !err_.empty(); });
-    if (!err_.empty()) throw Fail(err_);
+    if (!err_.empty()) throw IoFail("synth reader error: " + err_);
     if (ready_.empty()) return nullptr;
     SectorBuf* b = ready_.front();
     ready_.pop_front();
@@ -290,8 +338,8 @@ class SectorReader {
         }
         b->nf = counts_[i];
         b->index = i;
-        r1_.read_padded(b->b1, b->nf * bpf1_);
-        r2_.read_padded(b->b2, b->nf * bpf2_);
+        r1_->read_padded(b->b1, b->nf * bpf1_);
+        r2_->read_padded(b->b2, b->nf * bpf2_);
         bytes_ += b->nf * (bpf1_ + bpf2_);
         {
           std::lock_guard<std::mutex> lk(mu_);
@@ -309,7 +357,7 @@ class SectorReader {
     }
     cv_.notify_all();
   }
-  RawReader r1_, r2_;
+  std::unique_ptr<RawReader> r1_, r2_;
   std::vector<uint64_t> counts_;
   uint64_t bpf1_, bpf2_;
   std::vector<std::unique_ptr<SectorBuf>> owned_;
@@ -628,6 +676,16 @@ void run_once(const Args& args, Mode mode, const std::optional<Schedule>& sch, f
   if (spw1 == 0 || spw2 == 0) throw Fail("invalid samples-per-word while aligning input start");
   const uint64_t start1_a = (start1 / spw1) * spw1, start2_a = (start2 / spw2) * spw2;
   const uint64_t start1_byte = start1_a * bit1 / 8, start2_byte = start2_a * bit2 / 8;
+  const int64_t res1 = (int64_t)start1_a - (int64_t)start1, res2 = (int64_t)start2_a - (int64_t)start2;
+  logf("[info] Input start ant1: desired sample %llu -> byte %llu + bit 0 (actual sample %llu, "
+       "residual %lld sample)", (unsigned long long)start1, (unsigned long long)start1_byte,
+       (unsigned long long)start1_a, (long long)res1);
+  logf("[info] Input start ant2: desired sample %llu -> byte %llu + bit 0 (actual sample %llu, "
+       "residual %lld sample)", (unsigned long long)start2, (unsigned long long)start2_byte,
+       (unsigned long long)start2_a, (long long)res2);
+  if (res1 != 0 || res2 != 0)
+    logf("[info] Word-aligned seek residual: ant1=%lld sample(s), ant2=%lld sample(s)",
+         (long long)res1, (long long)res2);
   const double d_seek = ((double)((int64_t)start2_a - (int64_t)start1_a)) / fs;
 
   // delay model (main.rs:1618-1673)
@@ -1065,10 +1123,16 @@ int real_main(int argc, char** argv) {
 int main(int argc, char** argv) {
   try {
     return yi::real_main(argc, argv);
+  } catch (const yi::IoFail& e) {
+    // an io::Error::other(String) returned from main: its Debug form
+    std::fflush(stdout);
+    std::fprintf(stderr, "Error: Custom { kind: Other, error: %s }\n",
+                 yi::debug_quoted(e.what()).c_str());
+    return 1;
   } catch (const std::exception& e) {
     // a Rust main returning Err prints the error's Debug form and exits 1
     std::fflush(stdout);
-    std::fprintf(stderr, "Error: \"%s\"\n", e.what());
+    std::fprintf(stderr, "Error: %s\n", yi::debug_quoted(e.what()).c_str());
     return 1;
   }
 }

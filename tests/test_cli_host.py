@@ -16,26 +16,6 @@ ROOT = Path(__file__).resolve().parents[1]
 CLI = ROOT / "fx-corr_b200" / "cli"
 
 
-@pytest.fixture(scope="session")
-def tool(tmp_path_factory):
-    cxx = shutil.which("g++")
-    if cxx is None:
-        pytest.skip("g++ not available")
-    out = tmp_path_factory.mktemp("clihost") / "cli_host_check"
-    srcs = [ROOT / "tests" / "cli_host_check.cpp"] + [CLI / f for f in
-                                                     ("args.cpp", "cor_writer.cpp", "geom.cpp",
-                                                      "schedule.cpp")]
-    subprocess.run([cxx, "-std=c++17", "-O1", "-I", str(CLI), *map(str, srcs), "-o", str(out)],
-                   check=True, capture_output=True, text=True)
-
-    def run(*args):
-        r = subprocess.run([str(out), *map(str, args)], capture_output=True, text=True, timeout=60)
-        assert r.returncode == 0, r.stderr
-        return r.stdout.strip()
-
-    return run
-
-
 # ------------------------------------------------------------ src/geom.rs tests
 
 def test_reference_geom_tests(tool):
