@@ -812,8 +812,10 @@ def main():
             # the headline's served vs plain: the long-job stream of the serving
             # workload (0.1-5 s chunks, FFT 1024-16384, 2x real time offered)
             "headline": "long",
+            # long sectors saturate the host link from per-slot streams, the
+            # server's mode for long scans (batching pays off on short jobs)
             "long": guarded(lambda: serve_leg(
-                fxc, torch, eng, serve_jobs(args.serve_jobs, 2.0), slots=4, batch=True,
+                fxc, torch, eng, serve_jobs(args.serve_jobs, 2.0), slots=4, batch=False,
                 label="serving workload: long jobs, mixed FFT",
                 mix="Poisson arrivals at 2x real time; 0.1-5 s at 256/512/1024 Msps, 2-bit, "
                     "FFT 1024-16384, random delays/rates, 1-s dumps, pinned host buffers")),

@@ -337,6 +337,7 @@ LargeParams large_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2
   p.a2s = (int32_t)s->cfg.a2s;
   p.grid = s->cfg.grid;
   p.products = s->cfg.products;
+  p.err = s->d_err;
   return p;
 }
 
@@ -582,8 +583,6 @@ namespace fxc {
 fxc_status sector_stage(fxc_scan* s, const uint8_t* raw1, uint64_t n1, const uint8_t* raw2,
                         uint64_t n2, uint64_t nf, StagedSector* out) {
   if (!s || !out) return fail(FXC_EINVAL, "NULL argument");
-  if (s->cfg.products & FXC_PROD_RAW)
-    return fail(FXC_EINVAL, "staged sectors do not write phased .raw frames");
   DeviceGuard g(s->eng->device);
   SectorSlot* sl = nullptr;
   fxc_status st = stage_sector(s, raw1, n1, raw2, n2, nf, &sl);
@@ -593,6 +592,7 @@ fxc_status sector_stage(fxc_scan* s, const uint8_t* raw1, uint64_t n1, const uin
   out->d_raw1 = sl->d_raw1;
   out->d_raw2 = sl->d_raw2;
   out->d_acc = sl->d_acc;
+  out->d_raw_out = (s->cfg.products & FXC_PROD_RAW) ? sl->d_rawout : nullptr;
   out->h2d = sl->ev_h2d;
   return FXC_OK;
 }
@@ -1261,14 +1261,38 @@ void engine_release(fxc_engine* e, uint64_t bytes) {
 }
 
 fxc_status batch_describe(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
-                          uint64_t first, double* d_acc, BatchScan* out, int* group) {
+                          uint64_t first, double* d_acc, uint8_t* d_raw_out, BatchScan* out,
+                          int* group) {
   *group = -1;
   if (!d_acc) return fail(FXC_EINVAL, "d_acc is NULL");
   fxc_status st = nf ? check_device_inputs(s, r1, r2) : FXC_OK;
   if (st != FXC_OK) return st;
   const bool corr = (s->cfg.products & (FXC_PROD_ACF | FXC_PROD_XCF)) != 0;
   const bool phased = (s->cfg.products & (FXC_PROD_PHASED | FXC_PROD_RAW)) != 0;
-  if (nf == 0 || !corr || phased || s->n > 16384) return FXC_OK;
+  if ((s->cfg.products & FXC_PROD_RAW) && nf && !d_raw_out)
+    return fail(FXC_EINVAL, "the scan writes phased .raw frames but its raw output is NULL");
+  if (nf == 0 || (corr && phased)) return FXC_OK;  // the per-scan path
+  if (phased) {
+    // phased sectors of FFT 1024..8192 run in the phased batch kernels
+    if (s->n > 8192) return FXC_OK;
+    if ((st = grow_frame_info(s, nf)) != FXC_OK) return st;
+    BatchScan b{};
+    b.p = corr_params(s, r1, r2, nf, first);  // delay model and frame records
+    b.p.finfo = s->d_finfo;
+    b.p.partials = nullptr;
+    b.pp = phased_params(s, r1, r2, nf, first, d_raw_out);
+    b.pp.finfo = s->d_finfo;
+    b.pp.partials = nullptr;  // the batch's
+    b.acc = d_acc;
+    b.n = s->n;
+    b.h = s->h;
+    b.phased = 1;
+    *out = b;
+    *group = s->n == 1024 ? BG_PHASED_1024 : s->n == 2048 ? BG_PHASED_2048
+           : s->n == 4096 ? BG_PHASED_4096 : BG_PHASED_8192;
+    return FXC_OK;
+  }
+  if (s->n > 16384) return FXC_OK;
   CorrParams p = corr_params(s, r1, r2, nf, first);
   if (s->n == 16384 && !corr_fold2_supported(p)) return FXC_OK;
   if ((st = grow_frame_info(s, nf)) != FXC_OK) return st;
@@ -1290,13 +1314,14 @@ fxc_status batch_describe(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uin
 }
 
 fxc_status run_sector_internal(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
-                               uint64_t first, double* d_acc, cudaStream_t st) {
+                               uint64_t first, double* d_acc, uint8_t* d_raw_out,
+                               cudaStream_t st) {
   const fxc_status c = nf ? check_device_inputs(s, r1, r2) : FXC_OK;
   if (c != FXC_OK) return c;
   if (!d_acc) return fail(FXC_EINVAL, "d_acc is NULL");
-  if (s->cfg.products & FXC_PROD_RAW)
-    return fail(FXC_EINVAL, "a batch does not write phased .raw frames; use fxc_sector_run_device");
-  return run_sector_device(s, r1, r2, nf, first, d_acc, nullptr, st);
+  if ((s->cfg.products & FXC_PROD_RAW) && nf && !d_raw_out)
+    return fail(FXC_EINVAL, "the scan writes phased .raw frames but its raw output is NULL");
+  return run_sector_device(s, r1, r2, nf, first, d_acc, d_raw_out, st);
 }
 
 void engine_track_batch(fxc_engine* e, fxc_batch* b, bool add) {

@@ -1,7 +1,8 @@
 // batch.cu — batched sectors of many scans (include/fxc.h, fxc_batch_*).
 //
 // A call describes each scan's sector (BatchScan: the scan's tables, frame
-// record buffer, raw words and output), splits every sector into work items
+// record buffer, raw words and output; correlation or phased products),
+// splits every sector into work items
 // of `item_frames` frames (at most one per persistent CTA), uploads the
 // tables in one copy and runs
 //   batch_frame_info_kernel  the FP64 delay records of every frame,
@@ -40,16 +41,22 @@ namespace {
     }                                                                                      \
   } while (0)
 
-constexpr uint32_t kGroupN[kBatchGroups] = {1024, 2048, 4096, 8192, 16384};
-// kernel variants (frame pairs per CTA iteration) of each group
-const std::vector<int> kGroupFpc[kBatchGroups] = {{1, 2, 4}, {1, 2, 4}, {1, 2}, {1}, {1}};
-// single-scan defaults: the frames per iteration of corr_kernel
-constexpr int kDefaultFpc[kBatchGroups] = {4, 2, 1, 1, 1};
+constexpr uint32_t kGroupN[kBatchGroups] = {1024, 2048, 4096, 8192, 16384,
+                                            1024, 2048, 4096, 8192};
+// kernel variants (frame pairs per CTA iteration) of each group; the phased
+// groups have one variant each (the single-scan phased kernel's)
+const std::vector<int> kGroupFpc[kBatchGroups] = {{1, 2, 4}, {1, 2, 4}, {1, 2}, {1}, {1},
+                                                  {4}, {2}, {1}, {1}};
+// single-scan defaults: the frames per iteration of corr_kernel / phased_kernel
+constexpr int kDefaultFpc[kBatchGroups] = {4, 2, 1, 1, 1, 4, 2, 1, 1};
+
+bool phased_group(int g) { return g >= kCorrGroups; }
 constexpr uint32_t kDefaultItemFrames = 128;
 const uint32_t kItemCandidates[] = {32, 64, 128, 256, 512};
 
+// The correlation group of FFT length n (-1: none).
 int group_of(uint32_t n) {
-  for (int g = 0; g < kBatchGroups; ++g)
+  for (int g = 0; g < kCorrGroups; ++g)
     if (kGroupN[g] == n) return g;
   return -1;
 }
@@ -119,7 +126,8 @@ void drop_graphs(fxc_batch* b) {
 
 fxc_status prepare_variant(fxc_batch* b, int g, int fpc) {
   if (!b->prepared[g][fpc]) {
-    BCK(batch_prepare(g, fpc));
+    if (phased_group(g)) BCK(phased_batch_prepare(kGroupN[g]));
+    else BCK(batch_prepare(g, fpc));
     b->prepared[g][fpc] = true;
   }
   return FXC_OK;
@@ -128,7 +136,8 @@ fxc_status prepare_variant(fxc_batch* b, int g, int fpc) {
 fxc_status set_shape(fxc_batch* b, int g, int fpc, uint32_t item_frames) {
   fxc_status st = prepare_variant(b, g, fpc);
   if (st != FXC_OK) return st;
-  const int ctas = batch_group_ctas_per_sm(g, fpc);
+  const int ctas = phased_group(g) ? phased_batch_ctas_per_sm(kGroupN[g])
+                                   : batch_group_ctas_per_sm(g, fpc);
   if (ctas <= 0) return internal_fail(FXC_ECUDA, "batch kernel variant does not fit an SM");
   if (b->shape[g].fpc != fpc || b->shape[g].ctas != ctas) drop_graphs(b);
   b->shape[g].fpc = fpc;
@@ -206,7 +215,8 @@ uint64_t item_len(const Shape& sh, int sms, uint64_t nf) {
 
 fxc_status run_batch(fxc_batch* b, fxc_scan* const* scans, const uint8_t* const* r1,
                      const uint8_t* const* r2, const uint64_t* nf, const uint64_t* first,
-                     double* const* acc, uint32_t count, cudaStream_t stream, bool allow_graph);
+                     double* const* acc, uint8_t* const* raw_out, uint32_t count,
+                     cudaStream_t stream, bool allow_graph);
 
 // Times every variant x item size of group g on a synthetic batch and keeps
 // the fastest.  The caller holds b->mu.
@@ -304,7 +314,7 @@ fxc_status autotune_locked(fxc_batch* b, int g) {
         for (int rep = 0; rep < 4; ++rep) {
           if (cudaEventRecord(e0, st) != cudaSuccess) break;
           result = run_batch(b, scans.data(), r1.data(), r2.data(), nfs.data(), firsts.data(),
-                             accs.data(), kScans, st, false);
+                             accs.data(), nullptr, kScans, st, false);
           if (result != FXC_OK) break;
           float ms = 0.f;
           if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
@@ -342,7 +352,8 @@ fxc_status autotune_locked(fxc_batch* b, int g) {
 
 fxc_status run_batch(fxc_batch* b, fxc_scan* const* scans, const uint8_t* const* r1,
                      const uint8_t* const* r2, const uint64_t* nf, const uint64_t* first,
-                     double* const* acc, uint32_t count, cudaStream_t stream, bool allow_graph) {
+                     double* const* acc, uint8_t* const* raw_out, uint32_t count,
+                     cudaStream_t stream, bool allow_graph) {
   std::vector<Entry> ents;
   std::vector<uint32_t> others;
   ents.reserve(count);
@@ -358,7 +369,8 @@ fxc_status run_batch(fxc_batch* b, fxc_scan* const* scans, const uint8_t* const*
       return internal_fail(FXC_EINVAL, "scan belongs to another engine");
     Entry e{};
     e.idx = i;
-    fxc_status st = batch_describe(scans[i], r1[i], r2[i], nf[i], first[i], acc[i], &e.bs, &e.group);
+    fxc_status st = batch_describe(scans[i], r1[i], r2[i], nf[i], first[i], acc[i],
+                                   raw_out ? raw_out[i] : nullptr, &e.bs, &e.group);
     if (st != FXC_OK) return st;
     if (e.group < 0) others.push_back(i);
     else ents.push_back(e);
@@ -368,6 +380,7 @@ fxc_status run_batch(fxc_batch* b, fxc_scan* const* scans, const uint8_t* const*
   for (const Entry& e : ents) mask |= 1u << e.group;
   for (int g = 0; g < kBatchGroups; ++g) {
     if (!(mask & (1u << g))) continue;
+    if (phased_group(g)) b->shape[g].tuned = true;  // one variant, default item size
     if (b->autotune && !b->shape[g].tuned && !b->tuning[g]) {
       // first use: tune; if the tuner cannot run (e.g. no HBM for its
       // synthetic batch) the length keeps its default shape
@@ -397,6 +410,7 @@ fxc_status run_batch(fxc_batch* b, fxc_scan* const* scans, const uint8_t* const*
       const uint64_t per = item_len(sh, b->sms, n);
       const uint32_t nparts = (uint32_t)((n + per - 1) / per);
       const uint64_t h = e.bs.h;
+      const uint64_t slot = phased_group(g) ? h : 4 * h;  // partial doubles per item
       e.bs.part = part;
       e.bs.nparts = nparts;
       e.bs.fi0 = fi;
@@ -405,9 +419,9 @@ fxc_status run_batch(fxc_batch* b, fxc_scan* const* scans, const uint8_t* const*
       for (uint32_t k = 0; k < nparts; ++k) {
         const uint64_t f0 = k * per, f1 = std::min(n, f0 + per);
         for (uint32_t row = 0; row < (g == BG_16384 ? 2u : 1u); ++row)
-          items.push_back(BatchItem{si, row, f0, f1, part + (uint64_t)k * 4 * h});
+          items.push_back(BatchItem{si, row, f0, f1, part + (uint64_t)k * slot});
       }
-      part += (uint64_t)nparts * 4 * h;
+      part += (uint64_t)nparts * slot;
       fi += n;
       bins += h;
     }
@@ -441,8 +455,8 @@ fxc_status run_batch(fxc_batch* b, fxc_scan* const* scans, const uint8_t* const*
     a.partials = b->d_part;
     // the graph's kernels take the header and partials addresses as
     // arguments: graphs are dropped whenever either moves (grow)
-    uint64_t key = mask;
-    for (int g = 0; g < kBatchGroups; ++g) key |= (uint64_t)b->shape[g].fpc << (8 + 4 * g);
+    uint64_t key = mask;  // kBatchGroups bits
+    for (int g = 0; g < kCorrGroups; ++g) key |= (uint64_t)b->shape[g].fpc << (16 + 4 * g);
     key |= (uint64_t)ai << 40;
     const int grid_aux = b->sms * 8;
     auto enqueue = [&](cudaStream_t s, bool full) -> fxc_status {
@@ -454,7 +468,10 @@ fxc_status run_batch(fxc_batch* b, fxc_scan* const* scans, const uint8_t* const*
         const Shape& sh = b->shape[g];
         uint64_t grid = (uint64_t)b->sms * sh.ctas;
         if (!full) grid = std::min<uint64_t>(grid, hdr.nitems[g]);
-        BCK(launch_batch_group(g, sh.fpc, a, (int)std::max<uint64_t>(grid, 1), s));
+        if (phased_group(g))
+          BCK(launch_phased_batch(kGroupN[g], a, g, (int)std::max<uint64_t>(grid, 1), s));
+        else
+          BCK(launch_batch_group(g, sh.fpc, a, (int)std::max<uint64_t>(grid, 1), s));
       }
       const uint64_t rgrid = full ? (uint64_t)grid_aux
                                   : std::min<uint64_t>((uint64_t)grid_aux, (hdr.nbins + 255) / 256);
@@ -488,7 +505,8 @@ fxc_status run_batch(fxc_batch* b, fxc_scan* const* scans, const uint8_t* const*
     b->launches += kernels;
   }
   for (uint32_t i : others) {
-    fxc_status st = run_sector_internal(scans[i], r1[i], r2[i], nf[i], first[i], acc[i], stream);
+    fxc_status st = run_sector_internal(scans[i], r1[i], r2[i], nf[i], first[i], acc[i],
+                                        raw_out ? raw_out[i] : nullptr, stream);
     if (st != FXC_OK) return st;
   }
   BCK(cudaEventRecord(b->ev_done, stream));
@@ -586,8 +604,23 @@ fxc_status fxc_batch_run_device(fxc_batch* b, fxc_scan* const* scans, const uint
     return internal_fail(FXC_EINVAL, "NULL argument");
   std::lock_guard<std::mutex> lk(b->mu);
   DeviceGuardB dg(b->device);
-  return run_batch(b, scans, d_raw1, d_raw2, nf, first_frame, d_acc, count, (cudaStream_t)stream,
-                   true);
+  return run_batch(b, scans, d_raw1, d_raw2, nf, first_frame, d_acc, nullptr, count,
+                   (cudaStream_t)stream, true);
+}
+
+fxc_status fxc_batch_run_device_raw(fxc_batch* b, fxc_scan* const* scans,
+                                    const uint8_t* const* d_raw1, const uint8_t* const* d_raw2,
+                                    const uint64_t* nf, const uint64_t* first_frame,
+                                    double* const* d_acc, uint8_t* const* d_raw_out,
+                                    uint32_t count, void* stream) {
+  if (!b) return internal_fail(FXC_EINVAL, "batch is NULL");
+  if (count == 0) return FXC_OK;
+  if (!scans || !d_raw1 || !d_raw2 || !nf || !first_frame || !d_acc || !d_raw_out)
+    return internal_fail(FXC_EINVAL, "NULL argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  DeviceGuardB dg(b->device);
+  return run_batch(b, scans, d_raw1, d_raw2, nf, first_frame, d_acc, d_raw_out, count,
+                   (cudaStream_t)stream, true);
 }
 
 fxc_status fxc_batch_shape(fxc_batch* b, uint32_t fft_len, int32_t* fpc, uint32_t* item_frames,

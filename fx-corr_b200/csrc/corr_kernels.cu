@@ -449,7 +449,8 @@ __global__ void batch_frame_info_kernel(const BatchArgs a) {
 
 // Fixed-order sum of each sector's item partials (grid-stride over all bins
 // of the batch), with the same multipliers and output layout as
-// reduce_partials_kernel.
+// reduce_partials_kernel (a phased sector: its power in [4H, 5H), the
+// correlation columns zero, as reduce_phased_kernel after a zeroed block).
 __global__ void batch_reduce_kernel(const BatchArgs a) {
   const uint32_t ns = a.hdr->nscans;
   const uint64_t total = a.hdr->nbins;
@@ -459,12 +460,23 @@ __global__ void batch_reduce_kernel(const BatchArgs a) {
     const uint64_t k = x - b.bin0;
     const uint64_t h = b.h;
     const double* q = a.partials + b.part + k;
+    double* out = b.acc;
+    if (b.phased) {
+      // phased power: H partials per item, summed in item order
+      double t = 0.0;
+      for (uint32_t i = 0; i < b.nparts; ++i, q += h) t += *q;
+      out[k] = 0.0;
+      out[h + k] = 0.0;
+      out[2 * h + 2 * k] = 0.0;
+      out[2 * h + 2 * k + 1] = 0.0;
+      out[4 * h + k] = t;
+      continue;
+    }
     double s[4] = {0, 0, 0, 0};
     for (uint32_t i = 0; i < b.nparts; ++i, q += 4 * h) {
 #pragma unroll
       for (int v = 0; v < 4; ++v) s[v] += q[(size_t)v * h];
     }
-    double* out = b.acc;
     out[k] = b.m11 * s[0];
     out[h + k] = b.m22 * s[1];
     out[2 * h + 2 * k] = b.m12 * s[2];

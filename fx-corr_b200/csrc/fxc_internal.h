@@ -39,13 +39,17 @@ void engine_release(fxc_engine* e, uint64_t bytes);
 
 // Describes one sector of scan s on device inputs for a batch (*group = its
 // batch group), or leaves *group = -1 when the sector takes the per-scan
-// path (phased products, empty sector, FFT above 16384, odd band shift at
-// 16384).  Grows the scan's frame-record buffer; launches nothing.
+// path (empty sector, both correlation and phased products, phased above FFT
+// 8192, correlation above 16384, odd band shift at 16384).  d_raw_out receives
+// the phased .raw frames of a scan with FXC_PROD_RAW.  Grows the scan's
+// frame-record buffer; launches nothing.
 fxc_status batch_describe(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
-                          uint64_t first, double* d_acc, BatchScan* out, int* group);
-// The per-scan sector path (fxc_sector_run_device without .raw output).
+                          uint64_t first, double* d_acc, uint8_t* d_raw_out, BatchScan* out,
+                          int* group);
+// The per-scan sector path (fxc_sector_run_device).
 fxc_status run_sector_internal(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
-                               uint64_t first, double* d_acc, cudaStream_t st);
+                               uint64_t first, double* d_acc, uint8_t* d_raw_out,
+                               cudaStream_t st);
 
 // A sector copied into one of its scan's sector slots, for another stream to
 // compute (the serving loop's batches).
@@ -54,10 +58,11 @@ struct StagedSector {
   const uint8_t* d_raw1;
   const uint8_t* d_raw2;
   double* d_acc;      // 5 * H doubles, written by the computing stream
+  uint8_t* d_raw_out; // phased .raw frames (scans with FXC_PROD_RAW), else NULL
   cudaEvent_t h2d;    // after the input copies
 };
 // Reserves a sector slot of s and enqueues the copies of the host inputs on
-// the scan's copy stream (scans without FXC_PROD_RAW only).
+// the scan's copy stream.
 fxc_status sector_stage(fxc_scan* s, const uint8_t* raw1, uint64_t n1, const uint8_t* raw2,
                         uint64_t n2, uint64_t nf, StagedSector* out);
 // After the sector's products were enqueued (event `computed`): the

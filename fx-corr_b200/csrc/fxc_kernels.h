@@ -85,6 +85,7 @@ struct LargeParams {
   int32_t n, c;
   int32_t a1s, a1e, a2s, grid;
   uint32_t products;
+  uint32_t* err;           // device error word (ERR_*)
 };
 constexpr int kLargeGroups = 16;  // frame groups (partials) per sector
 int large_batch_frames(uint32_t n);
@@ -112,8 +113,13 @@ cudaError_t launch_large_split(const LargeParams& p, const float2* Y, uint64_t f
 // summed per sector in item order by one reduction over the whole batch.
 
 // Batch groups: the kernels a batch may launch, one per FFT length (16384 =
-// the two-row kernel, even band shifts only).
-enum { BG_1024 = 0, BG_2048 = 1, BG_4096 = 2, BG_8192 = 3, BG_16384 = 4, kBatchGroups = 5 };
+// the two-row kernel, even band shifts only), then the phased kernels of
+// FFT 1024..8192.
+enum {
+  BG_1024 = 0, BG_2048 = 1, BG_4096 = 2, BG_8192 = 3, BG_16384 = 4,
+  BG_PHASED_1024 = 5, BG_PHASED_2048 = 6, BG_PHASED_4096 = 7, BG_PHASED_8192 = 8,
+  kCorrGroups = 5, kBatchGroups = 9
+};
 
 // Frames [f0, f1) of the sector of scan `scan` (for the two-row kernel, the
 // bins of parity `row`), accumulated into partials + part ([4][H] f64).
@@ -125,14 +131,16 @@ struct BatchItem {
 
 struct BatchScan {
   CorrParams p;         // the sector: raw words, tables, frame records, error word
-  double* acc;          // [5][H] output (acf11, acf22, xcf re/im, phased = 0)
+                        // (a phased sector: its delay model and frame records only)
+  PhasedParams pp;      // a phased sector (phased != 0): the phased kernels' parameters
+  double* acc;          // [5][H] output (acf11, acf22, xcf re/im, phased power)
   double m11, m22, m12; // reduction multipliers (two-for-one 2x, level scaling)
   uint64_t part;        // partials offset of the sector's first item
   uint64_t fi0;         // first frame of the sector in the batch's frame numbering
   uint64_t bin0;        // first bin of the sector in the batch's bin numbering
   uint32_t nparts;      // partial slots (items; two-row items share one per row pair)
   uint32_t n, h;        // FFT length, bins
-  uint32_t pad;
+  uint32_t phased;      // 1: items hold [H] phased power partials instead of [4][H]
 };
 
 // Device-resident description of one batch: the kernels read every count and
@@ -166,6 +174,12 @@ cudaError_t launch_batch_group(int g, int fpc, const BatchArgs& a, int grid, cud
 // Frame records of every sector of the batch; the fixed-order reduction of
 // every sector's partials into its acc (grid-stride, any grid size).
 cudaError_t launch_batch_frame_info(const BatchArgs& a, int grid, cudaStream_t s);
+// Phased batch groups (phased_kernels.cu): FFT n in 1024..8192, frames per CTA
+// iteration as the single-scan phased kernel.
+cudaError_t phased_batch_prepare(uint32_t n);
+int phased_batch_ctas_per_sm(uint32_t n);
+int phased_frames_per_cta_iter(uint32_t n);
+cudaError_t launch_phased_batch(uint32_t n, const BatchArgs& a, int grp, int grid, cudaStream_t s);
 cudaError_t launch_batch_reduce(const BatchArgs& a, int grid, cudaStream_t s);
 
 cudaError_t launch_phased(uint32_t n, const PhasedParams& p, int grid, cudaStream_t s);

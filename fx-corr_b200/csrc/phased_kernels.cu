@@ -22,17 +22,56 @@
 
 namespace fxc {
 
+// Per-CTA state that outlives one sector: the twiddle bases and the number of
+// staging iterations consumed so far (it sets the mbarrier slot and phase, so
+// a persistent CTA can run spans of several scans back to back).
+template <int N>
+struct PhasedCta {
+  Twiddles<N> tw;
+  uint32_t seq;
+};
+
 template <int N, int FPC>
-__global__ void __launch_bounds__(FPC * N / 16, (N >= 8192 ? 1 : 2))
-phased_kernel(const PhasedParams p) {
+__device__ __forceinline__ void phased_cta_init(uint8_t* smem, const SmemLayout& L,
+                                                PhasedCta<N>& c) {
+  constexpr int T1 = N / 16;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.off_bar);
+  int* flag = reinterpret_cast<int*>(smem + L.off_flag);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    *flag = 0;
+    fence_proxy_async();
+  }
+  c.tw.init(threadIdx.x % T1);
+  c.seq = 0;
+}
+
+// Never leave a bulk copy in flight into a finished CTA's shared memory.
+__device__ __forceinline__ void phased_cta_drain(uint8_t* smem, const SmemLayout& L) {
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.off_bar);
+  const int* flag = reinterpret_cast<const int*>(smem + L.off_flag);
+  if (threadIdx.x == 0 && *flag) {
+    for (int s = 0; s < kStages; ++s) mbar_wait(&bars[s], 0, kWaitPolls);
+  }
+}
+
+// CTA iterations [it0, it1) (FPC frame pairs each) of the sector p: phased
+// power per bin into part[H] (f32 registers, f64 flushes) and, with
+// p.want_raw, the re-quantised frames at p.raw_out.  Returns false when a
+// bounded wait gave up (the CTA must stop).  Compiled once (not inlined) and
+// called by both the single-scan and the batched kernel, so that a frame's
+// .raw bytes do not depend on which of them computed it: two inlined copies
+// may contract or schedule the floating-point operations differently, which
+// moves samples that sit on a quantiser decision boundary.
+template <int N, int FPC>
+__device__ __noinline__ bool phased_span(const PhasedParams& p, uint64_t it0, uint64_t it1,
+                                            double* part, uint8_t* smem, const SmemLayout& L,
+                                            PhasedCta<N>& c) {
   constexpr int T1 = N / 16;
   constexpr int T = FPC * T1;
-  constexpr int H = N / 2 + 1;
   constexpr int BPT = (N / 2) / T;
   static_assert(BPT * T == N / 2 && BPT >= 2, "bins per thread");
 
-  extern __shared__ __align__(128) uint8_t smem[];
-  const SmemLayout L = smem_layout<N, FPC>(p.stage_bytes);
   float2* bufA = reinterpret_cast<float2*>(smem + L.off_a);
   float2* bufB = reinterpret_cast<float2*>(smem + L.off_b);
   uint8_t* stage = smem + L.off_stage;
@@ -48,29 +87,14 @@ phased_kernel(const PhasedParams p) {
   const int tid = threadIdx.x;
   const int g = tid / T1;
   const int t = tid % T1;
+  const Twiddles<N>& tw = c.tw;
+  const uint32_t seq0 = c.seq;
 
-  for (int i = tid; i < 512; i += T) lv[i] = p.st[i >> 8].levels[i & 255] * p.st[i >> 8].scale;
-  for (int s = 0; s < 2; ++s)
-    if (p.st[s].shkind == SH_GENERIC)
-      for (int i = tid; i < 1024; i += T) lut[s * 1024 + i] = p.st[s].shlut[i];
-  for (int i = tid; i < 256; i += T) ql[i] = i < (int)p.nqlevels ? p.qlevels[i] : 0.f;
-  for (int i = tid; i < 1024; i += T) elut[i] = p.enc_lut[i];
-  if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
-    *flag = 0;
-    fence_proxy_async();
-  }
-  Twiddles<N> tw;
-  tw.init(t);
-
-  const uint64_t iters = (p.nf + FPC - 1) / FPC;
-  const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
-  const uint64_t it1 = ((blockIdx.x + 1) * iters) / gridDim.x;
   const uint32_t bpf1 = p.st[0].bpf, bpf2 = p.st[1].bpf;
   constexpr uint32_t kRaw1 = FPC * kFiBytes;
 
   auto issue = [&](uint64_t it) {
-    const int slot = (int)((it - it0) % kStages);
+    const int slot = (int)((seq0 + (uint32_t)(it - it0)) % kStages);
     const uint64_t f0 = it * FPC;
     const uint64_t nvalid = (p.nf - f0) < (uint64_t)FPC ? (p.nf - f0) : (uint64_t)FPC;
     const uint32_t bf = (uint32_t)(nvalid * kFiBytes);
@@ -81,9 +105,21 @@ phased_kernel(const PhasedParams p) {
     bulk_g2s(dst + kRaw1, p.st[0].raw + f0 * bpf1, b1, &bars[slot]);
     bulk_g2s(dst + kRaw1 + FPC * bpf1, p.st[1].raw + f0 * bpf2, b2, &bars[slot]);
   };
+  // The previous span, if any, is past its last reads of the staging ring and
+  // the tables: the first frames' copies go out, the tables are built while
+  // they are in flight.
   __syncthreads();
-  if (tid == 0)
+  if (tid == 0) {
+    fence_proxy_async();
     for (uint64_t it = it0; it < it1 && it < it0 + kStages; ++it) issue(it);
+  }
+  for (int i = tid; i < 512; i += T) lv[i] = p.st[i >> 8].levels[i & 255] * p.st[i >> 8].scale;
+  for (int s = 0; s < 2; ++s)
+    if (p.st[s].shkind == SH_GENERIC)
+      for (int i = tid; i < 1024; i += T) lut[s * 1024 + i] = p.st[s].shlut[i];
+  for (int i = tid; i < 256; i += T) ql[i] = i < (int)p.nqlevels ? p.qlevels[i] : 0.f;
+  for (int i = tid; i < 1024; i += T) elut[i] = p.enc_lut[i];
+  __syncthreads();
 
   float acc[BPT + 1];
 #pragma unroll
@@ -95,7 +131,6 @@ phased_kernel(const PhasedParams p) {
   const float u1 = 0.5f / p.st[0].scale, u2 = 0.5f / p.st[1].scale;
   bool first_flush = true;
   uint32_t since_flush = 0;
-  double* part = p.partials + (size_t)blockIdx.x * H;
   const uint32_t spw = 32u / p.bits_out;           // samples per packed word
   const uint32_t wpf = (uint32_t)N / spw;          // words per output frame
   const uint32_t qmask = (p.bits_out >= 32) ? 0xFFFFFFFFu : ((1u << p.bits_out) - 1u);
@@ -113,9 +148,11 @@ phased_kernel(const PhasedParams p) {
     since_flush = 0;
   };
 
+  bool ok = true;
   for (uint64_t it = it0; it < it1; ++it) {
-    const int slot = (int)((it - it0) % kStages);
-    const uint32_t parity = (uint32_t)(((it - it0) / kStages) & 1u);
+    const uint32_t q_it = seq0 + (uint32_t)(it - it0);
+    const int slot = (int)(q_it % kStages);
+    const uint32_t parity = (q_it / kStages) & 1u;
     const uint64_t frame_local = it * FPC + g;
     const bool valid = frame_local < p.nf;
 
@@ -130,7 +167,10 @@ phased_kernel(const PhasedParams p) {
                     lut + 1024, tid, T);
     if (t == 0 && valid) finfo[g] = reinterpret_cast<const FrameInfo*>(st)[g];
     __syncthreads();
-    if (*flag) break;
+    if (*flag) {
+      ok = false;
+      break;
+    }
     const int s1 = valid ? finfo[g].s1 : 0;
     const int s2 = valid ? finfo[g].s2 : 0;
     const PackedStation pa{w1 + g * (bpf1 / 4), lv, (uint32_t)p.st[0].bits,
@@ -244,9 +284,51 @@ phased_kernel(const PhasedParams p) {
     __syncthreads();
   }
   if (since_flush > 0 || first_flush) flush();
-  if (tid == 0 && *flag) {
-    for (int s = 0; s < kStages; ++s) mbar_wait(&bars[s], 0, kWaitPolls);
+  c.seq = seq0 + (uint32_t)(it1 - it0);
+  return ok;
+}
+
+template <int N, int FPC>
+__global__ void __launch_bounds__(FPC * N / 16, (N >= 8192 ? 1 : 2))
+phased_kernel(const __grid_constant__ PhasedParams p) {
+  constexpr int H = N / 2 + 1;
+  extern __shared__ __align__(128) uint8_t smem[];
+  const SmemLayout L = smem_layout<N, FPC>(p.stage_bytes);
+  PhasedCta<N> c;
+  phased_cta_init<N, FPC>(smem, L, c);
+  const uint64_t iters = (p.nf + FPC - 1) / FPC;
+  const uint64_t it0 = (blockIdx.x * iters) / gridDim.x;
+  const uint64_t it1 = ((blockIdx.x + 1) * iters) / gridDim.x;
+  phased_span<N, FPC>(p, it0, it1, p.partials + (size_t)blockIdx.x * H, smem, L, c);
+  phased_cta_drain(smem, L);
+}
+
+// Batched: a persistent grid takes the items of batch group `grp` by ticket;
+// an item is a frame range of one scan's phased sector (its own tables, frame
+// records, raw words and .raw output) with its own H partials.  The layout is
+// sized for 8-bit stations, so one launch serves every bit depth, and every
+// frame is computed exactly as by phased_kernel.
+template <int N, int FPC>
+__global__ void __launch_bounds__(FPC * N / 16, (N >= 8192 ? 1 : 2))
+phased_batch_kernel(const BatchArgs a, int grp) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const SmemLayout L = smem_layout<N, FPC>(2u * FPC * N);
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(smem + L.off_flag + 4);
+  PhasedCta<N> c;
+  phased_cta_init<N, FPC>(smem, L, c);
+  const uint32_t n_items = a.hdr->nitems[grp];
+  const BatchItem* items = a.hdr->items + a.hdr->item0[grp];
+  const BatchScan* scans = a.hdr->scans;
+  for (;;) {
+    if (threadIdx.x == 0) *ticket = atomicAdd(&a.hdr->ticket[grp], 1u);
+    __syncthreads();
+    const uint32_t k = *ticket;  // phased_span opens with a barrier before the next write
+    if (k >= n_items) break;
+    const BatchItem w = items[k];
+    const uint64_t it0 = w.f0 / FPC, it1 = (w.f1 + FPC - 1) / FPC;
+    if (!phased_span<N, FPC>(scans[w.scan].pp, it0, it1, a.partials + w.part, smem, L, c)) break;
   }
+  phased_cta_drain(smem, L);
 }
 
 // Fixed-order sum of the per-CTA phased partials into acc[4H, 5H).
@@ -293,6 +375,67 @@ cudaError_t launch_phased(uint32_t n, const PhasedParams& p, int grid, cudaStrea
     case 8192: return launch_phased_one<8192, 1>(p, grid, s);
     default: return cudaErrorInvalidValue;
   }
+}
+
+namespace {
+template <int N, int FPC>
+uint32_t phased_batch_smem() {
+  return smem_layout<N, FPC>(2u * FPC * N).total + 1024 + 4096;
+}
+}  // namespace
+
+// Batch groups of the phased kernels: FFT 1024 / 2048 / 4096 / 8192 with the
+// single-scan kernels' frames per CTA iteration (4 / 2 / 1 / 1).
+cudaError_t phased_batch_prepare(uint32_t n) {
+  switch (n) {
+    case 1024: return cudaFuncSetAttribute(phased_batch_kernel<1024, 4>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)phased_batch_smem<1024, 4>());
+    case 2048: return cudaFuncSetAttribute(phased_batch_kernel<2048, 2>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)phased_batch_smem<2048, 2>());
+    case 4096: return cudaFuncSetAttribute(phased_batch_kernel<4096, 1>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)phased_batch_smem<4096, 1>());
+    case 8192: return cudaFuncSetAttribute(phased_batch_kernel<8192, 1>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)phased_batch_smem<8192, 1>());
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int phased_batch_ctas_per_sm(uint32_t n) {
+  int nb = 0;
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (n) {
+    case 1024: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, phased_batch_kernel<1024, 4>,
+                                                                 256, phased_batch_smem<1024, 4>());
+      break;
+    case 2048: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, phased_batch_kernel<2048, 2>,
+                                                                 256, phased_batch_smem<2048, 2>());
+      break;
+    case 4096: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, phased_batch_kernel<4096, 1>,
+                                                                 256, phased_batch_smem<4096, 1>());
+      break;
+    case 8192: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, phased_batch_kernel<8192, 1>,
+                                                                 512, phased_batch_smem<8192, 1>());
+      break;
+    default: break;
+  }
+  return e == cudaSuccess ? nb : 0;
+}
+
+int phased_frames_per_cta_iter(uint32_t n) { return n == 1024 ? 4 : (n == 2048 ? 2 : 1); }
+
+cudaError_t launch_phased_batch(uint32_t n, const BatchArgs& a, int grp, int grid, cudaStream_t s) {
+  switch (n) {
+    case 1024: phased_batch_kernel<1024, 4><<<grid, 256, phased_batch_smem<1024, 4>(), s>>>(a, grp); break;
+    case 2048: phased_batch_kernel<2048, 2><<<grid, 256, phased_batch_smem<2048, 2>(), s>>>(a, grp); break;
+    case 4096: phased_batch_kernel<4096, 1><<<grid, 256, phased_batch_smem<4096, 1>(), s>>>(a, grp); break;
+    case 8192: phased_batch_kernel<8192, 1><<<grid, 512, phased_batch_smem<8192, 1>(), s>>>(a, grp); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t launch_reduce_phased(const double* part, int nblk, int h, double* out, cudaStream_t s) {

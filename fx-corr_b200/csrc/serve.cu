@@ -161,7 +161,7 @@ fxc_status run_job(fxc_server* sv, fxc_scan** sp, Job* J) {
     if (st == FXC_OK) J->stats.sectors += 1;
     return st;
   };
-  if (sv->batch && !(cfg.products & FXC_PROD_RAW)) {
+  if (sv->batch) {
     // batched: stage, post to the dispatcher, collect behind its batch
     std::deque<std::pair<Posted, uint64_t>> posts;  // (post, sector index)
     std::condition_variable cv_mine;  // the dispatcher wakes this worker only
@@ -310,6 +310,7 @@ void dispatcher(fxc_server* sv) {
   std::vector<const uint8_t*> r1, r2;
   std::vector<uint64_t> nfs, firsts;
   std::vector<double*> accs;
+  std::vector<uint8_t*> raws;
   for (;;) {
     {
       std::unique_lock<std::mutex> lk(sv->mu);
@@ -344,6 +345,7 @@ void dispatcher(fxc_server* sv) {
     nfs.clear();
     firsts.clear();
     accs.clear();
+    raws.clear();
     for (Posted* p : take) {
       cudaStreamWaitEvent(sv->disp_stream, p->ss.h2d, 0);
       scans.push_back(p->s);
@@ -352,17 +354,19 @@ void dispatcher(fxc_server* sv) {
       nfs.push_back(p->nf);
       firsts.push_back(p->first);
       accs.push_back(p->ss.d_acc);
+      raws.push_back(p->ss.d_raw_out);
     }
-    fxc_status st = fxc_batch_run_device(sv->batch, scans.data(), r1.data(), r2.data(), nfs.data(),
-                                         firsts.data(), accs.data(), (uint32_t)take.size(),
-                                         sv->disp_stream);
+    fxc_status st = fxc_batch_run_device_raw(sv->batch, scans.data(), r1.data(), r2.data(),
+                                             nfs.data(), firsts.data(), accs.data(), raws.data(),
+                                             (uint32_t)take.size(), sv->disp_stream);
     std::string err;
     if (st == FXC_EBUSY || st == FXC_ENOMEM) {
       // no room for the batch's tables: each sector on its scan's own buffers
       st = FXC_OK;
       for (Posted* p : take) {
         const fxc_status s1 = fxc::run_sector_internal(p->s, p->ss.d_raw1, p->ss.d_raw2, p->nf,
-                                                       p->first, p->ss.d_acc, sv->disp_stream);
+                                                       p->first, p->ss.d_acc, p->ss.d_raw_out,
+                                                       sv->disp_stream);
         if (s1 != FXC_OK) {
           st = s1;
           break;

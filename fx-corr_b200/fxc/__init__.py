@@ -38,7 +38,8 @@ EXPORTS = [
     "fxc_host_alloc", "fxc_host_free", "fxc_batch_create", "fxc_batch_destroy",
     "fxc_batch_run_device", "fxc_batch_autotune", "fxc_batch_shape", "fxc_batch_launches",
     "fxc_batch_set_shape", "fxc_sector_noalloc_check", "fxc_debug_inject_wait_timeout",
-    "fxc_host_register", "fxc_host_unregister",
+    "fxc_host_register", "fxc_host_unregister", "fxc_batch_run_device_raw",
+    "fxc_probe_exchange", "fxc_probe_mma_f16",
 ]
 NOALLOC_MAX_FRAMES = 32768
 
@@ -160,6 +161,8 @@ def lib():
         "fxc_normalize": ([C.c_uint32, C.c_uint64, C.c_double, f64p, f64p, vp], st),
         "fxc_bytes_per_frame": ([C.c_uint32, C.c_uint32], C.c_uint64),
         "fxc_probe_fp32_peak": ([C.c_int32, f64p], st),
+        "fxc_probe_exchange": ([C.c_int32, f64p, f64p], st),
+        "fxc_probe_mma_f16": ([C.c_int32, f64p], st),
         "fxc_scan_set_profiling": ([vp, C.c_int32], st),
         "fxc_sector_run_device_noalloc": ([C.POINTER(ScanCfgC), vp, vp, C.c_uint64, C.c_uint64,
                                            vp, vp], st),
@@ -180,6 +183,9 @@ def lib():
         "fxc_batch_run_device": ([vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
                                   C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(vp),
                                   C.c_uint32, vp], st),
+        "fxc_batch_run_device_raw": ([vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                      C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                      C.POINTER(vp), C.POINTER(vp), C.c_uint32, vp], st),
         "fxc_batch_autotune": ([vp, C.c_uint32], st),
         "fxc_batch_shape": ([vp, C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_uint32),
                              C.POINTER(C.c_int32), f64p], st),
@@ -461,6 +467,19 @@ class Batch:
             VP(*[_ptr(x) for x in d_raw2]), U64(*nf), U64(*first_frame),
             VP(*[_ptr(x) for x in d_acc]), n, _stream(stream)))
 
+    def run_device_raw(self, scans, d_raw1, d_raw2, nf, first_frame, d_acc, d_raw_out,
+                       stream=None):
+        """run_device with phased .raw outputs: d_raw_out[i] is a device buffer
+        (or None) for scan i's re-quantised frames."""
+        n = len(scans)
+        VP = C.c_void_p * n
+        U64 = C.c_uint64 * n
+        check(lib().fxc_batch_run_device_raw(
+            self.h, VP(*[s.h.value for s in scans]), VP(*[_ptr(x) for x in d_raw1]),
+            VP(*[_ptr(x) for x in d_raw2]), U64(*nf), U64(*first_frame),
+            VP(*[_ptr(x) for x in d_acc]), VP(*[_ptr(x) for x in d_raw_out]), n,
+            _stream(stream)))
+
     def autotune(self, fft: int):
         check(lib().fxc_batch_autotune(self.h, fft))
 
@@ -619,6 +638,21 @@ def debug_inject_wait_timeout(wait_polls: int = 0, withhold_copies: bool = False
     `withhold_copies`, let them run out with no copy in flight.  (0, False)
     restores normal operation."""
     check(lib().fxc_debug_inject_wait_timeout(wait_polls, int(bool(withhold_copies))))
+
+
+def probe_exchange(device: int = 0) -> dict:
+    """fxc_probe_exchange: ns for one SM to redistribute 8192 complex values
+    among 512 threads through shared memory and by warp shuffles."""
+    a, b = C.c_double(), C.c_double()
+    check(lib().fxc_probe_exchange(device, C.byref(a), C.byref(b)))
+    return {"smem_ns": a.value, "shfl_ns": b.value}
+
+
+def probe_mma_f16(device: int = 0) -> float:
+    """fxc_probe_mma_f16: mma.sync m16n8k16 f16 throughput (TFLOP/s)."""
+    out = C.c_double()
+    check(lib().fxc_probe_mma_f16(device, C.byref(out)))
+    return out.value
 
 
 def probe_fp32_peak(device: int = 0) -> float:

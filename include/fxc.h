@@ -289,10 +289,13 @@ FXC_API fxc_status fxc_server_destroy(fxc_server* sv);
  * CTA iteration and frames per work item of each FFT length come from an
  * autotuner that times the kernel variants on a synthetic batch (at first use
  * of the length when opts.autotune is set, or by fxc_batch_autotune).
- * Sectors the batch kernels do not cover (phased products, FFT lengths above
- * 16384, FFT 16384 with an odd band shift, empty sectors) run through the
- * per-scan path on the same stream.  A sector's products equal
- * fxc_sector_run_device's within the library's FP32 tolerance, and are
+ * Phased sectors (yi-phasedarray: phased power and .raw frames, FFT
+ * 1024..8192) run in persistent phased kernels of the same batch.  Sectors the
+ * batch kernels do not cover (phased products above FFT 8192, correlation
+ * above 16384, FFT 16384 with an odd band shift, scans with both correlation
+ * and phased products, empty sectors) run through the per-scan path on the
+ * same stream.  A sector's products equal fxc_sector_run_device's within the
+ * library's FP32 tolerance (phased .raw frames byte for byte), and are
  * identical bit for bit whatever else shares the batch (the item split
  * depends only on the sector's frame count and the batch's tuning). */
 typedef struct fxc_batch fxc_batch;
@@ -315,6 +318,15 @@ FXC_API fxc_status fxc_batch_run_device(fxc_batch* b, fxc_scan* const* scans,
                                         const uint8_t* const* d_raw2, const uint64_t* nf,
                                         const uint64_t* first_frame, double* const* d_acc,
                                         uint32_t count, void* stream);
+/* The same with phased .raw output: d_raw_out[i] (nf[i] * bytes_per_frame(
+ * bits_out) device bytes) receives scan i's re-quantised phased frames when
+ * the scan has FXC_PROD_RAW (NULL entries for the other scans). */
+FXC_API fxc_status fxc_batch_run_device_raw(fxc_batch* b, fxc_scan* const* scans,
+                                            const uint8_t* const* d_raw1,
+                                            const uint8_t* const* d_raw2, const uint64_t* nf,
+                                            const uint64_t* first_frame, double* const* d_acc,
+                                            uint8_t* const* d_raw_out, uint32_t count,
+                                            void* stream);
 /* Times every kernel variant x work-item size of one FFT length (1024..16384)
  * on a synthetic 2-bit batch and keeps the fastest (blocks the host for tens
  * of milliseconds). */
@@ -380,6 +392,14 @@ FXC_API fxc_status fxc_normalize(uint32_t fft, uint64_t nf, double level_power, 
 FXC_API uint64_t fxc_bytes_per_frame(uint32_t fft, uint32_t bits);
 /* Measured FP32 FMA throughput of the device (TFLOP/s), for rooflines. */
 FXC_API fxc_status fxc_probe_fp32_peak(int32_t device, double* tflops);
+/* Design-choice probes (no reference counterpart), measured on `device`:
+ * smem_ns / shfl_ns = time for one SM to redistribute a frame's 8192 complex
+ * values among 512 threads (16 per thread) through padded shared memory
+ * (the exchange between two radix-16 passes) / by warp shuffles (a 16 x 16
+ * transpose within each half-warp); tflops = throughput of mma.sync m16n8k16
+ * (f16 inputs, f32 accumulation) over the whole GPU. */
+FXC_API fxc_status fxc_probe_exchange(int32_t device, double* smem_ns, double* shfl_ns);
+FXC_API fxc_status fxc_probe_mma_f16(int32_t device, double* tflops);
 
 #ifdef __cplusplus
 }

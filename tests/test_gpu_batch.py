@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 import oracle
-from _cases import assert_sector_close, make_scan, signal_raw, spectral_errors, to_fxc
+from _cases import (assert_sector_close, assert_spectra_close, make_scan, signal_raw,
+                    spectral_errors, to_fxc)
 
 pytestmark = pytest.mark.gpu
 
@@ -234,3 +235,86 @@ def test_batch_errors(fxc_lib, engine, mix):
     s2.close()
     other.close()
     b.close()
+
+
+PHASED = oracle.PROD_PHASED | oracle.PROD_RAW
+PH_MIX = [
+    (dict(fft=1024, bits1=2, bits2=2, shuffle="generic", lsb1=True, band=(8, 0, 504, 8),
+          products=PHASED), 300),
+    (dict(fft=2048, bits1=1, bits2=4, shuffle="pairswap", band=(-16, 16, 1024, 0), grid=1,
+          products=PHASED, w1=0.7, w2=1.3), 77),
+    (dict(fft=4096, bits1=2, bits2=2, lsb1=True, lsb2=True, band=(40, 0, 2008, 40),
+          products=PHASED), 129),
+    (dict(fft=8192, bits1=2, bits2=8, shuffle="generic", band=(64, 0, 4032, 64),
+          products=PHASED), 95),
+    (dict(fft=8192, bits1=2, bits2=2, band=(0, 0, 4096, 0), products=oracle.PROD_PHASED), 40),
+    # per-scan path inside the same call: phased above FFT 8192, with .raw
+    (dict(fft=16384, bits1=2, bits2=2, band=(128, 0, 8064, 128), products=PHASED), 9),
+    # a correlation sector beside them
+    (dict(fft=4096, bits1=2, bits2=2, shuffle="generic", band=(40, 0, 2008, 40)), 200),
+]
+
+
+def run_raw(batch, items):
+    import torch
+
+    accs = [torch.empty(5 * it["scan"].h, dtype=torch.float64, device="cuda") for it in items]
+    raws = [torch.full((max(1, it["nf"] * it["scan"].bpf(it["scan"].bits_out)),), 0xA5,
+                       dtype=torch.uint8, device="cuda")
+            if it["scan"].products & oracle.PROD_RAW else None for it in items]
+    batch.run_device_raw([it["s"] for it in items], [it["d1"] for it in items],
+                         [it["d2"] for it in items], [it["nf"] for it in items],
+                         [it["first"] for it in items], accs, raws)
+    torch.cuda.synchronize()
+    out = []
+    for it, a, r in zip(items, accs, raws):
+        it["s"].check()
+        h = it["scan"].h
+        a = a.cpu().numpy()
+        d = dict(acf11=a[:h], acf22=a[h:2 * h], xcf=a[2 * h:4 * h].view(np.complex128),
+                 phased=a[4 * h:])
+        if r is not None:
+            d["raw"] = r.cpu().numpy()[: it["nf"] * it["scan"].bpf(it["scan"].bits_out)]
+        out.append(d)
+    return out
+
+
+def test_batch_phased_sectors(fxc_lib, engine):
+    """yi-phasedarray sectors in the phased batch kernels: .raw frames equal
+    the per-scan path's byte for byte, the phased power within the FP32
+    tolerance of it (and of the FP64 oracle), correlation columns zero; each
+    sector's products identical alone and in the mix, with graphs or not."""
+    items = build(engine, PH_MIX, seed0=300)
+    b = fxc_lib.Batch(engine)
+    got = run_raw(b, items)
+    for it, g in zip(items, got):
+        sc = it["scan"]
+        one = it["s"].sector_device(it["d1"], it["d2"], it["nf"], first_frame=it["first"])
+        if sc.products & oracle.PROD_RAW:
+            assert np.array_equal(g["raw"], one["raw"]), sc.fft
+        if sc.products & oracle.PROD_PHASED:
+            assert_spectra_close(g["phased"], one["phased"], f"batched phased {sc.fft}")
+            assert all(np.all(g[k] == 0) for k in ("acf11", "acf22", "xcf"))
+            if sc.fft <= 4096:
+                ref = oracle.fp64_sector_phased(sc, it["r1"], it["r2"], it["nf"],
+                                                first_frame=it["first"])
+                assert_spectra_close(g["phased"], ref["phased"], f"phased vs fp64 {sc.fft}")
+        else:
+            for k in ("acf11", "acf22", "xcf"):
+                assert_spectra_close(g[k], one[k], f"correlation beside phased {k}")
+    # alone == in the mix, and graph replay
+    bg = fxc_lib.Batch(engine, use_graphs=True)
+    for k in range(len(items)):
+        alone = run_raw(fxc_lib.Batch(engine), [items[k]])[0]
+        for key in ("acf11", "acf22", "xcf", "phased"):
+            assert np.array_equal(alone[key], got[k][key]), (k, key)
+        if "raw" in alone:
+            assert np.array_equal(alone["raw"], got[k]["raw"])
+    for _ in range(2):
+        again = run_raw(bg, items)
+        for g0, g1 in zip(got, again):
+            for key in g0:
+                assert np.array_equal(g0[key], g1[key]), key
+    bg.close()
+    b.close()
+    close(items)
