@@ -386,7 +386,10 @@ fxc_status run_large(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t
   const LargeParams p = large_params(s, r1, r2);
   PhasedParams pp{};
   if (phased) pp = phased_params(s, r1, r2, nf, first, d_raw_out);
-  const int groups = (int)std::min<uint64_t>((uint64_t)kLargeGroups, s->big_frames);
+  // frame groups of a batch (one f64 partial row each): as few as keep every
+  // group within 32 frames, the f32 run length of the accumulation kernels
+  const int groups = (int)std::max<uint64_t>(
+      1, std::min<uint64_t>((uint64_t)kLargeGroups, (s->big_frames + 31) / 32));
   double* part_ph = s->d_partials + (uint64_t)kLargeGroups * 4 * h;
   bool first_batch = true;
   for (uint64_t f0 = 0; f0 < nf; f0 += s->big_frames) {

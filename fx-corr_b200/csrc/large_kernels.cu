@@ -5,12 +5,21 @@
 // radix-C step over the frame followed by C shared-memory FFTs of M points:
 //   y_q[m] = W_N^(m q) * sum_c z[m + M c] W_C^(c q),   Z[C k + q] = FFT_M(y_q)[k].
 // Kernels, per batch of frames held in device scratch:
-//   decode_global_kernel  decode + LSB flip + integer shift -> z   (src/utils.rs:126-376)
-//   dif_kernel<C>         the radix-C step with its twiddles    -> y
-//   cfft_kernel<M>        M-point Stockham FFT per row            -> Z (row q, column k)
+//   rows_fft_kernel<C>    C = 2: decode + shift + radix-C step + row FFT fused,
+//                         one (frame, row) per CTA iteration, the frame's packed words
+//                         staged in shared memory by bulk copies             -> Z
+//   dif_staged_kernel<C>  C = 4, 8: decode + shift (src/utils.rs:126-376) + radix-C
+//                         step from the frame's words staged in shared memory -> y
+//   cfft_kernel<M>        M-point Stockham FFT per row, the next row prefetched by
+//                         a bulk copy                                         -> Z
 //   acc_global_kernel     two-for-one split, band alignment, fringe x ramp rotation and
-//                         ACF/XCF accumulation (src/main.rs:2491-2568) per bin, in f64,
-//                         into per-frame-group partials reduced by reduce_partials_kernel.
+//                         ACF/XCF accumulation (src/main.rs:2491-2568) per bin, f32 over
+//                         each frame group (<= 32 frames), then f64 per-group partials
+//                         reduced by reduce_partials_kernel.
+//   phased_global_kernel  per-bin phased synthesis (src/main.rs:2222-2365) and the
+//                         Hermitian-extended inverse input; rows_fft_complex_kernel<C>
+//                         (C <= 4) or dif_kernel + cfft_kernel its FFT; quant_global_kernel
+//                         the re-quantised .raw frames (src/utils.rs:378-410).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -70,119 +79,491 @@ __global__ void decode_global_kernel(const LargeParams p, uint64_t f0, uint64_t 
   }
 }
 
-// Per-station decode plan of decode_dif_kernel: for a station whose samples
-// are contiguous runs of word bits after the shuffle (1- and 2-bit stations
-// under any shuffle, wider ones unshuffled), sample slot c of a word is read
-// with one or two shifts: code = (w >> p0) & mask, or, for a 2-bit sample whose
-// two bits the shuffle separates or swaps, ((w >> p0) & 1) | ((w >> p1) & 1) << 1.
-// Bit j of slot c's code is word bit perm[c b + j] (src/utils.rs:159-171).
-struct ShiftPlan {
-  uint32_t p0[32], p1[32];
-  uint32_t split;  // bit c: slot c takes two shifts
-};
+// ---------------------------------------------- fused decode + DIF + row FFT
+//
+// One work item = one row q of one frame: the frame's packed words are staged
+// in shared memory by bulk copies (the next item's copies in flight while this
+// one computes), thread t decodes its 16 column inputs m = t + 512 r straight
+// from the words for every segment c (samples m + M c of both stations, the
+// integer shifts and zero fill applied at the sample index), forms the
+// radix-C decimation-in-frequency input
+//   y_q[m] = W_N^(m q) * sum_c z[m + M c] W_C^(c q),   z = x1 + i x2,
+// and runs the M-point Stockham FFT of the row in shared memory; the row's
+// spectrum Z[C k + q] goes to y[f][q M + k], the layout acc_global_kernel and
+// the phased kernels read.  This replaces a decode + DIF kernel and cfft_kernel (two
+// round trips of the complex frame through global memory) when the frame's
+// words fit the staging space.
 
-__device__ __forceinline__ bool shift_decodable(const StationParams& q) {
-  return q.bits <= 2 || q.shkind == SH_IDENTITY;
+// Shared-memory layout (bytes): level tables (station 1 at 0, station 2 at
+// 2048, 2^b f32 each then their negations), rotate amounts, mbarriers, error
+// flag, byte LUTs of 4/8-bit generic shuffles, the two padded FFT buffers,
+// then the staging slots [FrameInfo (128 B)][station 1 words][station 2 words].
+constexpr uint32_t kRwPos = 4096, kRwBar = 4352, kRwFlag = 4384, kRwLut = 4608;
+constexpr uint32_t kRwA = kRwLut + 8192;
+constexpr uint32_t kRwBuf = (uint32_t)Geom<kLargeM>::CSTRIDE * (uint32_t)sizeof(float2);
+constexpr uint32_t kRwStage0 = kRwA + 2 * kRwBuf;
+constexpr uint32_t kRwMaxSmem = 232448;  // 227 KB per CTA on sm_100
+
+__host__ __device__ inline uint32_t rows_stage_stride(uint32_t bpf1, uint32_t bpf2) {
+  return (128u + bpf1 + bpf2 + 127u) & ~127u;
 }
 
-__device__ __forceinline__ void build_shift_plan(const StationParams& q, ShiftPlan& sp, int i) {
-  const int b = q.bits, spw = 32 / b;
-  if (i >= spw) return;
-  const bool natural = q.shkind == SH_IDENTITY;
-  const uint32_t p0 = natural ? (uint32_t)(i * b) : q.perm[i * b];
-  const uint32_t p1 = b == 2 ? (natural ? (uint32_t)(i * b + 1) : q.perm[i * b + 1]) : 0u;
-  sp.p0[i] = p0;
-  sp.p1[i] = p1;
-  if (b == 2 && p1 != p0 + 1) atomicOr(&sp.split, 1u << i);
+// Staging slots that fit: 2 (copies overlap the previous item) or 1; 0 = the
+// frame does not fit (the two-kernel path runs instead).
+__host__ __device__ inline int rows_stages(uint32_t bpf1, uint32_t bpf2) {
+  const uint32_t st = rows_stage_stride(bpf1, bpf2);
+  if (kRwStage0 + 2 * st <= kRwMaxSmem) return 2;
+  if (kRwStage0 + st <= kRwMaxSmem) return 1;
+  return 0;
 }
 
-// Decode + shift fused with the first (radix-C, decimation in frequency)
-// step of the four-step FFT: thread (frame, m) decodes samples m + M c of both
-// stations (z = x1 + i x2, station 2 negated on odd frames as in
-// decode_global_kernel), combines them with a C-point DFT and writes row q,
-// column m twiddled by W_N^(m q) — the complex frame never goes to HBM.
-// M is a whole number of words, so the C samples of a column sit in the same
-// slot of C words: the slot's shifts are looked up once per station.
-template <int C>
-__global__ void decode_dif_kernel(const LargeParams p, uint64_t f0, uint64_t nb,
-                                  float2* __restrict__ y) {
-  __shared__ uint32_t lut[2048];
-  __shared__ float lv[512];
-  __shared__ ShiftPlan plan[2];
-  for (int i = threadIdx.x; i < 512; i += blockDim.x)
-    lv[i] = p.st[i >> 8].levels[i & 255] * p.st[i >> 8].scale;
-  for (int s = 0; s < 2; ++s)
-    if (p.st[s].shkind == SH_GENERIC && !shift_decodable(p.st[s]))
-      for (int i = threadIdx.x; i < 1024; i += blockDim.x) lut[s * 1024 + i] = p.st[s].shlut[i];
-  if (threadIdx.x < 2) plan[threadIdx.x].split = 0;
-  __syncthreads();
-  for (int i = threadIdx.x; i < 64; i += blockDim.x)
-    if (shift_decodable(p.st[i >> 5])) build_shift_plan(p.st[i >> 5], plan[i >> 5], i & 31);
-  __syncthreads();
-  constexpr int M = kLargeM;
-  constexpr int N = C * M;
-  static_assert(M == 8192, "frame / column split by shifts");
-  const bool fast[2] = {shift_decodable(p.st[0]), shift_decodable(p.st[1])};
-  const uint64_t total = nb * (uint64_t)M;
-  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t fl = idx >> 13;
-    const int m = (int)(idx & (uint64_t)(M - 1));
-    const uint64_t f = f0 + fl;
-    const FrameInfo& F = p.finfo[f];
-    const bool odd = (f & 1u) != 0;
-    float xs[2][8];
+// Adds station ST's samples of the C segments to the 16 column inputs: x at
+// m0 + 512 r + M c (zero outside the frame) times W_C^(c q) (ST = 1: times
+// i W_C^(c q), the imaginary part of z).  The sample's bits are rotated to
+// byte-offset bits 2.. of the level table and merged with tbase (which picks
+// the station's table and the negated copy for odd samples of LSB input or
+// station 2 on odd frames), as in the FFT-8192 kernel.
+template <int C, int BITS, bool SPLIT, int ST>
+__device__ __forceinline__ void rows_station(const uint32_t* __restrict__ words,
+                                             const uint8_t* lvbase, int m0, uint32_t rots,
+                                             uint32_t tbase, const float2 (&wq)[C],
+                                             float2 (&v)[16]) {
+  constexpr int M = kLargeM, N = C * M;
+  constexpr int SPW = 32 / BITS;
+  constexpr int LOG2_SPW = BITS == 1 ? 5 : (BITS == 2 ? 4 : (BITS == 4 ? 3 : 2));
+  constexpr int WSTEP = 512 / SPW, SEGW = M / SPW;
+  constexpr uint32_t OMASK = ((1u << BITS) - 1u) << 2;
+  const int w0 = m0 >> LOG2_SPW;  // floor division
+  const uint32_t r0 = rots & 31u, r1 = (rots >> 8) & 31u;
+  auto level = [&](uint32_t w) -> float {
+    uint32_t off;
+    if constexpr (SPLIT) {
+      off = (__funnelshift_r(w, w, r0) & 4u) | tbase;
+      off |= __funnelshift_r(w, w, r1) & 8u;
+    } else {
+      off = (__funnelshift_r(w, w, r0) & OMASK) | tbase;
+    }
+    return *reinterpret_cast<const float*>(lvbase + off);
+  };
+  auto add = [&](int r, int c, float x) {
+    if constexpr (ST == 0) {
+      v[r].x = fmaf(x, wq[c].x, v[r].x);
+      v[r].y = fmaf(x, wq[c].y, v[r].y);
+    } else {
+      v[r].x = fmaf(-x, wq[c].y, v[r].x);
+      v[r].y = fmaf(x, wq[c].x, v[r].y);
+    }
+  };
+  if ((unsigned)m0 < 512u) {
+    // every sample of this thread lies inside the frame
 #pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      const StationParams& q = p.st[s];
-      const uint8_t* fr = q.raw + f * q.bpf;
-      const int m0 = m - (s == 0 ? F.s1 : F.s2);
-      const float* lvs = lv + 256 * s;
-      if (fast[s]) {
-        const int b = q.bits, lg = b == 1 ? 5 : (b == 2 ? 4 : (b == 4 ? 3 : 2));
-        const uint32_t spw = 32u / (uint32_t)b, mask = (1u << b) - 1u;
-        const int c = m0 & (int)(spw - 1u);
-        const uint32_t p0 = plan[s].p0[c], p1 = plan[s].p1[c];
-        const bool split = (plan[s].split >> c) & 1u;
-        const int w0 = m0 >> lg;  // floor division
-        const uint32_t* words = reinterpret_cast<const uint32_t*>(fr);
-        const bool neg = q.lsb && (m0 & 1);  // M is even: the same parity on every row
+    for (int c = 0; c < C; ++c)
 #pragma unroll
-        for (int r = 0; r < C; ++r) {
-          const int mr = m0 + M * r;
-          float x = 0.f;
-          if ((unsigned)mr < (unsigned)N) {
-            const uint32_t w = words[w0 + r * (M >> lg)];
-            const uint32_t code = split ? (((w >> p0) & 1u) | (((w >> p1) & 1u) << 1))
-                                        : ((w >> p0) & mask);
-            x = lvs[code];
-            if (neg) x = -x;
-          }
-          xs[s][r] = x;
-        }
-      } else {
+      for (int r = 0; r < 16; ++r) add(r, c, level(words[w0 + r * WSTEP + c * SEGW]));
+  } else {
 #pragma unroll
-        for (int r = 0; r < C; ++r)
-          xs[s][r] = sample_at(fr, q.bits, q.shkind, lut + 1024 * s, lvs, q.lsb, m0 + M * r, N);
+    for (int c = 0; c < C; ++c)
+#pragma unroll
+      for (int r = 0; r < 16; ++r) {
+        const int m = m0 + r * 512 + c * M;
+        const bool in = (unsigned)m < (unsigned)N;
+        const float x = level(words[in ? w0 + r * WSTEP + c * SEGW : 0]);
+        add(r, c, in ? x : 0.0f);
       }
+  }
+}
+
+template <int C, int ST>
+__device__ __forceinline__ void rows_station_any(int bits, bool split, const uint32_t* words,
+                                                 const uint8_t* lvbase, int m0, uint32_t rots,
+                                                 uint32_t tbase, const float2 (&wq)[C],
+                                                 float2 (&v)[16]) {
+  switch (bits) {
+    case 1: rows_station<C, 1, false, ST>(words, lvbase, m0, rots, tbase, wq, v); break;
+    case 2:
+      if (split) rows_station<C, 2, true, ST>(words, lvbase, m0, rots, tbase, wq, v);
+      else rows_station<C, 2, false, ST>(words, lvbase, m0, rots, tbase, wq, v);
+      break;
+    case 4: rows_station<C, 4, false, ST>(words, lvbase, m0, rots, tbase, wq, v); break;
+    default: rows_station<C, 8, false, ST>(words, lvbase, m0, rots, tbase, wq, v); break;
+  }
+}
+
+template <int C>
+__global__ void __launch_bounds__(512, 1) rows_fft_kernel(const LargeParams p, uint64_t f0,
+                                                          uint64_t nb, float2* __restrict__ y) {
+  constexpr int M = kLargeM, N = C * M, T = M / 16;
+  extern __shared__ __align__(128) uint8_t smem[];
+  const int tid = threadIdx.x;
+  float* lv = reinterpret_cast<float*>(smem);
+  uint32_t* pos = reinterpret_cast<uint32_t*>(smem + kRwPos);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kRwBar);
+  int* flag = reinterpret_cast<int*>(smem + kRwFlag);
+  uint32_t* lut = reinterpret_cast<uint32_t*>(smem + kRwLut);
+  float2* bufA = reinterpret_cast<float2*>(smem + kRwA);
+  float2* bufB = reinterpret_cast<float2*>(smem + kRwA + kRwBuf);
+  uint8_t* stage = smem + kRwStage0;
+  const StationParams& s1 = p.st[0];
+  const StationParams& s2 = p.st[1];
+  const uint32_t bpf1 = s1.bpf, bpf2 = s2.bpf;
+  const uint32_t stride = rows_stage_stride(bpf1, bpf2);
+  const int stages = rows_stages(bpf1, bpf2);
+  // 4- and 8-bit stations with a non-identity shuffle are rewritten in place
+  // (byte LUTs); 1- and 2-bit stations are decoded from the raw words
+  const bool pre1 = s1.bits > 2 && s1.shkind != SH_IDENTITY;
+  const bool pre2 = s2.bits > 2 && s2.shkind != SH_IDENTITY;
+  const uint64_t items = nb * (uint64_t)C;
+
+  if (tid == 0) {
+    for (int k = 0; k < 2; ++k) mbar_init(&bars[k], 1);
+    *flag = 0;
+    fence_proxy_async();
+  }
+  for (int i = tid; i < 1024; i += T) {
+    const StationParams& q = (i < 512) ? s1 : s2;
+    const int n = 1 << q.bits, c2 = i & 511;
+    const float x = c2 < 2 * n ? q.levels[c2 & (n - 1)] * q.scale : 0.0f;
+    lv[i] = c2 >= n ? -x : x;
+  }
+  for (int i = tid; i < 64; i += T) {
+    // rotate amounts of sample slot c: bit j of the sample is word bit p_j
+    const int k = i >> 5, cc = i & 31;
+    const StationParams& q = k ? s2 : s1;
+    const int b = q.bits;
+    const bool natural = (k ? pre2 : pre1) || q.shkind == SH_IDENTITY;
+    uint32_t r = 0;
+    if (cc * b < 32) {
+      const int q0 = natural ? cc * b : q.perm[cc * b];
+      const int q1 = b >= 2 ? (natural ? cc * b + 1 : q.perm[cc * b + 1]) : 0;
+      r = (uint32_t)((q0 - 2) & 31) | ((uint32_t)((q1 - 3) & 31) << 8);
+    }
+    pos[i] = r;
+  }
+  for (int k = 0; k < 2; ++k) {
+    const StationParams& q = k ? s2 : s1;
+    if ((k ? pre2 : pre1) && q.shkind == SH_GENERIC)
+      for (int i = tid; i < 1024; i += T) lut[k * 1024 + i] = q.shlut[i];
+  }
+  auto split2 = [](const StationParams& q) {
+    if (q.bits != 2 || q.shkind == SH_IDENTITY) return false;
+    for (int cc = 0; cc < 16; ++cc)
+      if (q.perm[2 * cc + 1] != q.perm[2 * cc] + 1 || (q.perm[2 * cc] & 1)) return true;
+    return false;
+  };
+  const bool sp1 = split2(s1), sp2 = split2(s2);
+  Twiddles<M> tw;
+  tw.init(tid);
+
+  // item i of this CTA's sequence: batch item blockIdx.x + i * gridDim.x
+  auto item_of = [&](uint32_t i) { return (uint64_t)blockIdx.x + (uint64_t)i * gridDim.x; };
+  auto issue = [&](uint32_t i) {
+    const uint64_t f = f0 + item_of(i) / C;  // sector-local frame
+    const int slot = (int)(i % (uint32_t)stages);
+    uint8_t* dst = stage + slot * stride;
+    mbar_expect_tx(&bars[slot], kFiBytes + bpf1 + bpf2);
+    bulk_g2s(dst, p.finfo + f, kFiBytes, &bars[slot]);
+    bulk_g2s(dst + 128, s1.raw + f * bpf1, bpf1, &bars[slot]);
+    bulk_g2s(dst + 128 + bpf1, s2.raw + f * bpf2, bpf2, &bars[slot]);
+  };
+  __syncthreads();  // mbarriers and tables
+  if (tid == 0) {
+    fence_proxy_async();
+    for (uint32_t i = 0; i < (uint32_t)stages && item_of(i) < items; ++i) issue(i);
+  }
+  for (uint32_t i = 0; item_of(i) < items; ++i) {
+    const uint64_t it = item_of(i);
+    const uint64_t fl = it / C;          // batch-local frame
+    const int q = (int)(it % C);         // row
+    const int slot = (int)(i % (uint32_t)stages);
+    const uint32_t parity = (i / (uint32_t)stages) & 1u;
+    if (!mbar_wait(&bars[slot], parity, kWaitPolls)) {
+      atomicOr(flag, 1);
+      atomicOr(p.err, ERR_WAIT_TIMEOUT);
+    }
+    uint8_t* st = stage + slot * stride;
+    uint32_t* w1 = reinterpret_cast<uint32_t*>(st + 128);
+    uint32_t* w2 = reinterpret_cast<uint32_t*>(st + 128 + bpf1);
+    __syncthreads();  // every thread past its wait (and the flag visible)
+    if (*flag) break;
+    if (pre1 || pre2) {
+      preshuffle_slot(w1, bpf1 / 4, pre1 ? s1.shkind : SH_IDENTITY, lut, w2, bpf2 / 4,
+                      pre2 ? s2.shkind : SH_IDENTITY, lut + 1024, tid, T);
+      __syncthreads();
+    }
+    const FrameInfo* F = reinterpret_cast<const FrameInfo*>(st);
+    const uint64_t f = f0 + fl;
+    const int odd = (int)(f & 1u);  // station 2 enters odd frames negated
+    // radix-C weights W_C^(c q)
+    float2 wq[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const int e = (c * q) % C;
+      float sn, cs;
+      sincospif(-2.0f * (float)e / (float)C, &sn, &cs);
+      wq[c] = make_float2(cs, sn);
     }
     float2 v[16];
 #pragma unroll
-    for (int c = 0; c < C; ++c) v[c] = make_float2(xs[0][c], odd ? -xs[1][c] : xs[1][c]);
-    if constexpr (C == 2) {
-      dft2<0>(v);
-    } else if constexpr (C == 4) {
-      dft4<0>(v);
-    } else {
-      dft8<0>(v);
+    for (int r = 0; r < 16; ++r) v[r] = make_float2(0.f, 0.f);
+    {
+      const int m1 = tid - F->s1, m2 = tid - F->s2;
+      const int c1 = m1 & ((32 / s1.bits) - 1), c2 = m2 & ((32 / s2.bits) - 1);
+      const uint32_t tb1 = (uint32_t)((m1 & (s1.lsb ? 1 : 0)) << (s1.bits + 2));
+      const uint32_t tb2 = 2048u + (uint32_t)((((uint32_t)m2 & (uint32_t)(s2.lsb ? 1 : 0)) ^
+                                               (uint32_t)odd) << (s2.bits + 2));
+      rows_station_any<C, 0>(s1.bits, sp1, w1, smem, m1, pos[c1], tb1, wq, v);
+      rows_station_any<C, 1>(s2.bits, sp2, w2, smem, m2, pos[32 + c2], tb2, wq, v);
     }
-    float2* yf = y + fl * (uint64_t)N;
+    if (q > 0) {
+      // W_N^(m q), m = t + 512 r (m q < N)
 #pragma unroll
-    for (int q = 0; q < C; ++q) {
-      float2 val = v[out_pos<C>(q)];
-      if (q > 0) val = cmul(val, p.tw[m * q]);
-      yf[q * M + m] = val;
+      for (int r = 0; r < 16; ++r) v[r] = cmul(v[r], p.tw[(tid + 512 * r) * q]);
     }
+    __syncthreads();  // the staged words are consumed: refill the slot
+    if (tid == 0 && item_of(i + stages) < items) {
+      fence_proxy_async();
+      issue(i + stages);
+    }
+    dft16(v);
+    float2* dst = bufA + 17 * tid;  // cpad(16 t + r) = 17 t + r
+#pragma unroll
+    for (int r = 0; r < 16; ++r) dst[r] = v[out_pos<16>(r)];
+    const float2* Z = fft_rest<M>(bufA, bufB, tid, tw);
+    __syncthreads();
+    float4* out = reinterpret_cast<float4*>(y + fl * (uint64_t)N + (uint64_t)q * M);
+    const float4* zin = reinterpret_cast<const float4*>(Z);
+    for (int k = tid; k < M / 2; k += T) out[k] = zin[k];
+    __syncthreads();  // the buffers are free for the next item
+  }
+  if (tid == 0 && *flag) {
+    for (int k = 0; k < stages; ++k) mbar_wait(&bars[k], 0, kWaitPolls);
+  }
+}
+
+// Decode + shift + radix-C step with the frame's words staged in shared memory
+// (the C = 4 and 8 forward path, and frames too large for rows_fft_kernel's
+// staging): one frame per CTA iteration, thread t decodes its 16 columns
+// m = t + 512 r from the staged words (each sample once), forms the C-point
+// DFT of z[m + M c] and writes y[f][q M + m] = W_N^(m q) Z_c->q for every row q,
+// the input of cfft_kernel.  The next frame's copies are in flight meanwhile.
+constexpr uint32_t kDsStage0 = kRwA;  // tables as rows_fft_kernel, then the staging slots
+
+__host__ __device__ inline int dif_staged_stages(uint32_t bpf1, uint32_t bpf2) {
+  const uint32_t st = rows_stage_stride(bpf1, bpf2);
+  if (kDsStage0 + 2 * st <= kRwMaxSmem) return 2;
+  if (kDsStage0 + st <= kRwMaxSmem) return 1;
+  return 0;
+}
+
+// One sample of a station (0 outside the frame): m is the sample index, w the
+// word index of m (m >> log2(samples per word)), the rotate amounts and table
+// base as in rows_station.
+__device__ __forceinline__ float staged_sample(const uint32_t* words, const uint8_t* lvbase, int m,
+                                               int w, int n, uint32_t rots, uint32_t omask,
+                                               uint32_t tbase, bool split) {
+  if ((unsigned)m >= (unsigned)n) return 0.0f;
+  const uint32_t x = words[w];
+  uint32_t off;
+  if (split) {
+    off = (__funnelshift_r(x, x, rots & 31u) & 4u) | tbase;
+    off |= __funnelshift_r(x, x, (rots >> 8) & 31u) & 8u;
+  } else {
+    off = (__funnelshift_r(x, x, rots & 31u) & omask) | tbase;
+  }
+  return *reinterpret_cast<const float*>(lvbase + off);
+}
+
+template <int C>
+__global__ void __launch_bounds__(512, 1) dif_staged_kernel(const LargeParams p, uint64_t f0,
+                                                            uint64_t nb, float2* __restrict__ y) {
+  constexpr int M = kLargeM, N = C * M, T = 512;
+  extern __shared__ __align__(128) uint8_t smem[];
+  const int tid = threadIdx.x;
+  float* lv = reinterpret_cast<float*>(smem);
+  uint32_t* pos = reinterpret_cast<uint32_t*>(smem + kRwPos);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kRwBar);
+  int* flag = reinterpret_cast<int*>(smem + kRwFlag);
+  uint32_t* lut = reinterpret_cast<uint32_t*>(smem + kRwLut);
+  uint8_t* stage = smem + kDsStage0;
+  const StationParams& s1 = p.st[0];
+  const StationParams& s2 = p.st[1];
+  const uint32_t bpf1 = s1.bpf, bpf2 = s2.bpf;
+  const uint32_t stride = rows_stage_stride(bpf1, bpf2);
+  const int stages = dif_staged_stages(bpf1, bpf2);
+  const bool pre1 = s1.bits > 2 && s1.shkind != SH_IDENTITY;
+  const bool pre2 = s2.bits > 2 && s2.shkind != SH_IDENTITY;
+
+  if (tid == 0) {
+    for (int k = 0; k < 2; ++k) mbar_init(&bars[k], 1);
+    *flag = 0;
+    fence_proxy_async();
+  }
+  for (int i = tid; i < 1024; i += T) {
+    const StationParams& q = (i < 512) ? s1 : s2;
+    const int n = 1 << q.bits, c2 = i & 511;
+    const float x = c2 < 2 * n ? q.levels[c2 & (n - 1)] * q.scale : 0.0f;
+    lv[i] = c2 >= n ? -x : x;
+  }
+  for (int i = tid; i < 64; i += T) {
+    const int k = i >> 5, cc = i & 31;
+    const StationParams& q = k ? s2 : s1;
+    const int b = q.bits;
+    const bool natural = (k ? pre2 : pre1) || q.shkind == SH_IDENTITY;
+    uint32_t r = 0;
+    if (cc * b < 32) {
+      const int q0 = natural ? cc * b : q.perm[cc * b];
+      const int q1 = b >= 2 ? (natural ? cc * b + 1 : q.perm[cc * b + 1]) : 0;
+      r = (uint32_t)((q0 - 2) & 31) | ((uint32_t)((q1 - 3) & 31) << 8);
+    }
+    pos[i] = r;
+  }
+  for (int k = 0; k < 2; ++k) {
+    const StationParams& q = k ? s2 : s1;
+    if ((k ? pre2 : pre1) && q.shkind == SH_GENERIC)
+      for (int i = tid; i < 1024; i += T) lut[k * 1024 + i] = q.shlut[i];
+  }
+  auto split2 = [](const StationParams& q) {
+    if (q.bits != 2 || q.shkind == SH_IDENTITY) return false;
+    for (int cc = 0; cc < 16; ++cc)
+      if (q.perm[2 * cc + 1] != q.perm[2 * cc] + 1 || (q.perm[2 * cc] & 1)) return true;
+    return false;
+  };
+  const bool sp1 = split2(s1), sp2 = split2(s2);
+  const int lg1 = s1.bits == 1 ? 5 : (s1.bits == 2 ? 4 : (s1.bits == 4 ? 3 : 2));
+  const int lg2 = s2.bits == 1 ? 5 : (s2.bits == 2 ? 4 : (s2.bits == 4 ? 3 : 2));
+  const uint32_t om1 = ((1u << s1.bits) - 1u) << 2, om2 = ((1u << s2.bits) - 1u) << 2;
+
+  auto frame_of = [&](uint32_t i) { return (uint64_t)blockIdx.x + (uint64_t)i * gridDim.x; };
+  auto issue = [&](uint32_t i) {
+    const uint64_t f = f0 + frame_of(i);
+    const int slot = (int)(i % (uint32_t)stages);
+    uint8_t* dst = stage + slot * stride;
+    mbar_expect_tx(&bars[slot], kFiBytes + bpf1 + bpf2);
+    bulk_g2s(dst, p.finfo + f, kFiBytes, &bars[slot]);
+    bulk_g2s(dst + 128, s1.raw + f * bpf1, bpf1, &bars[slot]);
+    bulk_g2s(dst + 128 + bpf1, s2.raw + f * bpf2, bpf2, &bars[slot]);
+  };
+  __syncthreads();
+  if (tid == 0) {
+    fence_proxy_async();
+    for (uint32_t i = 0; i < (uint32_t)stages && frame_of(i) < nb; ++i) issue(i);
+  }
+  for (uint32_t i = 0; frame_of(i) < nb; ++i) {
+    const uint64_t fl = frame_of(i);
+    const int slot = (int)(i % (uint32_t)stages);
+    const uint32_t parity = (i / (uint32_t)stages) & 1u;
+    if (!mbar_wait(&bars[slot], parity, kWaitPolls)) {
+      atomicOr(flag, 1);
+      atomicOr(p.err, ERR_WAIT_TIMEOUT);
+    }
+    uint8_t* st = stage + slot * stride;
+    const uint32_t* w1 = reinterpret_cast<const uint32_t*>(st + 128);
+    const uint32_t* w2 = reinterpret_cast<const uint32_t*>(st + 128 + bpf1);
+    __syncthreads();
+    if (*flag) break;
+    if (pre1 || pre2) {
+      preshuffle_slot(const_cast<uint32_t*>(w1), bpf1 / 4, pre1 ? s1.shkind : SH_IDENTITY, lut,
+                      const_cast<uint32_t*>(w2), bpf2 / 4, pre2 ? s2.shkind : SH_IDENTITY,
+                      lut + 1024, tid, T);
+      __syncthreads();
+    }
+    const FrameInfo* F = reinterpret_cast<const FrameInfo*>(st);
+    const uint64_t f = f0 + fl;
+    const uint32_t odd = (uint32_t)(f & 1u);  // station 2 enters odd frames negated
+    const int m1 = tid - F->s1, m2 = tid - F->s2;
+    const uint32_t rot1 = pos[m1 & ((32 / s1.bits) - 1)], rot2 = pos[32 + (m2 & ((32 / s2.bits) - 1))];
+    const uint32_t tb1 = (uint32_t)((m1 & (s1.lsb ? 1 : 0)) << (s1.bits + 2));
+    const uint32_t tb2 = 2048u + (uint32_t)((((uint32_t)m2 & (uint32_t)(s2.lsb ? 1 : 0)) ^ odd)
+                                            << (s2.bits + 2));
+    const int wb1 = m1 >> lg1, wb2 = m2 >> lg2;  // floor divisions
+    float2* yf = y + fl * (uint64_t)N;
+#pragma unroll 2
+    for (int r = 0; r < 16; ++r) {
+      const int m = tid + 512 * r;  // column
+      float2 v[16];
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int o = 512 * r + M * c;
+        const float a = staged_sample(w1, smem, m1 + o, wb1 + (o >> lg1), N, rot1, om1, tb1, sp1);
+        const float b = staged_sample(w2, smem, m2 + o, wb2 + (o >> lg2), N, rot2, om2, tb2, sp2);
+        v[c] = make_float2(a, b);
+      }
+      if constexpr (C == 2) {
+        dft2<0>(v);
+      } else if constexpr (C == 4) {
+        dft4<0>(v);
+      } else {
+        dft8<0>(v);
+      }
+#pragma unroll
+      for (int q = 0; q < C; ++q) {
+        float2 val = v[out_pos<C>(q)];
+        if (q > 0) val = cmul(val, p.tw[m * q]);  // W_N^(m q), m q < N
+        yf[q * M + m] = val;
+      }
+    }
+    __syncthreads();  // the staged words are consumed: refill the slot
+    if (tid == 0 && frame_of(i + stages) < nb) {
+      fence_proxy_async();
+      issue(i + stages);
+    }
+  }
+  if (tid == 0 && *flag) {
+    for (int k = 0; k < stages; ++k) mbar_wait(&bars[k], 0, kWaitPolls);
+  }
+}
+
+// The same fused DIF + row FFT on a complex input already in global memory
+// (the phased path's Hermitian-extended spectra): item (frame f, row q) reads
+// x[f][m + M c] for its 16 columns and every segment, forms
+// y_q[m] = W_N^(m q) sum_c x[m + M c] W_C^(c q) and writes FFT_M(y_q) to
+// y[f][q M + k].  Replaces dif_kernel + cfft_kernel (one global round trip).
+template <int C>
+__global__ void __launch_bounds__(512, 1) rows_fft_complex_kernel(const float2* __restrict__ x,
+                                                                  float2* __restrict__ y,
+                                                                  uint64_t nb,
+                                                                  const float2* __restrict__ twn) {
+  constexpr int M = kLargeM, N = C * M, T = M / 16;
+  extern __shared__ __align__(128) uint8_t smem[];
+  float2* bufA = reinterpret_cast<float2*>(smem);
+  float2* bufB = reinterpret_cast<float2*>(smem + kRwBuf);
+  const int tid = threadIdx.x;
+  Twiddles<M> tw;
+  tw.init(tid);
+  const uint64_t items = nb * (uint64_t)C;
+  for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const uint64_t fl = it / C;
+    const int q = (int)(it % C);
+    const float2* xf = x + fl * (uint64_t)N;
+    float2 wq[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      float sn, cs;
+      sincospif(-2.0f * (float)((c * q) % C) / (float)C, &sn, &cs);
+      wq[c] = make_float2(cs, sn);
+    }
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const float2 z = xf[tid + 512 * r + M * c];
+        a.x = fmaf(z.x, wq[c].x, fmaf(-z.y, wq[c].y, a.x));
+        a.y = fmaf(z.x, wq[c].y, fmaf(z.y, wq[c].x, a.y));
+      }
+      v[r] = q > 0 ? cmul(a, twn[(tid + 512 * r) * q]) : a;  // W_N^(m q), m q < N
+    }
+    dft16(v);
+    float2* dst = bufA + 17 * tid;  // cpad(16 t + r) = 17 t + r
+#pragma unroll
+    for (int r = 0; r < 16; ++r) dst[r] = v[out_pos<16>(r)];
+    const float2* Z = fft_rest<M>(bufA, bufB, tid, tw);
+    __syncthreads();
+    float4* out = reinterpret_cast<float4*>(y + fl * (uint64_t)N + (uint64_t)q * M);
+    const float4* zin = reinterpret_cast<const float4*>(Z);
+    for (int k = tid; k < M / 2; k += T) out[k] = zin[k];
+    __syncthreads();  // the buffers are free for the next item
   }
 }
 
@@ -226,32 +607,62 @@ __global__ void dif_kernel(const float2* __restrict__ z, float2* __restrict__ y,
   }
 }
 
-// In-place M-point FFT of each row of y (rows of M complex values), natural order.
+// In-place M-point FFT of each row of y (rows of M complex values), natural
+// order.  The next row of the CTA is brought into a shared-memory staging
+// row by a bulk copy while the current row is transformed.
 template <int M>
-__global__ void __launch_bounds__(M / 16, 1) cfft_kernel(float2* __restrict__ y, uint64_t rows) {
+__global__ void __launch_bounds__(M / 16, 1) cfft_kernel(float2* __restrict__ y, uint64_t rows,
+                                                         uint32_t* err) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr int T1 = M / 16;
+  constexpr uint32_t kRowBytes = (uint32_t)M * sizeof(float2);
   float2* bufA = reinterpret_cast<float2*>(smem);
   float2* bufB = bufA + Geom<M>::CSTRIDE;
-  float* x1 = reinterpret_cast<float*>(bufB);
-  float* x2 = x1 + Geom<M>::FSTRIDE;
+  float2* stg = bufB + Geom<M>::CSTRIDE;  // one row, unpadded
+  uint64_t* bar = reinterpret_cast<uint64_t*>(stg + M);
+  int* flag = reinterpret_cast<int*>(bar + 1);
   const int t = threadIdx.x;
   Twiddles<M> tw;
   tw.init(t);
-  for (uint64_t r = blockIdx.x; r < rows; r += gridDim.x) {
-    float2* row = y + r * M;
-    for (int i = t; i < M; i += T1) {
-      const float2 v = row[i];
-      x1[fpad(i)] = v.x;
-      x2[fpad(i)] = v.y;
+  if (t == 0) {
+    mbar_init(bar, 1);
+    *flag = 0;
+    fence_proxy_async();
+  }
+  __syncthreads();
+  auto fetch = [&](uint64_t r) {
+    mbar_expect_tx(bar, kRowBytes);
+    bulk_g2s(stg, y + r * M, kRowBytes, bar);
+  };
+  if (t == 0 && blockIdx.x < rows) fetch(blockIdx.x);
+  uint32_t n = 0;  // rows consumed
+  for (uint64_t r = blockIdx.x; r < rows; r += gridDim.x, ++n) {
+    if (!mbar_wait(bar, n & 1u, kWaitPolls)) {
+      atomicOr(flag, 1);
+      atomicOr(err, ERR_WAIT_TIMEOUT);
     }
     __syncthreads();
-    first_pass<M>(x1, x2, 0, 0, bufA, t);
+    if (*flag) break;
+    float2 v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = stg[t + T1 * k];
+    dft16(v);
+    float2* dst = bufA + 17 * t;  // cpad(16 t + r) = 17 t + r
+#pragma unroll
+    for (int k = 0; k < 16; ++k) dst[k] = v[out_pos<16>(k)];
     float2* Z = fft_rest<M>(bufA, bufB, t, tw);
+    // fft_rest opened with a barrier: the staging row is consumed
+    if (t == 0 && r + gridDim.x < rows) {
+      fence_proxy_async();
+      fetch(r + gridDim.x);
+    }
     __syncthreads();
-    for (int i = t; i < M; i += T1) row[i] = Z[i];
+    float4* row = reinterpret_cast<float4*>(y + r * M);
+    const float4* zin = reinterpret_cast<const float4*>(Z);
+    for (int i = t; i < M / 2; i += T1) row[i] = zin[i];
     __syncthreads();
   }
+  if (t == 0 && *flag) mbar_wait(bar, 0, kWaitPolls);
 }
 
 // Per-bin split + accumulation.  Bin g = C*kk + q: q = blockIdx.y, kk from x,
@@ -271,7 +682,9 @@ __global__ void acc_global_kernel(const LargeParams p, const float2* __restrict_
     k &= (N - 1);
     return Zf[(k % C) * M + k / C];
   };
-  double a[4] = {0, 0, 0, 0};
+  // f32 sums over the group's frames (at most 32 per launch), added to the
+  // f64 partials once per launch, as the FFT-8192 kernel flushes its registers
+  float a[4] = {0.f, 0.f, 0.f, 0.f};
   const uint64_t groups = gridDim.z;
   const uint64_t g0 = (blockIdx.z * nb) / groups, g1 = ((blockIdx.z + 1) * nb) / groups;
   // unrolled: the frames' loads go out together (the loop is latency-bound)
@@ -287,31 +700,31 @@ __global__ void acc_global_kernel(const LargeParams p, const float2* __restrict_
     if (p.grid == 0) {
       const bool inov = bin >= a1s && bin < a1e;
       const float2 p1 = make_float2(u.x + w.x, u.y - w.y);
-      if (want_acf && (!ov_only || inov)) a[0] += (double)cnorm2(p1);
+      if (want_acf && (!ov_only || inov)) a[0] += cnorm2(p1);
       if (inov) {
         const int i2 = bin + sb;
         const float2 c = zi(Zf, i2), d = zi(Zf, N - i2);
         const float2 q2 = make_float2(sg * (c.y + d.y), sg * (d.x - c.x));
-        if (want_acf) a[1] += (double)cnorm2(q2);
+        if (want_acf) a[1] += cnorm2(q2);
         if (want_xcf) {
           const float2 x = cmul(cmulc(p1, q2), r);
-          a[2] += (double)x.x;
-          a[3] += (double)x.y;
+          a[2] += x.x;
+          a[3] += x.y;
         }
       }
     } else {
       const bool inov = bin >= a2s && bin < a2s + ov;
       const float2 p2 = make_float2(sg * (u.y + w.y), sg * (w.x - u.x));
-      if (want_acf && (!ov_only || inov)) a[1] += (double)cnorm2(p2);
+      if (want_acf && (!ov_only || inov)) a[1] += cnorm2(p2);
       if (inov) {
         const int i1 = bin - sb;
         const float2 c = zi(Zf, i1), d = zi(Zf, N - i1);
         const float2 q1 = make_float2(c.x + d.x, c.y - d.y);
-        if (want_acf) a[0] += (double)cnorm2(q1);
+        if (want_acf) a[0] += cnorm2(q1);
         if (want_xcf) {
           const float2 x = cmul(cmulc(q1, p2), r);
-          a[2] += (double)x.x;
-          a[3] += (double)x.y;
+          a[2] += x.x;
+          a[3] += x.y;
         }
       }
     }
@@ -320,7 +733,7 @@ __global__ void acc_global_kernel(const LargeParams p, const float2* __restrict_
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
     double* d = pg + (size_t)v * H + bin;
-    *d = (first_batch ? 0.0 : *d) + a[v];
+    *d = (first_batch ? 0.0 : *d) + (double)a[v];
   }
 }
 
@@ -363,7 +776,9 @@ __global__ void phased_global_kernel(const LargeParams p, const PhasedParams pp,
     k &= (N - 1);
     return Zf[(k % C) * M + k / C];
   };
-  double acc = 0.0;
+  // f32 sums over the group's frames (at most 32 per launch), added to the
+  // f64 partials once per launch
+  float acc = 0.f;
   const uint64_t groups = gridDim.z;
   const uint64_t g0 = (blockIdx.z * nb) / groups, g1 = ((blockIdx.z + 1) * nb) / groups;
   for (uint64_t fl = g0; fl < g1; ++fl) {
@@ -376,8 +791,10 @@ __global__ void phased_global_kernel(const LargeParams p, const PhasedParams pp,
       const float2 a = zi(Zf, k), b = zi(Zf, N - k);
       float2 v = s == 0 ? make_float2(u1 * (a.x + b.x), u1 * (a.y - b.y))
                         : make_float2(sg * u2 * (a.y + b.y), sg * u2 * (b.x - a.x));
+      // SFU sin/cos: |angle| <= pi |frac| fs k / N <= pi / 2, abs error < 4e-7
+      // (as the FFT <= 8192 phased kernels)
       float sn, cs;
-      sincosf((float)k * (s == 0 ? F.st1 : F.st2), &sn, &cs);
+      __sincosf((float)k * (s == 0 ? F.st1 : F.st2), &sn, &cs);
       v = cmul(v, make_float2(cs, sn));
       if (k == N / 2) v.y = 0.f;
       return cmul(v, s == 0 ? F.fr_lo1 : F.fr_lo2);
@@ -391,7 +808,7 @@ __global__ void phased_global_kernel(const LargeParams p, const PhasedParams pp,
       if (bin >= a2s && bin < a2s + ov) a1 = station_bin(0, bin - sb);
     }
     float2 cb = make_float2(a1.x * pp.w1 + a2.x * pp.w2, a1.y * pp.w1 + a2.y * pp.w2);
-    acc += (double)cnorm2(cb);
+    acc += cnorm2(cb);
     if (pp.want_raw) {
       float2* wf = W + fl * (uint64_t)N;
       if (bin == 0 || bin == N / 2) cb.y = 0.f;
@@ -400,7 +817,7 @@ __global__ void phased_global_kernel(const LargeParams p, const PhasedParams pp,
     }
   }
   double* d = part + (size_t)blockIdx.z * H + bin;
-  *d = (first_batch ? 0.0 : *d) + acc;
+  *d = (first_batch ? 0.0 : *d) + (double)acc;
 }
 
 // Re-quantise and pack the phased time series (quantise_frame,
@@ -440,7 +857,9 @@ __global__ void quant_global_kernel(const LargeParams p, const PhasedParams pp,
 // ------------------------------------------------------------- launchers
 
 int large_batch_frames(uint32_t n) {
-  // two scratch buffers of batch * n complex f32 each, 64 MiB apiece
+  // two scratch buffers of batch * n complex f32 each, 64 MiB apiece; a batch
+  // is split into at most kLargeGroups frame groups of at most 32 frames each
+  // (16384: 512 / 16), the f32 run length of acc_global_kernel's sums
   const uint64_t per = (uint64_t)n * sizeof(float2);
   return (int)std::max<uint64_t>(1, (64ull << 20) / per);
 }
@@ -468,29 +887,118 @@ static cudaError_t large_fft_core(const LargeParams& p, uint64_t nb, const float
 
 static cudaError_t row_ffts(const LargeParams& p, uint64_t nb, float2* buf1, int sms,
                            cudaStream_t s) {
-  const uint32_t smem = 2 * Geom<kLargeM>::CSTRIDE * sizeof(float2);
+  // two padded FFT buffers, the staging row, its mbarrier and the error flag
+  const uint32_t smem = 2 * Geom<kLargeM>::CSTRIDE * sizeof(float2) + kLargeM * sizeof(float2) + 16;
   auto kern = cfft_kernel<kLargeM>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const uint64_t rows = nb * (uint64_t)p.c;
-  kern<<<(unsigned)std::min<uint64_t>(rows, (uint64_t)sms), kLargeM / 16, smem, s>>>(buf1, rows);
+  kern<<<(unsigned)std::min<uint64_t>(rows, (uint64_t)sms), kLargeM / 16, smem, s>>>(buf1, rows,
+                                                                                     p.err);
+  return cudaGetLastError();
+}
+
+// The fused kernel decodes every segment of the frame for each of its C rows.
+// Measured against dif_staged_kernel + cfft_kernel (device-resident 2-bit
+// sectors): C = 2 (FFT 16384, odd band shift) 201 against 166 Gsample/s;
+// C = 4 156 against 165; C = 8 95 against 134.  So it serves C = 2.
+bool rows_fft_supported(const LargeParams& p) {
+  return p.c == 2 && rows_stages(p.st[0].bpf, p.st[1].bpf) > 0;
+}
+
+cudaError_t launch_rows_fft(const LargeParams& p, uint64_t f0, uint64_t nb, float2* y, int sms,
+                            cudaStream_t s) {
+  const int stages = rows_stages(p.st[0].bpf, p.st[1].bpf);
+  const uint32_t smem = kRwStage0 + (uint32_t)stages * rows_stage_stride(p.st[0].bpf, p.st[1].bpf);
+  const uint64_t items = nb * (uint64_t)p.c;
+  const unsigned grid = (unsigned)std::min<uint64_t>(items, (uint64_t)sms);
+  cudaError_t e;
+  switch (p.c) {
+    case 2:
+      e = cudaFuncSetAttribute(rows_fft_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kRwMaxSmem);
+      if (e == cudaSuccess) rows_fft_kernel<2><<<grid, 512, smem, s>>>(p, f0, nb, y);
+      break;
+    case 4:
+      e = cudaFuncSetAttribute(rows_fft_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kRwMaxSmem);
+      if (e == cudaSuccess) rows_fft_kernel<4><<<grid, 512, smem, s>>>(p, f0, nb, y);
+      break;
+    case 8:
+      e = cudaFuncSetAttribute(rows_fft_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kRwMaxSmem);
+      if (e == cudaSuccess) rows_fft_kernel<8><<<grid, 512, smem, s>>>(p, f0, nb, y);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+// The DIF step and the row FFTs of a complex input in global memory (x -> y).
+cudaError_t launch_rows_fft_complex(const LargeParams& p, uint64_t nb, const float2* x, float2* y,
+                                    int sms, cudaStream_t s) {
+  const uint32_t smem = 2 * kRwBuf;
+  const unsigned grid = (unsigned)std::min<uint64_t>(nb * (uint64_t)p.c, (uint64_t)sms);
+  cudaError_t e;
+  switch (p.c) {
+    case 2:
+      e = cudaFuncSetAttribute(rows_fft_complex_kernel<2>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess) rows_fft_complex_kernel<2><<<grid, 512, smem, s>>>(x, y, nb, p.tw);
+      break;
+    case 4:
+      e = cudaFuncSetAttribute(rows_fft_complex_kernel<4>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess) rows_fft_complex_kernel<4><<<grid, 512, smem, s>>>(x, y, nb, p.tw);
+      break;
+    case 8:
+      e = cudaFuncSetAttribute(rows_fft_complex_kernel<8>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess) rows_fft_complex_kernel<8><<<grid, 512, smem, s>>>(x, y, nb, p.tw);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
 cudaError_t launch_large_fft(const LargeParams& p, uint64_t f0, uint64_t nb, float2* buf0,
                              float2* buf1, int sms, cudaStream_t s) {
-  // decode + DIF -> buf1, row FFTs in place on buf1 (buf0 is not used)
+  // decode + DIF + row FFTs fused (rows_fft_kernel) when the frame's words
+  // fit its staging; else decode + DIF -> buf1, row FFTs in place on buf1
   (void)buf0;
-  const uint64_t work = nb * kLargeM;
-  switch (p.c) {
-    case 2: decode_dif_kernel<2><<<grid_for(work, 256, sms), 256, 0, s>>>(p, f0, nb, buf1); break;
-    case 4: decode_dif_kernel<4><<<grid_for(work, 256, sms), 256, 0, s>>>(p, f0, nb, buf1); break;
-    case 8: decode_dif_kernel<8><<<grid_for(work, 256, sms), 256, 0, s>>>(p, f0, nb, buf1); break;
-    default: return cudaErrorInvalidValue;
+  if (rows_fft_supported(p)) return launch_rows_fft(p, f0, nb, buf1, sms, s);
+  const int dstages = dif_staged_stages(p.st[0].bpf, p.st[1].bpf);
+  if (dstages > 0) {
+    // decode + DIF from staged words, then the row FFTs
+    const uint32_t smem = kDsStage0 + (uint32_t)dstages * rows_stage_stride(p.st[0].bpf, p.st[1].bpf);
+    const unsigned grid = (unsigned)std::min<uint64_t>(nb, (uint64_t)sms);
+    cudaError_t e;
+    switch (p.c) {
+      case 2:
+        e = cudaFuncSetAttribute(dif_staged_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kRwMaxSmem);
+        if (e == cudaSuccess) dif_staged_kernel<2><<<grid, 512, smem, s>>>(p, f0, nb, buf1);
+        break;
+      case 4:
+        e = cudaFuncSetAttribute(dif_staged_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kRwMaxSmem);
+        if (e == cudaSuccess) dif_staged_kernel<4><<<grid, 512, smem, s>>>(p, f0, nb, buf1);
+        break;
+      case 8:
+        e = cudaFuncSetAttribute(dif_staged_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kRwMaxSmem);
+        if (e == cudaSuccess) dif_staged_kernel<8><<<grid, 512, smem, s>>>(p, f0, nb, buf1);
+        break;
+      default: return cudaErrorInvalidValue;
+    }
+    if (e != cudaSuccess) return e;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return row_ffts(p, nb, buf1, sms, s);
   }
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  return row_ffts(p, nb, buf1, sms, s);
+  // every frame of FFT <= 65536 at <= 8 bits fits one staging slot
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_twiddle_table(int n, float2* tw, cudaStream_t s) {
@@ -506,7 +1014,9 @@ cudaError_t launch_large_phased(const LargeParams& p, const PhasedParams& pp, fl
   phased_global_kernel<<<grid, 256, 0, s>>>(p, pp, buf1, f0, nb, first_batch, part, buf0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !pp.want_raw) return e;
-  if ((e = large_fft_core(p, nb, buf0, buf1, sms, s)) != cudaSuccess) return e;
+  e = p.c <= 4 ? launch_rows_fft_complex(p, nb, buf0, buf1, sms, s)
+               : large_fft_core(p, nb, buf0, buf1, sms, s);
+  if (e != cudaSuccess) return e;
   const uint64_t words = nb * (uint64_t)(p.n / (32 / pp.bits_out));
   quant_global_kernel<<<grid_for(words, 256, sms), 256, 0, s>>>(p, pp, buf1, f0, nb);
   return cudaGetLastError();
