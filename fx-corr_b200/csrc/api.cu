@@ -439,10 +439,12 @@ fxc_status run_sector_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, 
   if (fst != FXC_OK) return fst;
   s->all_launches += 1;
   if (s->n > 8192) {
-    // FFT 16384 correlation: the two-row shared-memory kernel when the band
-    // shift is even, else the four-step path
+    // correlation: the two-row shared-memory kernel for FFT 16384 with an even
+    // band shift, else the cluster kernel; the four-step path when neither
+    // can run (and for the phased products)
     bool corr_done = false;
-    if (s->n == 16384 && corr && corr_fold2_supported(corr_params(s, r1, r2, nf, first))) {
+    if (corr && (corr_cluster_capacity(s->n) > 0 ||
+                 (s->n == 16384 && corr_fold2_supported(corr_params(s, r1, r2, nf, first))))) {
       fst = run_corr_stage(s, r1, r2, nf, first, grid, d_acc, st);
       if (fst != FXC_OK) return fst;
       corr_done = true;
@@ -480,10 +482,18 @@ fxc_status run_corr_stage(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uin
     ev = &s->prof_events[s->prof_used++];
     CK(cudaEventRecord(ev->first, st));
   }
-  CK(launch_corr(s->n, MODE_CORR, p, grid, st));
+  int nblk = grid;  // partial rows to reduce
+  if (s->n > 8192 && !(s->n == 16384 && corr_fold2_supported(p))) {
+    nblk = corr_cluster_count(s->n, nf);
+    if (nblk <= 0) return fail(FXC_EUNSUPPORTED, "no cluster of %d CTAs fits this GPU",
+                               corr_cluster_size(s->n));
+    CK(launch_corr_cluster(s->n, p, nblk, st));
+  } else {
+    CK(launch_corr(s->n, MODE_CORR, p, grid, st));
+  }
   if (ev) CK(cudaEventRecord(ev->second, st));
   const double u1 = 1.0 / s->scale[0], u2 = 1.0 / s->scale[1];
-  CK(launch_reduce(s->d_partials, grid, (int)h, 0.25 * u1 * u1, 0.25 * u2 * u2, 0.25 * u1 * u2,
+  CK(launch_reduce(s->d_partials, nblk, (int)h, 0.25 * u1 * u1, 0.25 * u2 * u2, 0.25 * u1 * u2,
                    d_acc, st));
   s->kernel_launches += 1;
   s->all_launches += 2;
@@ -637,9 +647,14 @@ fxc_status scan_bind(fxc_scan* s, const fxc_scan_cfg* cfg) {
   const uint64_t maxg = n > 8192 ? (uint64_t)kLargeGroups
                                  : (uint64_t)e->sm_count * (uint64_t)corr_ctas_per_sm(n);
   // N > 8192: [group][4][H] correlation partials, then [group][H] phased partials;
-  // N = 16384 also serves the two-row kernel's [CTA][4][H]
+  // also the two-row kernel's [CTA][4][H] (N = 16384) and the cluster
+  // kernel's [cluster][4][H]
   uint64_t pel = maxg * (n > 8192 ? 5 : 4) * h;
   if (n == 16384) pel = std::max<uint64_t>(pel, (uint64_t)e->sm_count * 4 * h);
+  if (n > 8192) {
+    const uint64_t c = (uint64_t)corr_cluster_size(n);
+    pel = std::max<uint64_t>(pel, ((uint64_t)e->sm_count + c - 1) / c * 4 * h);
+  }
   const uint64_t bigf = n > 8192 ? (uint64_t)large_batch_frames(n) : 0;
   const uint64_t bige = bigf * (uint64_t)n;
   const uint64_t tlen = cfg->delay.geom_table ? cfg->delay.geom_len : 0;

@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "decode_tables.cuh"
 #include "fxc_device.cuh"
 #include "fxc_kernels.h"
 
@@ -50,7 +51,7 @@ constexpr int kSlots = 2 * kUnits + 1;  // accumulator rows (bin N/4 by thread 0
 struct FoldLayout {
   uint32_t off_a, off_b, off_stage, stage_stride, total;
 };
-constexpr uint32_t kOffPos = 4096, kOffFi = 4352, kOffBar = 4448, kOffFlag = 4464, kOffLut = 4608;
+constexpr uint32_t kOffPos = kTabPos, kOffFi = 4352, kOffBar = 4448, kOffFlag = 4464, kOffLut = kTabLut;
 constexpr uint32_t kOffA = kOffLut + 8192;
 
 __host__ __device__ inline FoldLayout fold_layout(uint32_t raw_bytes) {
@@ -162,52 +163,13 @@ __device__ __forceinline__ void fold_station(int bits, bool split, const uint32_
 }
 
 
-// The scan's decode tables in shared memory (primary station first): level
-// tables with their negated copies, the rotate amounts of every sample slot,
-// and the byte LUTs of 4- and 8-bit generic shuffles.  Needs a barrier before
-// use.
+// The scan's decode tables (primary station first, decode_tables.cuh).
 __device__ __forceinline__ void fold_build_tables(const StationParams& sp, const StationParams& ss,
                                                   bool preP, bool preS, uint8_t* smem, int tid) {
-  float* lv = reinterpret_cast<float*>(smem);
-  uint32_t* pos = reinterpret_cast<uint32_t*>(smem + kOffPos);
-  uint32_t* lut = reinterpret_cast<uint32_t*>(smem + kOffLut);
-  for (int i = tid; i < 1024; i += kT) {
-    // per station: 2^b levels, then their negations (the two sign groups of a
-    // warp's table loads fall in different banks)
-    const StationParams& q = (i < 512) ? sp : ss;
-    const int n = 1 << q.bits, c2 = i & 511;
-    const float x = c2 < 2 * n ? q.levels[c2 & (n - 1)] * q.scale : 0.0f;
-    lv[i] = c2 >= n ? -x : x;
-  }
-  for (int i = tid; i < 64; i += kT) {
-    // rotate amounts of sample slot c: bit j of the sample is word bit p_j
-    const int k = i >> 5, cc = i & 31;
-    const StationParams& q = k ? ss : sp;
-    const int b = q.bits;
-    const bool natural = (k ? preS : preP) || q.shkind == SH_IDENTITY;
-    uint32_t r = 0;
-    if (cc * b < 32) {
-      const int p0 = natural ? cc * b : q.perm[cc * b];
-      const int p1 = b >= 2 ? (natural ? cc * b + 1 : q.perm[cc * b + 1]) : 0;
-      r = (uint32_t)((p0 - 2) & 31) | ((uint32_t)((p1 - 3) & 31) << 8);
-    }
-    pos[i] = r;
-  }
-  for (int k = 0; k < 2; ++k) {
-    const StationParams& q = k ? ss : sp;
-    if ((k ? preS : preP) && q.shkind == SH_GENERIC)
-      for (int i = tid; i < 1024; i += kT) lut[k * 1024 + i] = q.shlut[i];
-  }
+  build_decode_tables(sp, ss, preP, preS, smem, tid, kT);
 }
 
-// A 2-bit shuffle keeps every sample's two bits adjacent and in order, or it
-// splits them (two rotates per sample).
-__device__ __forceinline__ bool fold_split2(const StationParams& q) {
-  if (q.bits != 2 || q.shkind == SH_IDENTITY) return false;
-  for (int cc = 0; cc < 16; ++cc)
-    if (q.perm[2 * cc + 1] != q.perm[2 * cc] + 1 || (q.perm[2 * cc] & 1)) return true;
-  return false;
-}
+__device__ __forceinline__ bool fold_split2(const StationParams& q) { return split_2bit(q); }
 
 // Per-CTA state of the fold kernels that does not depend on the scan: the
 // twiddle power chains, the two-row DIF twiddle bases, and the number of

@@ -75,6 +75,13 @@ cudaError_t launch_fold_decode(const CorrParams& p, int grid, cudaStream_t s);
 bool corr_fold2_supported(const CorrParams& p);
 cudaError_t launch_corr_fold2(const CorrParams& p, int grid, cudaStream_t s);
 uint32_t fold_smem_bytes(uint32_t stage_bytes);
+// FFT 16384 / 32768 / 65536 correlation (MODE_CORR) by clusters of C = N / 8192
+// CTAs exchanging through distributed shared memory (corr_cluster.cu): every
+// band shift and bit depth; partials [clusters][4][H].
+int corr_cluster_size(uint32_t n);      // C, 0 when N has no cluster kernel
+int corr_cluster_capacity(uint32_t n);  // clusters resident at once (0: none)
+int corr_cluster_count(uint32_t n, uint64_t nf);  // clusters of a sector's launch
+cudaError_t launch_corr_cluster(uint32_t n, const CorrParams& p, int clusters, cudaStream_t s);
 cudaError_t launch_reduce(const double* part, int nblk, int h, double m11, double m22, double m12,
                           double* out, cudaStream_t s);
 // FFT lengths above 8192 (N = c * 8192): global-memory four-step path.

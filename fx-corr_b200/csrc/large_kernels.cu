@@ -25,6 +25,7 @@
 
 #include <algorithm>
 
+#include "decode_tables.cuh"
 #include "fxc_device.cuh"
 #include "fxc_kernels.h"
 
@@ -98,7 +99,7 @@ __global__ void decode_global_kernel(const LargeParams p, uint64_t f0, uint64_t 
 // 2048, 2^b f32 each then their negations), rotate amounts, mbarriers, error
 // flag, byte LUTs of 4/8-bit generic shuffles, the two padded FFT buffers,
 // then the staging slots [FrameInfo (128 B)][station 1 words][station 2 words].
-constexpr uint32_t kRwPos = 4096, kRwBar = 4352, kRwFlag = 4384, kRwLut = 4608;
+constexpr uint32_t kRwPos = kTabPos, kRwBar = 4352, kRwFlag = 4384, kRwLut = kTabLut;
 constexpr uint32_t kRwA = kRwLut + 8192;
 constexpr uint32_t kRwBuf = (uint32_t)Geom<kLargeM>::CSTRIDE * (uint32_t)sizeof(float2);
 constexpr uint32_t kRwStage0 = kRwA + 2 * kRwBuf;
@@ -195,7 +196,6 @@ __global__ void __launch_bounds__(512, 1) rows_fft_kernel(const LargeParams p, u
   constexpr int M = kLargeM, N = C * M, T = M / 16;
   extern __shared__ __align__(128) uint8_t smem[];
   const int tid = threadIdx.x;
-  float* lv = reinterpret_cast<float*>(smem);
   uint32_t* pos = reinterpret_cast<uint32_t*>(smem + kRwPos);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kRwBar);
   int* flag = reinterpret_cast<int*>(smem + kRwFlag);
@@ -219,38 +219,8 @@ __global__ void __launch_bounds__(512, 1) rows_fft_kernel(const LargeParams p, u
     *flag = 0;
     fence_proxy_async();
   }
-  for (int i = tid; i < 1024; i += T) {
-    const StationParams& q = (i < 512) ? s1 : s2;
-    const int n = 1 << q.bits, c2 = i & 511;
-    const float x = c2 < 2 * n ? q.levels[c2 & (n - 1)] * q.scale : 0.0f;
-    lv[i] = c2 >= n ? -x : x;
-  }
-  for (int i = tid; i < 64; i += T) {
-    // rotate amounts of sample slot c: bit j of the sample is word bit p_j
-    const int k = i >> 5, cc = i & 31;
-    const StationParams& q = k ? s2 : s1;
-    const int b = q.bits;
-    const bool natural = (k ? pre2 : pre1) || q.shkind == SH_IDENTITY;
-    uint32_t r = 0;
-    if (cc * b < 32) {
-      const int q0 = natural ? cc * b : q.perm[cc * b];
-      const int q1 = b >= 2 ? (natural ? cc * b + 1 : q.perm[cc * b + 1]) : 0;
-      r = (uint32_t)((q0 - 2) & 31) | ((uint32_t)((q1 - 3) & 31) << 8);
-    }
-    pos[i] = r;
-  }
-  for (int k = 0; k < 2; ++k) {
-    const StationParams& q = k ? s2 : s1;
-    if ((k ? pre2 : pre1) && q.shkind == SH_GENERIC)
-      for (int i = tid; i < 1024; i += T) lut[k * 1024 + i] = q.shlut[i];
-  }
-  auto split2 = [](const StationParams& q) {
-    if (q.bits != 2 || q.shkind == SH_IDENTITY) return false;
-    for (int cc = 0; cc < 16; ++cc)
-      if (q.perm[2 * cc + 1] != q.perm[2 * cc] + 1 || (q.perm[2 * cc] & 1)) return true;
-    return false;
-  };
-  const bool sp1 = split2(s1), sp2 = split2(s2);
+  build_decode_tables(s1, s2, pre1, pre2, smem, tid, T);
+  const bool sp1 = split_2bit(s1), sp2 = split_2bit(s2);
   Twiddles<M> tw;
   tw.init(tid);
 
@@ -379,7 +349,6 @@ __global__ void __launch_bounds__(512, 1) dif_staged_kernel(const LargeParams p,
   constexpr int M = kLargeM, N = C * M, T = 512;
   extern __shared__ __align__(128) uint8_t smem[];
   const int tid = threadIdx.x;
-  float* lv = reinterpret_cast<float*>(smem);
   uint32_t* pos = reinterpret_cast<uint32_t*>(smem + kRwPos);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kRwBar);
   int* flag = reinterpret_cast<int*>(smem + kRwFlag);
@@ -398,37 +367,8 @@ __global__ void __launch_bounds__(512, 1) dif_staged_kernel(const LargeParams p,
     *flag = 0;
     fence_proxy_async();
   }
-  for (int i = tid; i < 1024; i += T) {
-    const StationParams& q = (i < 512) ? s1 : s2;
-    const int n = 1 << q.bits, c2 = i & 511;
-    const float x = c2 < 2 * n ? q.levels[c2 & (n - 1)] * q.scale : 0.0f;
-    lv[i] = c2 >= n ? -x : x;
-  }
-  for (int i = tid; i < 64; i += T) {
-    const int k = i >> 5, cc = i & 31;
-    const StationParams& q = k ? s2 : s1;
-    const int b = q.bits;
-    const bool natural = (k ? pre2 : pre1) || q.shkind == SH_IDENTITY;
-    uint32_t r = 0;
-    if (cc * b < 32) {
-      const int q0 = natural ? cc * b : q.perm[cc * b];
-      const int q1 = b >= 2 ? (natural ? cc * b + 1 : q.perm[cc * b + 1]) : 0;
-      r = (uint32_t)((q0 - 2) & 31) | ((uint32_t)((q1 - 3) & 31) << 8);
-    }
-    pos[i] = r;
-  }
-  for (int k = 0; k < 2; ++k) {
-    const StationParams& q = k ? s2 : s1;
-    if ((k ? pre2 : pre1) && q.shkind == SH_GENERIC)
-      for (int i = tid; i < 1024; i += T) lut[k * 1024 + i] = q.shlut[i];
-  }
-  auto split2 = [](const StationParams& q) {
-    if (q.bits != 2 || q.shkind == SH_IDENTITY) return false;
-    for (int cc = 0; cc < 16; ++cc)
-      if (q.perm[2 * cc + 1] != q.perm[2 * cc] + 1 || (q.perm[2 * cc] & 1)) return true;
-    return false;
-  };
-  const bool sp1 = split2(s1), sp2 = split2(s2);
+  build_decode_tables(s1, s2, pre1, pre2, smem, tid, T);
+  const bool sp1 = split_2bit(s1), sp2 = split_2bit(s2);
   const int lg1 = s1.bits == 1 ? 5 : (s1.bits == 2 ? 4 : (s1.bits == 4 ? 3 : 2));
   const int lg2 = s2.bits == 1 ? 5 : (s2.bits == 2 ? 4 : (s2.bits == 4 ? 3 : 2));
   const uint32_t om1 = ((1u << s1.bits) - 1u) << 2, om2 = ((1u << s2.bits) - 1u) << 2;

@@ -33,10 +33,12 @@ def injection(fxc_lib):
     fxc_lib.debug_inject_wait_timeout(0, False)
 
 
-@pytest.mark.parametrize("fft", [8192, 16384])
-def test_bounded_wait_runs_out_and_is_reported(engine, fxc_lib, injection, fft):
+# FFT 8192 and 16384 (even band shift): the fold kernels; 16384 with an odd
+# band shift and 65536: the cluster kernel, whose CTAs stop together
+@pytest.mark.parametrize("fft,sb", [(8192, 128), (16384, 128), (16384, 129), (65536, 136)])
+def test_bounded_wait_runs_out_and_is_reported(engine, fxc_lib, injection, fft, sb):
     scan = make_scan(fft=fft, fs=1024e6, shuffle="generic", lsb1=True,
-                     band=(128, 0, fft // 2 - 128, 128), delay=DELAY)
+                     band=(sb, 0, fft // 2 - sb, sb), delay=DELAY)
     nf = 600
     r1, r2 = signal_raw(scan, nf, seed=21, rho=0.2, delay_samples=3.3)
     d1, d2 = dev(r1), dev(r2)

@@ -249,13 +249,19 @@ def test_weak_correlation_long_integration(engine, fft, nf):
     s.close()
 
 
-@pytest.mark.parametrize("fft,d1", [(8192, -2.3e-6), (8192, 5.1e-6), (8192, 1.7e-5),
-                                    (16384, -9.1e-6), (16384, 2.0e-6), (16384, 3.3e-5)])
-def test_sector_large_shift(engine, fft, d1):
+@pytest.mark.parametrize("fft,d1,sb", [
+    (8192, -2.3e-6, 128), (8192, 5.1e-6, 128), (8192, 1.7e-5, 128),
+    (16384, -9.1e-6, 128), (16384, 2.0e-6, 128), (16384, 3.3e-5, 128),
+    # the cluster kernel: staged column ranges clamped at either end of the
+    # frame, whole ranges outside it, and (odd sb) secondary spectra exchanged
+    # between the CTAs of a cluster
+    (16384, -9.1e-6, 129), (32768, -9.1e-6, 128), (32768, 3.3e-5, 131), (32768, 7.0e-5, 128),
+    (65536, -5.3e-5, 133), (65536, 2.0e-6, 128), (65536, 1.4e-4, 128)])
+def test_sector_large_shift(engine, fft, d1, sb):
     """Integer shifts beyond N/16 (and beyond N: an all-zero station frame)."""
     delay = dict(DELAY, net_d1_base=d1)
     scan = make_scan(fft=fft, fs=512e6, delay=delay, shuffle="generic", lsb1=True,
-                     band=(128, 0, fft // 2 - 128, 128))
+                     band=(sb, 0, fft // 2 - sb, sb))
     nf = 9
     r1, r2 = signal_raw(scan, nf, seed=5, rho=0.2, delay_samples=6.4)
     s = engine.open_scan(to_fxc(scan))
@@ -410,13 +416,17 @@ LARGE_CASES = [
     dict(fft=16384, band=(-40, 40, 8192, 0), grid=1, shuffle="generic", lsb2=True),
     dict(fft=16384, bits1=4, bits2=2, band=(12, 0, 8180, 12), grid=0, shuffle="pairswap",
          products=oracle.PROD_ACF | oracle.PROD_ACF_OVERLAP_ONLY | oracle.PROD_XCF),
-    # odd band shift: the four-step path
+    # odd band shift: the cluster kernel, secondary spectra exchanged between CTAs
     dict(fft=16384, band=(-7, 7, 8192, 0), grid=0, lsb1=True),
+    dict(fft=16384, band=(3, 0, 8190, 3), grid=1, bits1=8, bits2=8, shuffle="generic"),
+    dict(fft=32768, band=(-6, 6, 16385, 0), grid=0, bits1=2, bits2=1, shuffle="sample2",
+         lsb2=True),
+    dict(fft=65536, band=(13, 0, 32755, 13), grid=1, shuffle="generic", lsb1=True),
     dict(fft=32768, band=(-64, 64, 16384, 0), grid=1, bits1=4, bits2=4),
     dict(fft=65536, band=(0, 0, 32768, 0), grid=0, bits1=1, bits2=2,
          products=oracle.PROD_ACF | oracle.PROD_ACF_OVERLAP_ONLY | oracle.PROD_XCF),
-    # the four-step decode's shift plans: shuffled 1- and 2-bit stations (bits
-    # kept together, reordered, split or swapped), and the generic 8/4-bit path
+    # shuffled 1- and 2-bit stations (bits kept together, reordered, split or
+    # swapped), and the generic 8/4-bit path
     dict(fft=32768, band=(64, 0, 16320, 64), grid=0, shuffle="generic", lsb2=True),
     dict(fft=32768, band=(0, 0, 16384, 0), grid=1, bits1=1, bits2=2, shuffle="pairswap",
          lsb1=True),
