@@ -59,17 +59,19 @@ def shuffle_internal(seed: int):
 PROD_ACF, PROD_XCF = 1, 2  # product bits (same values in fxc and the oracle)
 
 
-def scan_fields(band_alignment):
+def scan_fields(band_alignment, fft=N):
     """Resolve the scan the way run_once does (src/main.rs:1186-1212,
     1317-1328, 1618-1673) for the synthetic schedule above.  Returns the
     fields shared by fxc.ScanConfig and oracle.Scan; `band_alignment` is
-    either's restatement of compute_band_alignment (src/main.rs:360-372)."""
+    either's restatement of compute_band_alignment (src/main.rs:360-372).
+    `fft` other than 8192: the same schedule at another FFT length (the
+    --fft-sweep mode)."""
     bw = FS / 2e6
     c1 = OBS_MHZ + ROT1_HZ / 1e6 + 0.5 * bw
     c2 = OBS_MHZ + ROT2_HZ / 1e6 + 0.5 * bw
-    band = band_alignment(N, FS, c1, c2, bw, bw)
+    band = band_alignment(fft, FS, c1, c2, bw, bw)
     grid = 0 if abs(ROT1_HZ) <= abs(ROT2_HZ) else 1
-    df = FS / N
+    df = FS / fft
     rot_residual = (ROT1_HZ - ROT2_HZ) - band[0] * df
     rate_user = 0.01  # --resrate
     extra_rate = (-rot_residual + rate_user) / (OBS_MHZ * 1e6)
@@ -85,7 +87,7 @@ def scan_fields(band_alignment):
     delay = dict(time_offset_s=0.0, delay_user_samples=user, extra_delay_rate_sps=extra_rate,
                  d_seek=d_seek, lo1_hz=(OBS_MHZ + ROT1_HZ / 1e6) * 1e6,
                  lo2_hz=(OBS_MHZ + ROT2_HZ / 1e6) * 1e6)
-    return dict(fft=N, fs=FS, bits1=BITS, bits2=BITS, levels1=LEVELS, levels2=LEVELS,
+    return dict(fft=fft, fs=FS, bits1=BITS, bits2=BITS, levels1=LEVELS, levels2=LEVELS,
                 shuffle1=shuffle_internal(101), shuffle2=shuffle_internal(102),
                 lsb1=True, lsb2=False, band=tuple(band), grid=grid,
                 products=PROD_ACF | PROD_XCF, delay=delay, geom_table=table)
@@ -666,6 +668,54 @@ def serve_leg(fxc, torch, eng, jobs, slots, batch, plain_jobs=None, label="", mi
     }
 
 
+def fft_sweep(args):
+    """Device-resident throughput of the correlation and phased (.raw)
+    products by FFT length: the full-rate scan's schedule (1024 Msps, 2-bit,
+    generic shuffle, LSB/USB, 16 MHz band offset) at each length, one sector
+    of --sweep-samples samples per station per call, CUDA events on the
+    calling stream over --steps calls after --warmup.  One JSON line; not the
+    benchmark line."""
+    import torch
+
+    import fxc
+
+    torch.cuda.set_device(0)
+    eng = fxc.Engine(0)
+    stream = torch.cuda.Stream()
+    out = {"mode": "fft-sweep", "unit": "Gsample/s (device-resident, 2-bit)",
+           "samples_per_station_per_call": args.sweep_samples, "calls": args.steps}
+    for fft in [int(v) for v in args.sweep_ffts.split(",")]:
+        for prod in args.sweep_products.split(","):
+            fields = scan_fields(fxc.band_alignment, fft=fft)
+            if prod == "phased":
+                fields["products"] = fxc.PROD_PHASED | fxc.PROD_RAW
+            cfg = fxc.ScanConfig(**fields)
+            scan = eng.open_scan(cfg)
+            nf = args.sweep_samples // fft
+            d1, d2 = gen_station_pair_gpu(torch, nf * fft, seed=fft, cfg=cfg)
+            acc = torch.empty(5 * cfg.h, dtype=torch.float64, device="cuda")
+            raw = (torch.empty(nf * cfg.bpf(BITS), dtype=torch.uint8, device="cuda")
+                   if prod == "phased" else None)
+
+            def call():
+                scan.run_device(d1, d2, nf, 0, acc, d_raw_out=raw, stream=stream)
+
+            for _ in range(args.warmup):
+                call()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                call()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            scan.check()
+            ms = e0.elapsed_time(e1) / args.steps
+            out[f"{prod}_{fft}"] = round(2 * nf * fft / (ms * 1e-3) / 1e9, 1)
+            scan.close()
+            del d1, d2, raw
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -683,8 +733,17 @@ def main():
                     help="sectors per step (profiling cases only; the workload is 10)")
     ap.add_argument("--frames-per-sector", type=int, default=NF_SECTOR,
                     help="frame pairs per sector (profiling cases only; the workload is 125000)")
+    ap.add_argument("--fft-sweep", action="store_true",
+                    help="print device-resident throughput by FFT length instead of the "
+                         "benchmark line")
+    ap.add_argument("--sweep-ffts", default="1024,2048,4096,8192,16384,32768,65536")
+    ap.add_argument("--sweep-products", default="corr,phased")
+    ap.add_argument("--sweep-samples", type=int, default=1 << 29,
+                    help="samples per station per call in --fft-sweep")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.fft_sweep:
+        return fft_sweep(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
