@@ -36,6 +36,7 @@
 
 #include <atomic>
 
+#include "cluster_frame.cuh"
 #include "decode_tables.cuh"
 #include "fxc_device.cuh"
 #include "fxc_kernels.h"
@@ -43,8 +44,9 @@
 namespace fxc {
 namespace {
 
-constexpr int kM = 8192;           // row length
-constexpr int kT = 512;            // threads per CTA
+using clu::kM;
+using clu::kT;
+using namespace clu;
 constexpr int kJ = kM / 2 / kT;    // bins per thread (8)
 
 // Shared memory (bytes): the decode tables [0, kTabEnd) with the frame
@@ -64,11 +66,10 @@ constexpr uint32_t kClMaxSmem = 232448;  // 227 KB per CTA on sm_100
 static_assert(kClFi + 2 * kFiBytes <= kClBar && kClFlag + 4 <= kTabLut, "records fit the gap");
 static_assert(kClX % 128 == 0 && kClStage0 % 128 == 0, "alignment");
 
-// Words of one staged region: the CTA's M/C columns of a segment plus the
-// slack of a start rounded down to 16 bytes and a shift that is not a whole
-// number of words (a multiple of 4 words, so every copy is 16-byte sized).
+// Words of one staged region: the CTA's M/C columns of a segment
+// (cluster_frame.cuh).
 __host__ __device__ constexpr int cl_region_words(int c, int bits) {
-  return kM / (c * (32 / bits)) + 4;
+  return region_words(kM / c, bits);
 }
 __host__ __device__ inline uint32_t cl_stage_stride(int c, int bits_p, int bits_s) {
   return (128u + 4u * (uint32_t)c *
@@ -80,123 +81,6 @@ __host__ __device__ inline uint32_t cl_smem_bytes(int c, int bits_p, int bits_s)
 }
 static_assert(kClStage0 + 2 * ((128 + 4 * 2 * 2 * (kM / 8 + 4) + 127) & ~127) <= kClMaxSmem,
               "8-bit stations fit");
-
-__device__ __forceinline__ uint32_t cl_rank() {
-  uint32_t r;
-  asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ uint32_t cl_id() {
-  uint32_t r;
-  asm("mov.u32 %0, %%clusterid.x;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ uint32_t cl_count() {
-  uint32_t r;
-  asm("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
-  return r;
-}
-// Split cluster barrier: every thread of every CTA of the cluster arrives;
-// release / acquire order the shared-memory stores (local and remote) before it
-// with the loads after it.
-__device__ __forceinline__ void cl_arrive() {
-  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void cl_wait() {
-  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void cl_sync() {
-  cl_arrive();
-  cl_wait();
-}
-// Address of the same shared-memory object in CTA `rank` of the cluster.
-__device__ __forceinline__ uint32_t cl_map(const void* p, uint32_t rank) {
-  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-  uint32_t r;
-  asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
-  return r;
-}
-__device__ __forceinline__ void cl_st(uint32_t addr, float2 v) {
-  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y)
-               : "memory");
-}
-__device__ __forceinline__ void cl_st_u32(uint32_t addr, uint32_t v) {
-  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
-}
-
-template <int C>
-__device__ __forceinline__ void dft_c(float2* v) {
-  if constexpr (C == 2) dft2<0>(v);
-  else if constexpr (C == 4) dft4<0>(v);
-  else dft8<0>(v);
-}
-
-// One station's U x C inputs of thread t (U = M / (C T)): the sample
-// m = m0 + T u + M c (m0 = r M/C + t - shift; zero outside [0, N)) into
-// v[u C + c] (.x primary, .y secondary).  Region c starts at words + c L and
-// lw is the thread's word index in a region; the sample's bits are rotated
-// into a byte offset of the level table as in the FFT-8192 kernel's decode.
-template <int C, int BITS, bool SPLIT, bool IMAG>
-__device__ __forceinline__ void cl_inputs(const uint32_t* __restrict__ words, const uint8_t* lvbase,
-                                          int m0, int lw, uint32_t rots, uint32_t tbase,
-                                          bool inside, float2 (&v)[16]) {
-  constexpr int N = C * kM, U = kM / (C * kT);
-  constexpr int SPW = 32 / BITS;
-  constexpr int L = cl_region_words(C, BITS);
-  constexpr int USTEP = kT / SPW;
-  constexpr uint32_t OMASK = ((1u << BITS) - 1u) << 2;
-  static_assert(U * C == 16, "16 inputs per thread");
-  const uint32_t r0 = rots & 31u, r1 = (rots >> 8) & 31u;
-  auto level = [&](uint32_t w) -> float {
-    uint32_t off;
-    if constexpr (SPLIT) {
-      off = (__funnelshift_r(w, w, r0) & 4u) | tbase;
-      off |= __funnelshift_r(w, w, r1) & 8u;
-    } else {
-      off = (__funnelshift_r(w, w, r0) & OMASK) | tbase;
-    }
-    return *reinterpret_cast<const float*>(lvbase + off);
-  };
-  auto put = [&](int i, float x) {
-    if (IMAG) v[i].y = x; else v[i].x = x;
-  };
-  if (inside) {
-    const uint32_t* w = words + lw;
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-#pragma unroll
-      for (int c = 0; c < C; ++c) put(u * C + c, level(w[c * L + u * USTEP]));
-  } else {
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-#pragma unroll
-      for (int c = 0; c < C; ++c) {
-        const int m = m0 + kT * u + kM * c;
-        const bool in = (unsigned)m < (unsigned)N;
-        const float x = level(words[in ? lw + c * L + u * USTEP : 0]);
-        put(u * C + c, in ? x : 0.0f);
-      }
-  }
-}
-
-template <int C, bool IMAG>
-__device__ __forceinline__ void cl_station(int bits, bool split, const uint32_t* words,
-                                           const uint8_t* lvbase, int m0, int lw, uint32_t rots,
-                                           uint32_t tbase, bool inside, float2 (&v)[16]) {
-  switch (bits) {
-    case 1: cl_inputs<C, 1, false, IMAG>(words, lvbase, m0, lw, rots, tbase, inside, v); break;
-    case 2:
-      if (split) cl_inputs<C, 2, true, IMAG>(words, lvbase, m0, lw, rots, tbase, inside, v);
-      else cl_inputs<C, 2, false, IMAG>(words, lvbase, m0, lw, rots, tbase, inside, v);
-      break;
-    case 4: cl_inputs<C, 4, false, IMAG>(words, lvbase, m0, lw, rots, tbase, inside, v); break;
-    default: cl_inputs<C, 8, false, IMAG>(words, lvbase, m0, lw, rots, tbase, inside, v); break;
-  }
-}
-
-__device__ __forceinline__ int log2_spw(int bits) {
-  return bits == 1 ? 5 : (bits == 2 ? 4 : (bits == 4 ? 3 : 2));
-}
 
 template <int C>
 __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(kT, 1)
@@ -387,8 +271,9 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(kT, 1)
       // the secondary station enters odd frames negated (undone by sgn below)
       const uint32_t tbS = 2048u + (uint32_t)((((uint32_t)mS & (uint32_t)lsbS) ^ (uint32_t)(it & 1u))
                                               << (bitsS + 2));
-      cl_station<C, false>(bitsP, splitP, wP, smem, mP, lwP, pos[cP], tbP, inP, v);
-      cl_station<C, true>(bitsS, splitS, wS, smem, mS, lwS, pos[32 + cS], tbS, inS, v);
+      cl_station<C, kM / C, 0, U, 8, false>(bitsP, splitP, wP, smem, mP, lwP, pos[cP], tbP, inP, v);
+      cl_station<C, kM / C, 0, U, 8, true>(bitsS, splitS, wS, smem, mS, lwS, pos[32 + cS], tbS, inS,
+                                           v);
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         float2 s[C], z[C];
