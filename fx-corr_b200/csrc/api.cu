@@ -483,7 +483,10 @@ fxc_status run_corr_stage(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uin
     CK(cudaEventRecord(ev->first, st));
   }
   int nblk = grid;  // partial rows to reduce
-  if (s->n > 8192 && !(s->n == 16384 && corr_fold2_supported(p))) {
+  if (s->n > 8192 && corr_pair_supported(s->n, p)) {
+    nblk = corr_pair_count(s->n, nf);
+    CK(launch_corr_pair(s->n, p, nblk, st));
+  } else if (s->n > 8192 && !(s->n == 16384 && corr_fold2_supported(p))) {
     nblk = corr_cluster_count(s->n, nf);
     if (nblk <= 0) return fail(FXC_EUNSUPPORTED, "no cluster of %d CTAs fits this GPU",
                                corr_cluster_size(s->n));
@@ -652,7 +655,8 @@ fxc_status scan_bind(fxc_scan* s, const fxc_scan_cfg* cfg) {
   uint64_t pel = maxg * (n > 8192 ? 5 : 4) * h;
   if (n == 16384) pel = std::max<uint64_t>(pel, (uint64_t)e->sm_count * 4 * h);
   if (n > 8192) {
-    const uint64_t c = (uint64_t)corr_cluster_size(n);
+    // clusters of C CTAs, or of C/2 (two rows per CTA) at FFT 32768 / 65536
+    const uint64_t c = (uint64_t)corr_cluster_size(n) / (n > 16384 ? 2 : 1);
     pel = std::max<uint64_t>(pel, ((uint64_t)e->sm_count + c - 1) / c * 4 * h);
   }
   const uint64_t bigf = n > 8192 ? (uint64_t)large_batch_frames(n) : 0;

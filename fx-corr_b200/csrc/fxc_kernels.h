@@ -82,6 +82,13 @@ int corr_cluster_size(uint32_t n);      // C, 0 when N has no cluster kernel
 int corr_cluster_capacity(uint32_t n);  // clusters resident at once (0: none)
 int corr_cluster_count(uint32_t n, uint64_t nf);  // clusters of a sector's launch
 cudaError_t launch_corr_cluster(uint32_t n, const CorrParams& p, int clusters, cudaStream_t s);
+// FFT 32768 / 65536 with 1- and 2-bit stations and a band shift that is a
+// multiple of C: clusters of C/2 CTAs, each owning a mirror pair of rows
+// (corr_pair.cu); partials [clusters][4][H].
+bool corr_pair_supported(uint32_t n, const CorrParams& p);
+int corr_pair_capacity(uint32_t n);
+int corr_pair_count(uint32_t n, uint64_t nf);
+cudaError_t launch_corr_pair(uint32_t n, const CorrParams& p, int clusters, cudaStream_t s);
 cudaError_t launch_reduce(const double* part, int nblk, int h, double m11, double m22, double m12,
                           double* out, cudaStream_t s);
 // FFT lengths above 8192 (N = c * 8192): global-memory four-step path.
