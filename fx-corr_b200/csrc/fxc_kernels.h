@@ -197,6 +197,11 @@ cudaError_t launch_phased_batch(uint32_t n, const BatchArgs& a, int grp, int gri
 cudaError_t launch_batch_reduce(const BatchArgs& a, int grid, cudaStream_t s);
 
 cudaError_t launch_phased(uint32_t n, const PhasedParams& p, int grid, cudaStream_t s);
+// FFT 16384 phased products with 1- and 2-bit stations: one CTA per frame
+// pair, both rows in shared memory (phased_pair.cu); partials [grid][H].
+bool phased_pair_supported(uint32_t n, const PhasedParams& p);
+int phased_pair_grid(int sms, uint64_t nf);
+cudaError_t launch_phased_pair(const PhasedParams& p, int grid, cudaStream_t s);
 cudaError_t launch_reduce_phased(const double* part, int nblk, int h, double* out, cudaStream_t s);
 cudaError_t launch_frame_info(const DelayParams& p, uint64_t first, uint64_t nf, int n,
                               double df_hz, int a1s, int a2s, FrameInfo* out, cudaStream_t s);

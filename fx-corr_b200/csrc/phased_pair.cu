@@ -1,0 +1,376 @@
+// phased_pair.cu — phased-array synthesis for FFT 16384 (yi-phasedarray,
+// src/main.rs:2222-2412) with 1- and 2-bit stations: one CTA per frame pair,
+// both 8192-point rows of the frame in its shared memory.
+//
+// Per frame pair (the contract of phased_kernel, whose N <= 8192 frame loop
+// holds a frame in one FFT):
+//   1. forward: each row of the radix-2 decimation in frequency,
+//      y_q[m] = W_N^(m q) (z[m] + (-1)^q z[m + M]), z = x1 + i x2, is decoded
+//      straight from the staged words by the FFT-16384 fold kernel's decode
+//      (fold_decode.cuh) into its first radix-16 pass; the row FFTs run in
+//      shared memory, the trailing radix-2 pass in place, so bin 2 j + q of
+//      the frame is Z_q[j];
+//   2. per bin: both stations' spectra from the shared FFT (two-for-one),
+//      each rotated by its fractional delay with the Nyquist imaginary part
+//      zeroed and multiplied by its fringe phasor, band-aligned onto the
+//      output grid and summed with the weights (src/main.rs:2264-2280,
+//      src/utils.rs:69-124); |cb|^2 accumulates in f32 registers (f64
+//      flushes every flush_every frames);
+//   3. for the .raw product: cb[0].im = cb[N/2].im = 0, the inverse real FFT
+//      as the forward FFT of the Hermitian-extended conj(cb) scaled by 1/N
+//      (src/utils.rs:60-66) through the same two-row decomposition (x[m] and
+//      x[m + M] gathered from cb), odd samples negated when both inputs are
+//      LSB, nearest-level re-quantisation with ant1's levels and packing with
+//      ant1's shuffle (src/utils.rs:378-410) of whole words from both rows.
+// Three padded row buffers; the staging slot and the output tables fill the
+// rest, which leaves room for 1- and 2-bit stations (the four-step path
+// serves the others).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "decode_tables.cuh"
+#include "fold_decode.cuh"
+#include "fxc_device.cuh"
+#include "fxc_kernels.h"
+
+namespace fxc {
+namespace {
+
+constexpr int kM = fold::kN;   // row length
+constexpr int kT = kM / 16;    // threads per CTA
+constexpr int kN2 = 2 * kM;    // frame length
+constexpr int kH2 = kN2 / 2 + 1;
+constexpr int kJ = kM / 2 / kT;  // bin pairs (rows 0 and 1) per thread
+
+// Shared memory (bytes): decode tables [0, 4608) (levels, rotate amounts;
+// 1- and 2-bit stations need no byte LUTs, so [4608, 12800) holds ant1's
+// output encode LUT); the gap [4352, 4608) holds the frame record, the
+// staging mbarrier, the error flag and the output levels; then the three row
+// buffers and one staging slot [FrameInfo (128 B)][station 1][station 2].
+constexpr uint32_t kPpFi = 4352, kPpBar = 4400, kPpFlag = 4408, kPpQl = 4416;  // 16 levels max
+constexpr uint32_t kPpEnc = kTabLut;  // [4][256] u32
+constexpr uint32_t kPpBuf = (uint32_t)Geom<kM>::CSTRIDE * (uint32_t)sizeof(float2);
+constexpr uint32_t kPpB0 = kTabEnd, kPpB1 = kPpB0 + kPpBuf, kPpB2 = kPpB1 + kPpBuf;
+constexpr uint32_t kPpStage = kPpB2 + kPpBuf;
+constexpr uint32_t kPpMaxSmem = 232448;  // 227 KB per CTA on sm_100
+static_assert(kPpFi + kFiBytes <= kPpBar && kPpQl + 16 * 4 <= kTabLut, "records fit the gap");
+static_assert(kPpStage % 128 == 0, "alignment");
+
+__host__ __device__ constexpr uint32_t pp_smem_bytes(uint32_t bpf1, uint32_t bpf2) {
+  return kPpStage + ((128u + bpf1 + bpf2 + 127u) & ~127u);
+}
+static_assert(pp_smem_bytes(kN2 / 4, kN2 / 4) <= kPpMaxSmem, "2-bit stations fit");
+
+// The trailing radix-2 pass of a row in place: Z[j], Z[j + M/2] from the last
+// radix-16 pass's output, j = t + T i.
+__device__ __forceinline__ void row_radix2(float2* Z, int tid, const Twiddles<kM>& tw) {
+#pragma unroll
+  for (int i = 0; i < kJ; ++i) {
+    const int j = tid + kT * i;
+    float2 wj;  // W_M^j = W_M^t W_16^i
+    switch (i) {  // compile-time after unrolling
+      case 0: wj = tw.w[Geom<kM>::P16]; break;
+      case 1: wj = mul_w16<1>(tw.w[Geom<kM>::P16]); break;
+      case 2: wj = mul_w16<2>(tw.w[Geom<kM>::P16]); break;
+      case 3: wj = mul_w16<3>(tw.w[Geom<kM>::P16]); break;
+      case 4: wj = mul_w16<4>(tw.w[Geom<kM>::P16]); break;
+      case 5: wj = mul_w16<5>(tw.w[Geom<kM>::P16]); break;
+      case 6: wj = mul_w16<6>(tw.w[Geom<kM>::P16]); break;
+      default: wj = mul_w16<7>(tw.w[Geom<kM>::P16]); break;
+    }
+    const float2 a = Z[j], wb = cmul(wj, Z[j + kM / 2]);
+    Z[j] = cadd(a, wb);
+    Z[j + kM / 2] = csub(a, wb);
+  }
+}
+
+// Row 1's decimation-in-frequency twiddle W_N^m, m = t + T r: W^t W_32^r from
+// the bases b0 = W_N^t and b1 = W_N^(t + T) (even / odd r) times W_16^(r/2).
+__device__ __forceinline__ void row1_twiddle(float2 (&v)[16], float2 b0, float2 b1) {
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    float2 w;
+    switch (r >> 1) {  // compile-time after unrolling
+      case 0: w = (r & 1) ? b1 : b0; break;
+      case 1: w = mul_w16<1>((r & 1) ? b1 : b0); break;
+      case 2: w = mul_w16<2>((r & 1) ? b1 : b0); break;
+      case 3: w = mul_w16<3>((r & 1) ? b1 : b0); break;
+      case 4: w = mul_w16<4>((r & 1) ? b1 : b0); break;
+      case 5: w = mul_w16<5>((r & 1) ? b1 : b0); break;
+      case 6: w = mul_w16<6>((r & 1) ? b1 : b0); break;
+      default: w = mul_w16<7>((r & 1) ? b1 : b0); break;
+    }
+    v[r] = cmul(v[r], w);
+  }
+}
+
+// First radix-16 pass of a row from its 16 inputs (t + T r) into a padded buffer.
+__device__ __forceinline__ void first_pass_regs(float2 (&v)[16], float2* dst, int tid) {
+  dft16(v);
+  float2* d = dst + 17 * tid;  // cpad(16 t + r) = 17 t + r
+#pragma unroll
+  for (int r = 0; r < 16; ++r) d[r] = v[out_pos<16>(r)];
+}
+
+__global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constant__ PhasedParams p) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const int tid = threadIdx.x;
+  FrameInfo* finfo = reinterpret_cast<FrameInfo*>(smem + kPpFi);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kPpBar);
+  int* flag = reinterpret_cast<int*>(smem + kPpFlag);
+  float* ql = reinterpret_cast<float*>(smem + kPpQl);
+  uint32_t* elut = reinterpret_cast<uint32_t*>(smem + kPpEnc);
+  const uint32_t* pos = reinterpret_cast<const uint32_t*>(smem + kTabPos);
+  float2* B0 = reinterpret_cast<float2*>(smem + kPpB0);
+  float2* B1 = reinterpret_cast<float2*>(smem + kPpB1);
+  float2* B2 = reinterpret_cast<float2*>(smem + kPpB2);
+  uint8_t* stage = smem + kPpStage;
+
+  const StationParams& s1 = p.st[0];
+  const StationParams& s2 = p.st[1];
+  const uint32_t bpf1 = s1.bpf, bpf2 = s2.bpf;
+  const uint64_t it0 = ((uint64_t)blockIdx.x * p.nf) / gridDim.x;
+  const uint64_t it1 = ((uint64_t)(blockIdx.x + 1) * p.nf) / gridDim.x;
+  double* part = p.partials + (size_t)blockIdx.x * kH2;
+
+  auto issue = [&](uint64_t it) {
+    mbar_expect_tx(bar, kFiBytes + bpf1 + bpf2);
+    bulk_g2s(stage, p.finfo + it, kFiBytes, bar);
+    bulk_g2s(stage + 128, s1.raw + it * bpf1, bpf1, bar);
+    bulk_g2s(stage + 128 + bpf1, s2.raw + it * bpf2, bpf2, bar);
+  };
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    *flag = 0;
+    fence_proxy_async();
+    if (it0 < it1) issue(it0);
+  }
+  build_decode_tables(s1, s2, false, false, smem, tid, kT);
+  for (int i = tid; i < 16; i += kT) ql[i] = i < (int)p.nqlevels ? p.qlevels[i] : 0.f;
+  for (int i = tid; i < 1024; i += kT) elut[i] = p.enc_lut[i];
+  const bool split1 = split_2bit(s1), split2 = split_2bit(s2);
+  Twiddles<kM> tw;
+  tw.init(tid);
+  // row 1's DIF twiddle bases W_N^t, W_N^(t + T), correctly rounded from FP64
+  float2 dtw0, dtw1;
+  {
+    double sn, cs;
+    sincospi(-2.0 * (double)tid / (double)kN2, &sn, &cs);
+    dtw0 = make_float2((float)cs, (float)sn);
+    sincospi(-2.0 * (double)(tid + kT) / (double)kN2, &sn, &cs);
+    dtw1 = make_float2((float)cs, (float)sn);
+  }
+  __syncthreads();
+
+  const int a1s = p.a1s, a1e = p.a1e, a2s = p.a2s;
+  const int ov = a1e - a1s, sb = a2s - a1s;
+  const bool g0 = p.grid == 0;
+  // output bin b: primary (on the output grid) at b, secondary at b + qoff
+  const int ovs = g0 ? a1s : a2s;
+  const int qoff = g0 ? sb : -sb;
+  // undo the two-for-one factor 2 and the exact per-station level scaling
+  const float u1 = 0.5f / s1.scale, u2 = 0.5f / s2.scale;
+  const int lsb1 = s1.lsb ? 1 : 0, lsb2 = s2.lsb ? 1 : 0;
+  const bool half = tid == 0;  // bin N/2
+  const uint32_t spw = 32u / p.bits_out;
+  const uint32_t wpf = (uint32_t)kN2 / spw;
+  const uint32_t qmask = (1u << p.bits_out) - 1u;
+  const float inv_n = 1.0f / (float)kN2;
+
+  // acc[2 i + q]: bin 2 (t + T i) + q; acc[2 kJ]: bin N/2
+  float acc[2 * kJ + 1];
+#pragma unroll
+  for (int i = 0; i <= 2 * kJ; ++i) acc[i] = 0.f;
+  bool first_flush = true;
+  uint32_t since_flush = 0;
+  auto flush = [&]() {
+#pragma unroll
+    for (int i = 0; i <= 2 * kJ; ++i) {
+      if (i == 2 * kJ && !half) continue;
+      const int bin = i == 2 * kJ ? kN2 / 2 : 2 * (tid + kT * (i >> 1)) + (i & 1);
+      double* d = part + bin;
+      *d = (first_flush ? 0.0 : *d) + (double)acc[i];
+      acc[i] = 0.f;
+    }
+    first_flush = false;
+    since_flush = 0;
+  };
+
+  uint32_t phase = 0;
+  bool stopped = false;
+  for (uint64_t it = it0; it < it1; ++it) {
+    if (!mbar_wait(bar, phase, kWaitPolls)) {
+      atomicOr(flag, 1);
+      atomicOr(p.err, ERR_WAIT_TIMEOUT);
+    }
+    phase ^= 1u;
+    __syncthreads();  // every thread past its wait, the flag visible
+    if (*flag) {
+      stopped = true;
+      break;
+    }
+    const uint32_t* w1 = reinterpret_cast<const uint32_t*>(stage + 128);
+    const uint32_t* w2 = reinterpret_cast<const uint32_t*>(stage + 128 + bpf1);
+    const FrameInfo* fs = reinterpret_cast<const FrameInfo*>(stage);
+    const int sh1 = fs->s1, sh2 = fs->s2;
+    if (tid == 0) *finfo = *fs;  // before the refill overwrites the slot
+    const float sg = (it & 1u) ? -1.0f : 1.0f;  // station 2 enters odd frames negated
+
+    // ---- 1. forward: rows 0 and 1 of the radix-2 DIF, decoded into their first pass
+    {
+      const int m1 = tid - sh1, m2 = tid - sh2;
+      const int c1 = m1 & ((32 / s1.bits) - 1), c2 = m2 & ((32 / s2.bits) - 1);
+      const uint32_t tb1 = (uint32_t)((m1 & lsb1) << (s1.bits + 2));
+      const uint32_t tb2 = 2048u + (uint32_t)((((uint32_t)m2 & (uint32_t)lsb2) ^ (uint32_t)(it & 1u))
+                                              << (s2.bits + 2));
+      for (int q = 0; q < 2; ++q) {
+        float2 v[16];
+        fold::fold_station<false, 2>(s1.bits, split1, w1, smem, sh1, pos[c1], tb1, v, tid, q == 1);
+        fold::fold_station<true, 2>(s2.bits, split2, w2, smem, sh2, pos[32 + c2], tb2, v, tid,
+                                    q == 1);
+        if (q == 1) row1_twiddle(v, dtw0, dtw1);
+        first_pass_regs(v, q == 0 ? B0 : B1, tid);
+        if (q == 0) {
+          fft_rest<kM, true>(B0, B2, tid, tw);  // row 0's spectrum in B0, unpadded
+          __syncthreads();
+          row_radix2(B0, tid, tw);
+        }
+      }
+    }
+    fft_rest<kM, true>(B1, B2, tid, tw);  // row 1's spectrum in B1
+    // the staged words are consumed (fft_rest opened with a barrier): refill
+    if (tid == 0 && it + 1 < it1) {
+      fence_proxy_async();
+      issue(it + 1);
+    }
+    __syncthreads();
+    row_radix2(B1, tid, tw);
+    __syncthreads();
+
+    // ---- 2. per bin: both stations rotated; the secondary one into B2 by bin
+    const FrameInfo& F = *finfo;
+    auto station = [&](float2 u, float2 w, int k, int s) -> float2 {
+      // spectrum of station s at its own bin k: unscaled, rotated by the
+      // station's fractional delay, Nyquist imaginary part zeroed, times fr_lo
+      float2 v = s == 0 ? make_float2(u1 * (u.x + w.x), u1 * (u.y - w.y))
+                        : make_float2(sg * u2 * (u.y + w.y), sg * u2 * (w.x - u.x));
+      float sn, cs;
+      __sincosf((float)k * (s == 0 ? F.st1 : F.st2), &sn, &cs);
+      v = cmul(v, make_float2(cs, sn));
+      if (k == kN2 / 2) v.y = 0.f;
+      return cmul(v, s == 0 ? F.fr_lo1 : F.fr_lo2);
+    };
+    const int sp = g0 ? 0 : 1;  // the station on the output grid
+    float2 prim[2 * kJ + 1];
+#pragma unroll
+    for (int i = 0; i < 2 * kJ; ++i) {
+      const int q = i & 1, j = tid + kT * (i >> 1), k = 2 * j + q;
+      const float2* Z = q ? B1 : B0;
+      const float2 u = Z[j];
+      const float2 w = q ? B1[kM - 1 - j] : B0[(kM - j) & (kM - 1)];  // Z[N - k]
+      prim[i] = station(u, w, k, sp);
+      B2[k] = station(u, w, k, 1 - sp);
+    }
+    prim[2 * kJ] = make_float2(0.f, 0.f);
+    if (half) {  // Z[N/2] = row 0's index M/2 pairs with itself
+      const float2 u = B0[kM / 2];
+      prim[2 * kJ] = station(u, u, kN2 / 2, sp);
+      B2[kN2 / 2] = station(u, u, kN2 / 2, 1 - sp);
+    }
+    __syncthreads();
+    // ---- band alignment and the weighted sum; cb by bin into B0
+    auto combine = [&](int b, float2 pv) -> float2 {
+      float2 sv = make_float2(0.f, 0.f);
+      if ((unsigned)(b - ovs) < (unsigned)ov) sv = B2[b + qoff];
+      // cb = w1 a1 + w2 a2 with a1 / a2 the station-1 / station-2 terms
+      const float2 a1 = g0 ? pv : sv, a2 = g0 ? sv : pv;
+      return make_float2(a1.x * p.w1 + a2.x * p.w2, a1.y * p.w1 + a2.y * p.w2);
+    };
+#pragma unroll
+    for (int i = 0; i < 2 * kJ; ++i) {
+      const int b = 2 * (tid + kT * (i >> 1)) + (i & 1);
+      float2 cb = combine(b, prim[i]);
+      acc[i] += cnorm2(cb);
+      if (b == 0) cb.y = 0.f;
+      B0[b] = cb;
+    }
+    if (half) {
+      float2 cb = combine(kN2 / 2, prim[2 * kJ]);
+      acc[2 * kJ] += cnorm2(cb);
+      cb.y = 0.f;
+      B0[kN2 / 2] = cb;
+    }
+    if (++since_flush >= p.flush_every) flush();
+
+    if (p.want_raw) {
+      __syncthreads();
+      // ---- 3. inverse: x[n] = conj(cb[n]) (n <= N/2), cb[N - n] (n > N/2);
+      // rows x[m] +- x[m + M] = conj(cb[m]) +- cb[M - m], m = t + T r
+      for (int q = 0; q < 2; ++q) {
+        float2 v[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+          const int m = tid + kT * r;
+          const float2 lo = B0[m], hi = B0[kM - m];
+          v[r] = q == 0 ? make_float2(lo.x + hi.x, hi.y - lo.y) : make_float2(lo.x - hi.x, -lo.y - hi.y);
+        }
+        if (q == 1) row1_twiddle(v, dtw0, dtw1);
+        if (q == 0) {
+          first_pass_regs(v, B1, tid);
+          fft_rest<kM, true>(B1, B2, tid, tw);  // X[2 k] (pre radix-2) in B1
+          __syncthreads();
+          row_radix2(B1, tid, tw);
+        } else {
+          first_pass_regs(v, B2, tid);
+          fft_rest<kM, true>(B2, B0, tid, tw);  // X[2 k + 1] in B2 (cb consumed)
+          __syncthreads();
+          row_radix2(B2, tid, tw);
+        }
+      }
+      __syncthreads();
+      // ---- re-quantise and pack: sample n is row n & 1, index n >> 1.  Each
+      // lane starts its word at a different sample so that a warp's loads
+      // spread over the banks.
+      uint8_t* out = p.raw_out + it * p.bpf_out;
+      const uint32_t lane = (uint32_t)tid & 31u;
+      const uint32_t rot = spw >= 16 ? lane : lane / (16u / spw);
+      for (uint32_t wdx = (uint32_t)tid; wdx < wpf; wdx += kT) {
+        uint32_t word = 0;
+        for (uint32_t i = 0; i < spw; ++i) {
+          const uint32_t ii = (i + rot) & (spw - 1u);
+          const uint32_t n = wdx * spw + ii;
+          float x = ((n & 1u) ? B2 : B1)[n >> 1].x * inv_n;
+          if (p.out_lsb && (n & 1u)) x = -x;
+          word |= (nearest_level(x, ql, (int)p.nqlevels, p.qmonotonic) & qmask) << (ii * p.bits_out);
+        }
+        reinterpret_cast<uint32_t*>(out)[wdx] =
+            elut[word & 255u] | elut[256 + ((word >> 8) & 255u)] |
+            elut[512 + ((word >> 16) & 255u)] | elut[768 + (word >> 24)];
+      }
+    }
+    __syncthreads();  // the buffers are free for the next frame
+  }
+  if (since_flush > 0 || first_flush) flush();
+  // never leave a bulk copy in flight into a finished CTA's shared memory
+  if (stopped && tid == 0) mbar_wait(bar, phase ^ 1u, kWaitPolls);
+}
+
+}  // namespace
+
+bool phased_pair_supported(uint32_t n, const PhasedParams& p) {
+  return n == (uint32_t)kN2 && p.st[0].bits <= 2 && p.st[1].bits <= 2 && p.bits_out <= 2;
+}
+
+int phased_pair_grid(int sms, uint64_t nf) {
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>(nf, (uint64_t)sms));
+}
+
+cudaError_t launch_phased_pair(const PhasedParams& p, int grid, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(phased_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kPpMaxSmem);
+  if (e != cudaSuccess) return e;
+  phased_pair_kernel<<<grid, kT, pp_smem_bytes(p.st[0].bpf, p.st[1].bpf), s>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace fxc
