@@ -449,14 +449,25 @@ fxc_status run_sector_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, 
       if (fst != FXC_OK) return fst;
       corr_done = true;
     }
-    // phased products: the two-row kernel for FFT 16384 with 1- and 2-bit
-    // stations, else the four-step path
+    // phased products with 1- and 2-bit stations: the two-row kernel (FFT
+    // 16384) or the cluster pair kernel (32768 / 65536, band shift a multiple
+    // of C); else the four-step path
     if (phased) {
       const PhasedParams pp = phased_params(s, r1, r2, nf, first, d_raw_out);
       if (phased_pair_supported(s->n, pp)) {
         if (!corr) CK(cudaMemsetAsync(d_acc, 0, sizeof(double) * 5 * h, st));
         const int g = phased_pair_grid(s->eng->sm_count, nf);
         CK(launch_phased_pair(pp, g, st));
+        CK(launch_reduce_phased(s->d_partials, g, (int)h, d_acc, st));
+        s->all_launches += 2;
+        return run_large(s, r1, r2, nf, first, d_acc, d_raw_out, corr && !corr_done, false, true,
+                         st);
+      }
+      if (phased_cpair_supported(s->n, pp)) {
+        if (!corr) CK(cudaMemsetAsync(d_acc, 0, sizeof(double) * 5 * h, st));
+        if (pp.want_raw) CK(cudaMemsetAsync(d_raw_out, 0, (size_t)nf * s->bpfo, st));
+        const int g = phased_cpair_count(s->n, nf);
+        CK(launch_phased_cpair(s->n, pp, g, st));
         CK(launch_reduce_phased(s->d_partials, g, (int)h, d_acc, st));
         s->all_launches += 2;
         return run_large(s, r1, r2, nf, first, d_acc, d_raw_out, corr && !corr_done, false, true,

@@ -202,6 +202,13 @@ cudaError_t launch_phased(uint32_t n, const PhasedParams& p, int grid, cudaStrea
 bool phased_pair_supported(uint32_t n, const PhasedParams& p);
 int phased_pair_grid(int sms, uint64_t nf);
 cudaError_t launch_phased_pair(const PhasedParams& p, int grid, cudaStream_t s);
+// FFT 32768 / 65536 phased products with 1- and 2-bit stations and a band
+// shift that is a multiple of C: clusters of C/2 CTAs in the correlation pair
+// kernel's row layout (phased_cpair.cu); partials [clusters][H]; the .raw
+// words are ORed together by the cluster's CTAs (zero them first).
+bool phased_cpair_supported(uint32_t n, const PhasedParams& p);
+int phased_cpair_count(uint32_t n, uint64_t nf);
+cudaError_t launch_phased_cpair(uint32_t n, const PhasedParams& p, int clusters, cudaStream_t s);
 cudaError_t launch_reduce_phased(const double* part, int nblk, int h, double* out, cudaStream_t s);
 cudaError_t launch_frame_info(const DelayParams& p, uint64_t first, uint64_t nf, int n,
                               double df_hz, int a1s, int a2s, FrameInfo* out, cudaStream_t s);
