@@ -227,6 +227,13 @@ __global__ void __cluster_dims__(C / 2, 1, 1) __launch_bounds__(kT, 1)
   const bool splitP = split_2bit(sp), splitS = split_2bit(ss);
   Twiddles<kM> tw;
   tw.init(tid);
+  // W_M^(t+1): the mirror half's trailing radix-2 twiddle (correctly rounded)
+  float2 wb1;
+  {
+    double sn, cs;
+    sincospi(-2.0 * (double)(tid + 1) / (double)kM, &sn, &cs);
+    wb1 = make_float2((float)cs, (float)sn);
+  }
   // radix-C step twiddle bases W_N^m of the thread's columns m = r CW + t + T u
   float2 dbase[U];
 #pragma unroll
@@ -368,28 +375,6 @@ __global__ void __cluster_dims__(C / 2, 1, 1) __launch_bounds__(kT, 1)
     }
     fft_rest<kM, true>(Y, XA, tid, tw);  // result in Y, unpadded
     __syncthreads();
-    // trailing radix-2 pass in place: Z[j], Z[j + M/2]
-    auto radix2 = [&](float2* Z) {
-#pragma unroll
-      for (int i = 0; i < kJ; ++i) {
-        const int j = tid + kT * i;
-        float2 wj;  // W_M^j = W_M^t W_16^i
-        switch (i) {  // compile-time after unrolling
-          case 0: wj = tw.w[Geom<kM>::P16]; break;
-          case 1: wj = mul_w16<1>(tw.w[Geom<kM>::P16]); break;
-          case 2: wj = mul_w16<2>(tw.w[Geom<kM>::P16]); break;
-          case 3: wj = mul_w16<3>(tw.w[Geom<kM>::P16]); break;
-          case 4: wj = mul_w16<4>(tw.w[Geom<kM>::P16]); break;
-          case 5: wj = mul_w16<5>(tw.w[Geom<kM>::P16]); break;
-          case 6: wj = mul_w16<6>(tw.w[Geom<kM>::P16]); break;
-          default: wj = mul_w16<7>(tw.w[Geom<kM>::P16]); break;
-        }
-        const float2 a = Z[j], wb = cmul(wj, Z[j + kM / 2]);
-        Z[j] = cadd(a, wb);
-        Z[j + kM / 2] = csub(a, wb);
-      }
-    };
-    radix2(Y);
     // ---- row B: XB -> XA (first pass), then XA <-> XB, spectrum in XA
     {
       float2 v[16];
@@ -401,8 +386,6 @@ __global__ void __cluster_dims__(C / 2, 1, 1) __launch_bounds__(kT, 1)
       for (int q = 0; q < 16; ++q) dst[q] = v[out_pos<16>(q)];
     }
     fft_rest<kM, true>(XA, XB, tid, tw);  // result in XA, unpadded
-    __syncthreads();
-    radix2(XA);
     __syncthreads();
 
     // ---- 3./4. per row: two-for-one split from the CTA's own spectra, the
@@ -422,24 +405,42 @@ __global__ void __cluster_dims__(C / 2, 1, 1) __launch_bounds__(kT, 1)
     auto row_pass = [&](auto rb) {
       constexpr int RB = decltype(rb)::value;
       const int row = RB ? rowB : rowA;
-      const float2* Z = RB ? XA : Y;
+      // the rows' last radix-16 pass outputs (unpadded): Z[j] = Yo[j] + W^j Yo[j + M/2];
+      // the mirror row's upper half Z[c + M/2] = Ym[c] - W^c Ym[c + M/2] with
+      // W^c = -conj(W^(M/2 - c)), folded here instead of a radix-2 pass in place
+      const float2* Yo = RB ? XA : Y;
+      const float2* Ym = RB ? (r == 0 ? XA : Y) : (r == 0 ? Y : XA);
+      constexpr bool kSelf0Row = RB == 0;  // row 0 (CTA 0's row A) mirrors at M - j
       float2* Q = RB ? QB : QA;
       float2 prim[kJ];
 #pragma unroll
       for (int i = 0; i < kJ; ++i) {
         const int j = tid + kT * i;
-        const float2 u = Z[j];
-        float2 w;  // Z[N - k], k = C j + row
-        if (RB == 0) w = r == 0 ? Y[(kM - j) & (kM - 1)] : XA[kM - 1 - j];
-        else w = r == 0 ? XA[kM - 1 - j] : Y[kM - 1 - j];
+        float2 wj, wj1;  // W_M^j = W_M^t W_16^i, W_M^(j+1) = W_M^(t+1) W_16^i
+        switch (i) {  // compile-time after unrolling
+          case 0: wj = tw.w[Geom<kM>::P16]; wj1 = wb1; break;
+          case 1: wj = mul_w16<1>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<1>(wb1); break;
+          case 2: wj = mul_w16<2>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<2>(wb1); break;
+          case 3: wj = mul_w16<3>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<3>(wb1); break;
+          case 4: wj = mul_w16<4>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<4>(wb1); break;
+          case 5: wj = mul_w16<5>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<5>(wb1); break;
+          case 6: wj = mul_w16<6>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<6>(wb1); break;
+          default: wj = mul_w16<7>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<7>(wb1); break;
+        }
+        const float2 u = cadd(Yo[j], cmul(wj, Yo[j + kM / 2]));  // Z[j]
+        // Z[N - k], k = C j + row: the mirror row's index M - 1 - j (row 0: M - j)
+        const bool self0 = kSelf0Row && r == 0;
+        const int c = self0 ? ((kM / 2 - j) & (kM / 2 - 1)) : kM / 2 - 1 - j;
+        float2 w = cadd(Ym[c], cmulc(Ym[c + kM / 2], self0 ? wj : wj1));
+        if (self0 && j == 0) w = u;  // bin 0 pairs with itself
         prim[i] = make_float2(u.x + w.x, u.y - w.y);
         const int kp = C * j + row - qoff;
         if ((unsigned)(kp - ovs) < (unsigned)ov)
           Q[j + dq] = make_float2(sgn * (u.y + w.y), sgn * (w.x - u.x));
       }
       float2 prim_h = make_float2(0.f, 0.f);
-      if (RB == 0 && half) {  // Z[N/2] pairs with itself
-        const float2 u = Y[kM / 2];
+      if (RB == 0 && half) {  // Z[N/2] = Y[0] - Y[M/2] pairs with itself
+        const float2 u = csub(Y[0], Y[kM / 2]);
         prim_h = make_float2(2.f * u.x, 0.f);
         const int kp = N / 2 - qoff;
         if ((unsigned)(kp - ovs) < (unsigned)ov) Q[kM / 2 + dq] = make_float2(sgn * 2.f * u.y, 0.f);
