@@ -505,6 +505,82 @@ def batch_leg(fxc, torch, eng, n_sectors=64, calls=20, warm=3, seed=8383):
     return out
 
 
+def batch_mixed_leg(fxc, torch, eng, n_scans=64, calls=10, warm=3, seed=9494):
+    """The batched multi-scan schedule's shape: one fxc_batch call = one
+    sector each of n_scans scans with FFT lengths {1024, 4096, 16384}, bit
+    depths {1, 2, 4} (both stations) and, alternately, the correlation
+    (ACF x2 + XCF) or the phased (power + .raw) products; uneven sectors of
+    0.05-0.3 s at 512 Msps with random delays; CUDA graphs and the autotuner
+    on; CUDA events around each call.  Device-resident random .raw bytes."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ffts, bitss = (1024, 4096, 16384), (1, 2, 4)
+    fs = 512e6
+    specs = []
+    for k in range(n_scans):
+        fft = ffts[k % 3]
+        bits = bitss[(k // 3) % 3]
+        phased = (k // 9) % 2 == 1
+        nf = max(1, int(rng.uniform(0.05, 0.3) * fs / fft))
+        delay = dict(net_d1_base=float(rng.uniform(-3e-6, 3e-6)),
+                     total_rate1_base=float(rng.uniform(-2e-6, 2e-6)), lo1_hz=8.4e9, lo2_hz=8.4e9)
+        specs.append((fft, bits, phased, nf, delay))
+    levels = {1: [-1.0, 1.0], 2: [-3.0, -1.0, 1.0, 3.0],
+              4: [float(v) for v in np.arange(-7.5, 8.0, 1.0)]}
+    scans, r1, r2, accs, nfs, raws = [], [], [], [], [], []
+    tot = sum(nf * fft * bits // 8 for fft, bits, _, nf, _ in specs)
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    d = torch.randint(0, 256, (2, tot), dtype=torch.uint8, device="cuda", generator=g)
+    off = 0
+    for fft, bits, phased, nf, delay in specs:
+        c = fxc.ScanConfig(fft=fft, fs=fs, bits1=bits, bits2=bits, levels1=levels[bits],
+                           levels2=levels[bits], shuffle1=shuffle_internal(101),
+                           shuffle2=shuffle_internal(102),
+                           products=(fxc.PROD_PHASED | fxc.PROD_RAW) if phased
+                           else (fxc.PROD_ACF | fxc.PROD_XCF), delay=delay)
+        scans.append(eng.open_scan(c))
+        n = nf * c.bpf(bits)
+        r1.append(d[0, off:off + n])
+        r2.append(d[1, off:off + n])
+        off += n
+        accs.append(torch.empty(5 * c.h, dtype=torch.float64, device="cuda"))
+        raws.append(torch.empty(n, dtype=torch.uint8, device="cuda") if phased else None)
+        nfs.append(nf)
+    b = fxc.Batch(eng, use_graphs=True, autotune=True)
+    st = torch.cuda.current_stream()
+    firsts = [0] * n_scans
+    for _ in range(warm):
+        b.run_device_raw(scans, r1, r2, nfs, firsts, accs, raws, stream=st)
+    torch.cuda.synchronize()
+    l0 = b.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(calls):
+        b.run_device_raw(scans, r1, r2, nfs, firsts, accs, raws, stream=st)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / calls
+    for s in scans:
+        s.check()
+    samples = sum(2.0 * fft * nf for fft, _, _, nf, _ in specs)
+    # sectors a batch cannot hold run through their scans' own kernels inside
+    # the call: phased FFT 16384 (the two-row kernel for 1- and 2-bit
+    # stations, the four-step path for 4-bit ones)
+    per_scan = sum(1 for fft, _, phased, _, _ in specs if phased and fft == 16384)
+    out = {"gsample_s": samples / (ms * 1e-3) / 1e9, "ms_per_call": ms, "scans": n_scans,
+           "frame_pairs_per_call": int(sum(nfs)), "input_bytes_per_call": 2 * tot,
+           "kernels_per_call": (b.launches() - l0) / calls,
+           "sectors_in_persistent_kernels": n_scans - per_scan,
+           "sectors_through_per_scan_kernels": per_scan,
+           "mix": "FFT {1024, 4096, 16384} x bits {1, 2, 4} x {ACF+XCF, phased power + .raw}, "
+                  "0.05-0.3 s sectors at 512 Msps, random delays",
+           "path": "fxc_batch_run_device_raw (CUDA graph replay, autotuned), device-resident"}
+    b.close()
+    for s in scans:
+        s.close()
+    del d
+    return out
+
+
 def serve_leg(fxc, torch, eng, jobs, slots, batch, plain_jobs=None, label="", mix=""):
     """Served (fxc_server, continuous batching) vs plain (one job at a time:
     scan open, per sector a synchronous H2D + kernels + dump, scan close) on
@@ -854,9 +930,13 @@ def main():
     clk = clocks.stop()
 
     # ---- batched sectors of many short scans, device-resident (rank 0 of N=1)
-    batched = None
+    batched = batched_mixed = None
     if rank == 0 and world == 1 and not args.no_batch:
         batched = batch_leg(fxc, torch, eng)
+        try:
+            batched_mixed = batch_mixed_leg(fxc, torch, eng)
+        except Exception as e:  # report, keep the rest of the line
+            batched_mixed = {"error": str(e)[:300]}
 
     # ---- serving: continuous batching vs one job at a time (rank 0 of N=1)
     serve = None
@@ -930,6 +1010,7 @@ def main():
             "parity": parity,
             "e2e": e2e,
             "batched": batched,
+            "batched_mixed": batched_mixed,
             "serving": serve,
             "gpu_launches": all_launches,
             "clocks": clk,
