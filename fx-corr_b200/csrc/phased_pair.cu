@@ -65,6 +65,9 @@ static_assert(pp_smem_bytes(kN2 / 4, kN2 / 4) <= kPpMaxSmem, "2-bit stations fit
 using rows::first_pass_regs;
 using rows::row1_twiddle;
 using rows::row_radix2;
+using rows::fold_lower;
+using rows::fold_mirror;
+using rows::fold_twiddles;
 
 __global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constant__ PhasedParams p) {
   extern __shared__ __align__(128) uint8_t smem[];
@@ -105,6 +108,7 @@ __global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constan
   const bool split1 = split_2bit(s1), split2 = split_2bit(s2);
   Twiddles<kM> tw;
   tw.init(tid);
+  const float2 wb1 = rows::fold_base1(tid);  // W_M^(t+1)
   // row 1's DIF twiddle bases W_N^t, W_N^(t + T), correctly rounded from FP64
   float2 dtw0, dtw1;
   {
@@ -184,11 +188,7 @@ __global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constan
                                     q == 1);
         if (q == 1) row1_twiddle(v, dtw0, dtw1);
         first_pass_regs(v, q == 0 ? B0 : B1, tid);
-        if (q == 0) {
-          fft_rest<kM, true>(B0, B2, tid, tw);  // row 0's spectrum in B0, unpadded
-          __syncthreads();
-          row_radix2(B0, tid, tw);
-        }
+        if (q == 0) fft_rest<kM, true>(B0, B2, tid, tw);  // row 0's last pass output in B0
       }
     }
     fft_rest<kM, true>(B1, B2, tid, tw);  // row 1's spectrum in B1
@@ -197,8 +197,6 @@ __global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constan
       fence_proxy_async();
       issue(it + 1);
     }
-    __syncthreads();
-    row_radix2(B1, tid, tw);
     __syncthreads();
 
     // ---- 2. per bin: both stations rotated; the secondary one into B2 by bin
@@ -217,17 +215,25 @@ __global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constan
     const int sp = g0 ? 0 : 1;  // the station on the output grid
     float2 prim[2 * kJ + 1];
 #pragma unroll
-    for (int i = 0; i < 2 * kJ; ++i) {
-      const int q = i & 1, j = tid + kT * (i >> 1), k = 2 * j + q;
-      const float2* Z = q ? B1 : B0;
-      const float2 u = Z[j];
-      const float2 w = q ? B1[kM - 1 - j] : B0[(kM - j) & (kM - 1)];  // Z[N - k]
-      prim[i] = station(u, w, k, sp);
-      B2[k] = station(u, w, k, 1 - sp);
+    for (int i2 = 0; i2 < kJ; ++i2) {
+      const int j = tid + kT * i2;
+      float2 wj, wj1;
+      fold_twiddles(tw, wb1, i2, wj, wj1);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        // the rows' trailing radix-2 pass folded in: Z_q[j] and Z[N - k],
+        // which is row 1's index M - 1 - j or row 0's index M - j
+        const int k = 2 * j + q;
+        const float2* Y = q ? B1 : B0;
+        const float2 u = fold_lower(Y, j, wj);
+        const float2 w = fold_mirror(Y, j, q == 0, wj, wj1);
+        prim[2 * i2 + q] = station(u, w, k, sp);
+        B2[k] = station(u, w, k, 1 - sp);
+      }
     }
     prim[2 * kJ] = make_float2(0.f, 0.f);
-    if (half) {  // Z[N/2] = row 0's index M/2 pairs with itself
-      const float2 u = B0[kM / 2];
+    if (half) {  // Z[N/2] = row 0's index M/2 (Y[0] - Y[M/2]) pairs with itself
+      const float2 u = csub(B0[0], B0[kM / 2]);
       prim[2 * kJ] = station(u, u, kN2 / 2, sp);
       B2[kN2 / 2] = station(u, u, kN2 / 2, 1 - sp);
     }

@@ -1,7 +1,7 @@
 // row_fft.cuh — pieces of the 8192-point row FFTs shared by the kernels that
 // hold whole rows in shared memory (phased_pair.cu, phased_cpair.cu): the
-// trailing radix-2 pass in place, a radix-2 decimation-in-frequency twiddle,
-// and the first radix-16 pass from registers.
+// trailing radix-2 pass in place or folded into its reader, a radix-2
+// decimation-in-frequency twiddle, and the first radix-16 pass from registers.
 #pragma once
 
 #include "fxc_device.cuh"
@@ -34,6 +34,44 @@ __device__ __forceinline__ void row_radix2(float2* Z, int tid, const Twiddles<kM
     Z[j] = cadd(a, wb);
     Z[j + kM / 2] = csub(a, wb);
   }
+}
+
+// The trailing radix-2 pass folded into a reader (no write-back): with Y the
+// last radix-16 pass's output (unpadded) and j = t + T i, j < M/2,
+//   Z[j]            = Y[j] + W^j Y[j + M/2]
+//   Z[c + M/2]      = Y[c] + conj(W^(M/2 - c)) Y[c + M/2]     (W^c = -conj(W^(M/2-c)))
+// so the mirror's upper-half values at c = M/2 - 1 - j (index M - 1 - j) take
+// W^(j+1) and at c = M/2 - j (index M - j) take W^j.  wb1 = W_M^(t+1).
+__device__ __forceinline__ void fold_twiddles(const Twiddles<kM>& tw, float2 wb1, int i, float2& wj,
+                                              float2& wj1) {
+  switch (i) {  // compile-time after unrolling
+    case 0: wj = tw.w[Geom<kM>::P16]; wj1 = wb1; break;
+    case 1: wj = mul_w16<1>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<1>(wb1); break;
+    case 2: wj = mul_w16<2>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<2>(wb1); break;
+    case 3: wj = mul_w16<3>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<3>(wb1); break;
+    case 4: wj = mul_w16<4>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<4>(wb1); break;
+    case 5: wj = mul_w16<5>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<5>(wb1); break;
+    case 6: wj = mul_w16<6>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<6>(wb1); break;
+    default: wj = mul_w16<7>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<7>(wb1); break;
+  }
+}
+// Z[j] of a row (j < M/2).
+__device__ __forceinline__ float2 fold_lower(const float2* Y, int j, float2 wj) {
+  return cadd(Y[j], cmul(wj, Y[j + kM / 2]));
+}
+// Z[M - 1 - j] (self0 false: wk = W^(j+1)) or Z[(M - j) mod M] (self0 true:
+// wk = W^j; j = 0 gives Z[0]) of a row, j < M/2.
+__device__ __forceinline__ float2 fold_mirror(const float2* Y, int j, bool self0, float2 wj,
+                                              float2 wj1) {
+  if (self0 && j == 0) return fold_lower(Y, 0, wj);
+  const int c = self0 ? kM / 2 - j : kM / 2 - 1 - j;
+  return cadd(Y[c], cmulc(Y[c + kM / 2], self0 ? wj : wj1));
+}
+// W_M^(t+1), correctly rounded.
+__device__ __forceinline__ float2 fold_base1(int t) {
+  double sn, cs;
+  sincospi(-2.0 * (double)(t + 1) / (double)kM, &sn, &cs);
+  return make_float2((float)cs, (float)sn);
 }
 
 // Row 1's twiddle W_N^m of a radix-2 decimation in frequency (N = 2 M),
