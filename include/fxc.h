@@ -204,7 +204,7 @@ FXC_API fxc_status fxc_scan_profile(fxc_scan* s, double* kernel_ms, uint64_t* ke
  * larger requests fail with FXC_EINVAL / FXC_EUNSUPPORTED.  Runs on the
  * current device, enqueued on `stream`, which must belong to that device
  * (FXC_EINVAL otherwise).  The first call on each device looks up the array's
- * device address, so make that first call before any stream capture.  All
+ * device address (cudaGetSymbolAddress) and caches it.  All
  * calls share the array: calls whose work overlaps on one GPU (other streams
  * or host threads) race and must be serialised by the caller.
  *
