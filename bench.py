@@ -563,9 +563,8 @@ def batch_mixed_leg(fxc, torch, eng, n_scans=64, calls=10, warm=3, seed=9494):
         s.check()
     samples = sum(2.0 * fft * nf for fft, _, _, nf, _ in specs)
     # sectors a batch cannot hold run through their scans' own kernels inside
-    # the call: phased FFT 16384 (the two-row kernel for 1- and 2-bit
-    # stations, the four-step path for 4-bit ones)
-    per_scan = sum(1 for fft, _, phased, _, _ in specs if phased and fft == 16384)
+    # the call: phased FFT 16384 with 4-bit stations (the four-step path)
+    per_scan = sum(1 for fft, bits, phased, _, _ in specs if phased and fft == 16384 and bits > 2)
     out = {"gsample_s": samples / (ms * 1e-3) / 1e9, "ms_per_call": ms, "scans": n_scans,
            "frame_pairs_per_call": int(sum(nfs)), "input_bytes_per_call": 2 * tot,
            "kernels_per_call": (b.launches() - l0) / calls,

@@ -341,9 +341,8 @@ LargeParams large_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2
   return p;
 }
 
-// FFT lengths above 8192: batches of frames through the global-memory path,
-// per-frame-group f64 partials, then the fixed-order reduction.  The frame
-// records of the sector must already be staged.
+// The phased kernels' parameters of a sector (every phased kernel, per scan or
+// batched).  The frame records of the sector must already be staged.
 PhasedParams phased_params(const fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uint64_t nf,
                            uint64_t first, uint8_t* d_raw_out) {
   PhasedParams p{};
@@ -1320,14 +1319,17 @@ fxc_status batch_describe(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uin
     return fail(FXC_EINVAL, "the scan writes phased .raw frames but its raw output is NULL");
   if (nf == 0 || (corr && phased)) return FXC_OK;  // the per-scan path
   if (phased) {
-    // phased sectors of FFT 1024..8192 run in the phased batch kernels
-    if (s->n > 8192) return FXC_OK;
+    // phased sectors of FFT 1024..8192 run in the phased batch kernels, FFT
+    // 16384 with 1- and 2-bit stations in the two-row kernel's batch group
+    if (s->n > 16384) return FXC_OK;
+    const PhasedParams pp = phased_params(s, r1, r2, nf, first, d_raw_out);
+    if (s->n == 16384 && !phased_pair_supported(s->n, pp)) return FXC_OK;
     if ((st = grow_frame_info(s, nf)) != FXC_OK) return st;
     BatchScan b{};
     b.p = corr_params(s, r1, r2, nf, first);  // delay model and frame records
     b.p.finfo = s->d_finfo;
     b.p.partials = nullptr;
-    b.pp = phased_params(s, r1, r2, nf, first, d_raw_out);
+    b.pp = pp;
     b.pp.finfo = s->d_finfo;
     b.pp.partials = nullptr;  // the batch's
     b.acc = d_acc;
@@ -1336,7 +1338,7 @@ fxc_status batch_describe(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uin
     b.phased = 1;
     *out = b;
     *group = s->n == 1024 ? BG_PHASED_1024 : s->n == 2048 ? BG_PHASED_2048
-           : s->n == 4096 ? BG_PHASED_4096 : BG_PHASED_8192;
+           : s->n == 4096 ? BG_PHASED_4096 : s->n == 8192 ? BG_PHASED_8192 : BG_PHASED_16384;
     return FXC_OK;
   }
   if (s->n > 16384) return FXC_OK;

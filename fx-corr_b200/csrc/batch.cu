@@ -42,16 +42,19 @@ namespace {
   } while (0)
 
 constexpr uint32_t kGroupN[kBatchGroups] = {1024, 2048, 4096, 8192, 16384,
-                                            1024, 2048, 4096, 8192};
+                                            1024, 2048, 4096, 8192, 16384};
 // kernel variants (frame pairs per CTA iteration) of each group; the phased
 // groups have one variant each (the single-scan phased kernel's)
 const std::vector<int> kGroupFpc[kBatchGroups] = {{1, 2, 4}, {1, 2, 4}, {1, 2}, {1}, {1},
-                                                  {4}, {2}, {1}, {1}};
+                                                  {4}, {2}, {1}, {1}, {1}};
 // single-scan defaults: the frames per iteration of corr_kernel / phased_kernel
-constexpr int kDefaultFpc[kBatchGroups] = {4, 2, 1, 1, 1, 4, 2, 1, 1};
+constexpr int kDefaultFpc[kBatchGroups] = {4, 2, 1, 1, 1, 4, 2, 1, 1, 1};
 
 bool phased_group(int g) { return g >= kCorrGroups; }
-constexpr uint32_t kDefaultItemFrames = 128;
+// Default frames per item (the tuner replaces a correlation group's).  Items
+// of the FFT-16384 phased group take ~0.8 ms at 32 frames: larger ones leave
+// SMs idle for up to an item's time after the last tickets of a call.
+constexpr uint32_t kDefaultItems[kBatchGroups] = {128, 128, 128, 128, 128, 128, 128, 128, 128, 32};
 const uint32_t kItemCandidates[] = {32, 64, 128, 256, 512};
 
 // The correlation group of FFT length n (-1: none).
@@ -65,7 +68,7 @@ uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
 struct Shape {
   int fpc = 1;
-  uint32_t item_frames = kDefaultItemFrames;
+  uint32_t item_frames = 128;
   int ctas = 0;  // resident CTAs per SM of the variant
   double gsps = 0.0;
   bool tuned = false;
@@ -555,7 +558,7 @@ fxc_status fxc_batch_create(fxc_engine* e, const fxc_batch_opts* opts, fxc_batch
   b->item_override = opts ? opts->item_frames : 0;
   for (int g = 0; g < kBatchGroups; ++g) {
     b->shape[g].fpc = kDefaultFpc[g];
-    b->shape[g].item_frames = b->item_override ? b->item_override : kDefaultItemFrames;
+    b->shape[g].item_frames = b->item_override ? b->item_override : kDefaultItems[g];
   }
   DeviceGuardB dg(b->device);
   auto bail = [&](cudaError_t err) {

@@ -132,7 +132,7 @@ cudaError_t launch_large_split(const LargeParams& p, const float2* Y, uint64_t f
 enum {
   BG_1024 = 0, BG_2048 = 1, BG_4096 = 2, BG_8192 = 3, BG_16384 = 4,
   BG_PHASED_1024 = 5, BG_PHASED_2048 = 6, BG_PHASED_4096 = 7, BG_PHASED_8192 = 8,
-  kCorrGroups = 5, kBatchGroups = 9
+  BG_PHASED_16384 = 9, kCorrGroups = 5, kBatchGroups = 10
 };
 
 // Frames [f0, f1) of the sector of scan `scan` (for the two-row kernel, the
@@ -189,7 +189,7 @@ cudaError_t launch_batch_group(int g, int fpc, const BatchArgs& a, int grid, cud
 // every sector's partials into its acc (grid-stride, any grid size).
 cudaError_t launch_batch_frame_info(const BatchArgs& a, int grid, cudaStream_t s);
 // Phased batch groups (phased_kernels.cu): FFT n in 1024..8192, frames per CTA
-// iteration as the single-scan phased kernel.
+// iteration as the single-scan phased kernel; n = 16384 the two-row kernel's.
 cudaError_t phased_batch_prepare(uint32_t n);
 int phased_batch_ctas_per_sm(uint32_t n);
 int phased_frames_per_cta_iter(uint32_t n);
@@ -202,6 +202,11 @@ cudaError_t launch_phased(uint32_t n, const PhasedParams& p, int grid, cudaStrea
 bool phased_pair_supported(uint32_t n, const PhasedParams& p);
 int phased_pair_grid(int sms, uint64_t nf);
 cudaError_t launch_phased_pair(const PhasedParams& p, int grid, cudaStream_t s);
+// Its persistent batch form (group BG_PHASED_16384, sectors that
+// phased_pair_supported accepts): shared-memory limit, occupancy, launch.
+cudaError_t phased_pair_batch_prepare();
+int phased_pair_batch_ctas_per_sm();
+cudaError_t launch_phased_pair_batch(const BatchArgs& a, int grp, int grid, cudaStream_t s);
 // FFT 32768 / 65536 phased products with 1- and 2-bit stations and a band
 // shift that is a multiple of C: clusters of C/2 CTAs in the correlation pair
 // kernel's row layout (phased_cpair.cu); partials [clusters][H]; the .raw

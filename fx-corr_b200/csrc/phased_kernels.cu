@@ -385,9 +385,11 @@ uint32_t phased_batch_smem() {
 }  // namespace
 
 // Batch groups of the phased kernels: FFT 1024 / 2048 / 4096 / 8192 with the
-// single-scan kernels' frames per CTA iteration (4 / 2 / 1 / 1).
+// single-scan kernels' frames per CTA iteration (4 / 2 / 1 / 1); FFT 16384
+// (1- and 2-bit stations) is the two-row kernel's group (phased_pair.cu).
 cudaError_t phased_batch_prepare(uint32_t n) {
   switch (n) {
+    case 16384: return phased_pair_batch_prepare();
     case 1024: return cudaFuncSetAttribute(phased_batch_kernel<1024, 4>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)phased_batch_smem<1024, 4>());
@@ -420,6 +422,7 @@ int phased_batch_ctas_per_sm(uint32_t n) {
     case 8192: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, phased_batch_kernel<8192, 1>,
                                                                  512, phased_batch_smem<8192, 1>());
       break;
+    case 16384: return phased_pair_batch_ctas_per_sm();
     default: break;
   }
   return e == cudaSuccess ? nb : 0;
@@ -433,6 +436,7 @@ cudaError_t launch_phased_batch(uint32_t n, const BatchArgs& a, int grp, int gri
     case 2048: phased_batch_kernel<2048, 2><<<grid, 256, phased_batch_smem<2048, 2>(), s>>>(a, grp); break;
     case 4096: phased_batch_kernel<4096, 1><<<grid, 256, phased_batch_smem<4096, 1>(), s>>>(a, grp); break;
     case 8192: phased_batch_kernel<8192, 1><<<grid, 512, phased_batch_smem<8192, 1>(), s>>>(a, grp); break;
+    case 16384: return launch_phased_pair_batch(a, grp, grid, s);
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -48,7 +48,8 @@ constexpr int kJ = kM / 2 / kT;  // bin pairs (rows 0 and 1) per thread
 // output encode LUT); the gap [4352, 4608) holds the frame record, the
 // staging mbarrier, the error flag and the output levels; then the three row
 // buffers and one staging slot [FrameInfo (128 B)][station 1][station 2].
-constexpr uint32_t kPpFi = 4352, kPpBar = 4400, kPpFlag = 4408, kPpQl = 4416;  // 16 levels max
+constexpr uint32_t kPpFi = 4352, kPpBar = 4400, kPpFlag = 4408, kPpTicket = 4412;
+constexpr uint32_t kPpQl = 4416;  // 16 levels max
 constexpr uint32_t kPpEnc = kTabLut;  // [4][256] u32
 constexpr uint32_t kPpBuf = (uint32_t)Geom<kM>::CSTRIDE * (uint32_t)sizeof(float2);
 constexpr uint32_t kPpB0 = kTabEnd, kPpB1 = kPpB0 + kPpBuf, kPpB2 = kPpB1 + kPpBuf;
@@ -69,8 +70,49 @@ using rows::fold_lower;
 using rows::fold_mirror;
 using rows::fold_twiddles;
 
-__global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constant__ PhasedParams p) {
-  extern __shared__ __align__(128) uint8_t smem[];
+// Per-CTA state that does not depend on the scan: the twiddle chains and
+// bases, and the staging mbarrier's next phase (a persistent CTA runs spans
+// of several scans back to back on one mbarrier).
+struct PpCta {
+  Twiddles<kM> tw;
+  float2 wb1, dtw0, dtw1;
+  uint32_t phase;
+  bool stopped;
+};
+
+__device__ __forceinline__ void pp_cta_init(uint8_t* smem, PpCta& c) {
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(reinterpret_cast<uint64_t*>(smem + kPpBar), 1);
+    *reinterpret_cast<int*>(smem + kPpFlag) = 0;
+    fence_proxy_async();
+  }
+  c.tw.init(tid);
+  c.wb1 = rows::fold_base1(tid);  // W_M^(t+1)
+  // row 1's DIF twiddle bases W_N^t, W_N^(t + T), correctly rounded from FP64
+  double sn, cs;
+  sincospi(-2.0 * (double)tid / (double)kN2, &sn, &cs);
+  c.dtw0 = make_float2((float)cs, (float)sn);
+  sincospi(-2.0 * (double)(tid + kT) / (double)kN2, &sn, &cs);
+  c.dtw1 = make_float2((float)cs, (float)sn);
+  c.phase = 0;
+  c.stopped = false;
+}
+
+// Never leave a bulk copy in flight into a finished CTA's shared memory: after
+// a wait gave up, wait (bounded) once more for the phase that did not complete.
+__device__ __forceinline__ void pp_cta_drain(uint8_t* smem, const PpCta& c) {
+  if (c.stopped && threadIdx.x == 0)
+    mbar_wait(reinterpret_cast<uint64_t*>(smem + kPpBar), c.phase ^ 1u, kWaitPolls);
+}
+
+// Frame pairs [it0, it1) of the sector described by p, phased power summed
+// into the f64 partials at part ([H]) and .raw frames written when asked.
+// Opens with a CTA barrier (the previous span, if any, is past its last use
+// of the tables and the staging slot).  Returns false when a bounded wait
+// gave up (the CTA must stop).
+__device__ __forceinline__ bool pp_span(const PhasedParams& p, uint64_t it0, uint64_t it1,
+                                        double* part, uint8_t* smem, PpCta& c) {
   const int tid = threadIdx.x;
   FrameInfo* finfo = reinterpret_cast<FrameInfo*>(smem + kPpFi);
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kPpBar);
@@ -86,9 +128,6 @@ __global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constan
   const StationParams& s1 = p.st[0];
   const StationParams& s2 = p.st[1];
   const uint32_t bpf1 = s1.bpf, bpf2 = s2.bpf;
-  const uint64_t it0 = ((uint64_t)blockIdx.x * p.nf) / gridDim.x;
-  const uint64_t it1 = ((uint64_t)(blockIdx.x + 1) * p.nf) / gridDim.x;
-  double* part = p.partials + (size_t)blockIdx.x * kH2;
 
   auto issue = [&](uint64_t it) {
     mbar_expect_tx(bar, kFiBytes + bpf1 + bpf2);
@@ -96,28 +135,17 @@ __global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constan
     bulk_g2s(stage + 128, s1.raw + it * bpf1, bpf1, bar);
     bulk_g2s(stage + 128 + bpf1, s2.raw + it * bpf2, bpf2, bar);
   };
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    *flag = 0;
+  __syncthreads();
+  if (tid == 0 && it0 < it1) {
     fence_proxy_async();
-    if (it0 < it1) issue(it0);
+    issue(it0);
   }
   build_decode_tables(s1, s2, false, false, smem, tid, kT);
   for (int i = tid; i < 16; i += kT) ql[i] = i < (int)p.nqlevels ? p.qlevels[i] : 0.f;
   for (int i = tid; i < 1024; i += kT) elut[i] = p.enc_lut[i];
   const bool split1 = split_2bit(s1), split2 = split_2bit(s2);
-  Twiddles<kM> tw;
-  tw.init(tid);
-  const float2 wb1 = rows::fold_base1(tid);  // W_M^(t+1)
-  // row 1's DIF twiddle bases W_N^t, W_N^(t + T), correctly rounded from FP64
-  float2 dtw0, dtw1;
-  {
-    double sn, cs;
-    sincospi(-2.0 * (double)tid / (double)kN2, &sn, &cs);
-    dtw0 = make_float2((float)cs, (float)sn);
-    sincospi(-2.0 * (double)(tid + kT) / (double)kN2, &sn, &cs);
-    dtw1 = make_float2((float)cs, (float)sn);
-  }
+  const Twiddles<kM>& tw = c.tw;
+  const float2 wb1 = c.wb1, dtw0 = c.dtw0, dtw1 = c.dtw1;
   __syncthreads();
 
   const int a1s = p.a1s, a1e = p.a1e, a2s = p.a2s;
@@ -154,8 +182,8 @@ __global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constan
     since_flush = 0;
   };
 
-  uint32_t phase = 0;
-  bool stopped = false;
+  uint32_t phase = c.phase;
+  bool ok = true;
   for (uint64_t it = it0; it < it1; ++it) {
     if (!mbar_wait(bar, phase, kWaitPolls)) {
       atomicOr(flag, 1);
@@ -164,7 +192,7 @@ __global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constan
     phase ^= 1u;
     __syncthreads();  // every thread past its wait, the flag visible
     if (*flag) {
-      stopped = true;
+      ok = false;
       break;
     }
     const uint32_t* w1 = reinterpret_cast<const uint32_t*>(stage + 128);
@@ -311,8 +339,43 @@ __global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constan
     __syncthreads();  // the buffers are free for the next frame
   }
   if (since_flush > 0 || first_flush) flush();
-  // never leave a bulk copy in flight into a finished CTA's shared memory
-  if (stopped && tid == 0) mbar_wait(bar, phase ^ 1u, kWaitPolls);
+  c.phase = phase;
+  c.stopped = !ok;
+  return ok;
+}
+
+__global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constant__ PhasedParams p) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  PpCta c;
+  pp_cta_init(smem, c);
+  const uint64_t it0 = ((uint64_t)blockIdx.x * p.nf) / gridDim.x;
+  const uint64_t it1 = ((uint64_t)(blockIdx.x + 1) * p.nf) / gridDim.x;
+  pp_span(p, it0, it1, p.partials + (size_t)blockIdx.x * kH2, smem, c);
+  pp_cta_drain(smem, c);
+}
+
+// Batched: a persistent grid takes the items of batch group `grp` by ticket;
+// an item is a frame range of one scan's phased FFT-16384 sector (its own
+// tables, frame records, raw words and .raw output) with its own H partials.
+// Shared memory is sized for 2-bit stations, so one launch serves 1- and
+// 2-bit sectors, and every frame is computed exactly as by phased_pair_kernel.
+__global__ void __launch_bounds__(kT, 1) phased_pair_batch_kernel(const BatchArgs a, int grp) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(smem + kPpTicket);
+  PpCta c;
+  pp_cta_init(smem, c);
+  const uint32_t n_items = a.hdr->nitems[grp];
+  const BatchItem* items = a.hdr->items + a.hdr->item0[grp];
+  const BatchScan* scans = a.hdr->scans;
+  for (;;) {
+    if (threadIdx.x == 0) *ticket = atomicAdd(&a.hdr->ticket[grp], 1u);
+    __syncthreads();
+    const uint32_t k = *ticket;  // pp_span opens with a barrier before the next write
+    if (k >= n_items) break;
+    const BatchItem w = items[k];
+    if (!pp_span(scans[w.scan].pp, w.f0, w.f1, a.partials + w.part, smem, c)) break;
+  }
+  pp_cta_drain(smem, c);
 }
 
 }  // namespace
@@ -330,6 +393,24 @@ cudaError_t launch_phased_pair(const PhasedParams& p, int grid, cudaStream_t s) 
                                        (int)kPpMaxSmem);
   if (e != cudaSuccess) return e;
   phased_pair_kernel<<<grid, kT, pp_smem_bytes(p.st[0].bpf, p.st[1].bpf), s>>>(p);
+  return cudaGetLastError();
+}
+
+// The batch group's kernel, its layout sized for 2-bit stations.
+cudaError_t phased_pair_batch_prepare() {
+  return cudaFuncSetAttribute(phased_pair_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)pp_smem_bytes(kN2 / 4, kN2 / 4));
+}
+
+int phased_pair_batch_ctas_per_sm() {
+  int nb = 0;
+  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &nb, phased_pair_batch_kernel, kT, pp_smem_bytes(kN2 / 4, kN2 / 4));
+  return e == cudaSuccess ? nb : 0;
+}
+
+cudaError_t launch_phased_pair_batch(const BatchArgs& a, int grp, int grid, cudaStream_t s) {
+  phased_pair_batch_kernel<<<grid, kT, pp_smem_bytes(kN2 / 4, kN2 / 4), s>>>(a, grp);
   return cudaGetLastError();
 }
 

@@ -248,8 +248,10 @@ PH_MIX = [
     (dict(fft=8192, bits1=2, bits2=8, shuffle="generic", band=(64, 0, 4032, 64),
           products=PHASED), 95),
     (dict(fft=8192, bits1=2, bits2=2, band=(0, 0, 4096, 0), products=oracle.PROD_PHASED), 40),
-    # per-scan path inside the same call: phased above FFT 8192, with .raw
+    # FFT 16384 with 2-bit stations: the two-row kernel's batch group
     (dict(fft=16384, bits1=2, bits2=2, band=(128, 0, 8064, 128), products=PHASED), 9),
+    # per-scan path inside the same call: 4-bit stations above FFT 8192
+    (dict(fft=16384, bits1=4, bits2=2, band=(0, 0, 8192, 0), products=PHASED), 5),
     # a correlation sector beside them
     (dict(fft=4096, bits1=2, bits2=2, shuffle="generic", band=(40, 0, 2008, 40)), 200),
 ]
@@ -316,5 +318,39 @@ def test_batch_phased_sectors(fxc_lib, engine):
             for key in g0:
                 assert np.array_equal(g0[key], g1[key]), key
     bg.close()
+    b.close()
+    close(items)
+
+
+PH16_MIX = [
+    (dict(fft=16384, bits1=2, bits2=2, shuffle="generic", lsb1=True, band=(-64, 64, 8128, 0),
+          products=PHASED), 3200),
+    (dict(fft=16384, bits1=1, bits2=2, shuffle="pairswap", band=(96, 0, 8096, 96), grid=1,
+          products=PHASED, w1=0.6, w2=1.4), 2900),
+]
+
+
+def test_batch_phased_16384_spans(fxc_lib, engine):
+    """FFT-16384 phased sectors in the two-row kernel's persistent batch group,
+    cut into 32-frame items: two sectors give more items than resident CTAs,
+    so CTAs run spans of both scans back to back on one staging barrier.
+    .raw frames equal the per-scan kernel's byte for byte, the phased power
+    is within the FP32 tolerance of it, and the call is three launches (frame
+    records, the group's kernel, the reduction)."""
+    import torch
+
+    items = build(engine, PH16_MIX, seed0=500)
+    b = fxc_lib.Batch(engine, item_frames=32)
+    n0 = b.launches()
+    got = run_raw(b, items)
+    assert b.launches() - n0 == 3
+    # one 512-thread CTA per SM (the two rows fill shared memory): more items than CTAs
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert sum(-(-it["nf"] // 32) for it in items) > sms
+    for it, g in zip(items, got):
+        one = it["s"].sector_device(it["d1"], it["d2"], it["nf"], first_frame=it["first"])
+        assert np.array_equal(g["raw"], one["raw"])
+        assert_spectra_close(g["phased"], one["phased"], "batched phased 16384")
+        assert all(np.all(g[k] == 0) for k in ("acf11", "acf22", "xcf"))
     b.close()
     close(items)
