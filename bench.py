@@ -562,9 +562,9 @@ def batch_mixed_leg(fxc, torch, eng, n_scans=64, calls=10, warm=3, seed=9494):
     for s in scans:
         s.check()
     samples = sum(2.0 * fft * nf for fft, _, _, nf, _ in specs)
-    # sectors a batch cannot hold run through their scans' own kernels inside
-    # the call: phased FFT 16384 with 4-bit stations (the four-step path)
-    per_scan = sum(1 for fft, bits, phased, _, _ in specs if phased and fft == 16384 and bits > 2)
+    # every sector of this mix has a batch group (none runs through its scan's
+    # own kernels inside the call)
+    per_scan = 0
     out = {"gsample_s": samples / (ms * 1e-3) / 1e9, "ms_per_call": ms, "scans": n_scans,
            "frame_pairs_per_call": int(sum(nfs)), "input_bytes_per_call": 2 * tot,
            "kernels_per_call": (b.launches() - l0) / calls,
@@ -748,8 +748,9 @@ def fft_sweep(args):
     products by FFT length: the full-rate scan's schedule (1024 Msps, 2-bit,
     generic shuffle, LSB/USB, 16 MHz band offset) at each length, one sector
     of --sweep-samples samples per station per call, CUDA events on the
-    calling stream over --steps calls after --warmup.  One JSON line; not the
-    benchmark line."""
+    calling stream over --steps calls after --warmup.  --sweep-bits other than
+    2: both stations at that bit depth (odd-integer levels) with random .raw
+    bytes.  One JSON line; not the benchmark line."""
     import torch
 
     import fxc
@@ -757,19 +758,28 @@ def fft_sweep(args):
     torch.cuda.set_device(0)
     eng = fxc.Engine(0)
     stream = torch.cuda.Stream()
-    out = {"mode": "fft-sweep", "unit": "Gsample/s (device-resident, 2-bit)",
+    bits = args.sweep_bits
+    out = {"mode": "fft-sweep", "unit": f"Gsample/s (device-resident, {bits}-bit)",
            "samples_per_station_per_call": args.sweep_samples, "calls": args.steps}
     for fft in [int(v) for v in args.sweep_ffts.split(",")]:
         for prod in args.sweep_products.split(","):
             fields = scan_fields(fxc.band_alignment, fft=fft)
+            if bits != BITS:
+                lv = [float(v) for v in range(1 - (1 << bits), 1 << bits, 2)]
+                fields.update(bits1=bits, bits2=bits, levels1=lv, levels2=lv)
             if prod == "phased":
                 fields["products"] = fxc.PROD_PHASED | fxc.PROD_RAW
             cfg = fxc.ScanConfig(**fields)
             scan = eng.open_scan(cfg)
             nf = args.sweep_samples // fft
-            d1, d2 = gen_station_pair_gpu(torch, nf * fft, seed=fft, cfg=cfg)
+            if bits == BITS:
+                d1, d2 = gen_station_pair_gpu(torch, nf * fft, seed=fft, cfg=cfg)
+            else:
+                g = torch.Generator(device="cuda").manual_seed(fft)
+                d1, d2 = (torch.randint(0, 256, (nf * cfg.bpf(bits),), dtype=torch.uint8,
+                                        device="cuda", generator=g) for _ in range(2))
             acc = torch.empty(5 * cfg.h, dtype=torch.float64, device="cuda")
-            raw = (torch.empty(nf * cfg.bpf(BITS), dtype=torch.uint8, device="cuda")
+            raw = (torch.empty(nf * cfg.bpf(cfg.bits_out), dtype=torch.uint8, device="cuda")
                    if prod == "phased" else None)
 
             def call():
@@ -813,6 +823,8 @@ def main():
                          "benchmark line")
     ap.add_argument("--sweep-ffts", default="1024,2048,4096,8192,16384,32768,65536")
     ap.add_argument("--sweep-products", default="corr,phased")
+    ap.add_argument("--sweep-bits", type=int, default=2, choices=(1, 2, 4, 8),
+                    help="--fft-sweep: both stations' bit depth")
     ap.add_argument("--sweep-samples", type=int, default=1 << 29,
                     help="samples per station per call in --fft-sweep")
     args = ap.parse_args()

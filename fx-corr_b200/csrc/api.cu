@@ -448,9 +448,9 @@ fxc_status run_sector_device(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, 
       if (fst != FXC_OK) return fst;
       corr_done = true;
     }
-    // phased products with 1- and 2-bit stations: the two-row kernel (FFT
-    // 16384) or the cluster pair kernel (32768 / 65536, band shift a multiple
-    // of C); else the four-step path
+    // phased products: the two-row kernel (FFT 16384, any bit depth) or, with
+    // 1- and 2-bit stations, the cluster pair kernel (32768 / 65536, band
+    // shift a multiple of C); else the four-step path
     if (phased) {
       const PhasedParams pp = phased_params(s, r1, r2, nf, first, d_raw_out);
       if (phased_pair_supported(s->n, pp)) {
@@ -1320,7 +1320,7 @@ fxc_status batch_describe(fxc_scan* s, const uint8_t* r1, const uint8_t* r2, uin
   if (nf == 0 || (corr && phased)) return FXC_OK;  // the per-scan path
   if (phased) {
     // phased sectors of FFT 1024..8192 run in the phased batch kernels, FFT
-    // 16384 with 1- and 2-bit stations in the two-row kernel's batch group
+    // 16384 in the two-row kernel's batch group
     if (s->n > 16384) return FXC_OK;
     const PhasedParams pp = phased_params(s, r1, r2, nf, first, d_raw_out);
     if (s->n == 16384 && !phased_pair_supported(s->n, pp)) return FXC_OK;

@@ -197,13 +197,14 @@ cudaError_t launch_phased_batch(uint32_t n, const BatchArgs& a, int grp, int gri
 cudaError_t launch_batch_reduce(const BatchArgs& a, int grid, cudaStream_t s);
 
 cudaError_t launch_phased(uint32_t n, const PhasedParams& p, int grid, cudaStream_t s);
-// FFT 16384 phased products with 1- and 2-bit stations: one CTA per frame
-// pair, both rows in shared memory (phased_pair.cu); partials [grid][H].
+// FFT 16384 phased products (1- to 8-bit stations): one CTA per frame pair,
+// both rows in shared memory (phased_pair.cu); partials [grid][H].
 bool phased_pair_supported(uint32_t n, const PhasedParams& p);
 int phased_pair_grid(int sms, uint64_t nf);
 cudaError_t launch_phased_pair(const PhasedParams& p, int grid, cudaStream_t s);
 // Its persistent batch form (group BG_PHASED_16384, sectors that
-// phased_pair_supported accepts): shared-memory limit, occupancy, launch.
+// phased_pair_supported accepts, any mix of bit depths): shared-memory
+// limit, occupancy, launch.
 cudaError_t phased_pair_batch_prepare();
 int phased_pair_batch_ctas_per_sm();
 cudaError_t launch_phased_pair_batch(const BatchArgs& a, int grp, int grid, cudaStream_t s);

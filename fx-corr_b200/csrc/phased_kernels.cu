@@ -386,7 +386,7 @@ uint32_t phased_batch_smem() {
 
 // Batch groups of the phased kernels: FFT 1024 / 2048 / 4096 / 8192 with the
 // single-scan kernels' frames per CTA iteration (4 / 2 / 1 / 1); FFT 16384
-// (1- and 2-bit stations) is the two-row kernel's group (phased_pair.cu).
+// is the two-row kernel's group (phased_pair.cu).
 cudaError_t phased_batch_prepare(uint32_t n) {
   switch (n) {
     case 16384: return phased_pair_batch_prepare();

@@ -1,6 +1,6 @@
 // phased_pair.cu — phased-array synthesis for FFT 16384 (yi-phasedarray,
-// src/main.rs:2222-2412) with 1- and 2-bit stations: one CTA per frame pair,
-// both 8192-point rows of the frame in its shared memory.
+// src/main.rs:2222-2412), 1- to 8-bit stations: one CTA per frame pair, both
+// 8192-point rows of the frame in its shared memory.
 //
 // Per frame pair (the contract of phased_kernel, whose N <= 8192 frame loop
 // holds a frame in one FFT):
@@ -22,9 +22,11 @@
 //      x[m + M] gathered from cb), odd samples negated when both inputs are
 //      LSB, nearest-level re-quantisation with ant1's levels and packing with
 //      ant1's shuffle (src/utils.rs:378-410) of whole words from both rows.
-// Three padded row buffers; the staging slot and the output tables fill the
-// rest, which leaves room for 1- and 2-bit stations (the four-step path
-// serves the others).
+// Three padded row buffers.  With 1- and 2-bit stations a staging slot of its
+// own follows them and the next frame's words are copied while the frame is
+// computed; 4- and 8-bit stations (twice or four times the words) stage into
+// the third row buffer once the frame is done with it (during the
+// re-quantiser, or after the frame when no .raw is written).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -43,11 +45,15 @@ constexpr int kN2 = 2 * kM;    // frame length
 constexpr int kH2 = kN2 / 2 + 1;
 constexpr int kJ = kM / 2 / kT;  // bin pairs (rows 0 and 1) per thread
 
-// Shared memory (bytes): decode tables [0, 4608) (levels, rotate amounts;
-// 1- and 2-bit stations need no byte LUTs, so [4608, 12800) holds ant1's
-// output encode LUT); the gap [4352, 4608) holds the frame record, the
-// staging mbarrier, the error flag and the output levels; then the three row
-// buffers and one staging slot [FrameInfo (128 B)][station 1][station 2].
+// Shared memory (bytes): decode tables [0, 4608) (levels, rotate amounts); the
+// gap [4352, 4608) holds the frame record, the staging mbarrier, the error
+// flag and the batch ticket; then the three row buffers.  Narrow stations
+// (1- and 2-bit, output <= 2 bits): need no byte LUTs, so [4608, 12800) holds
+// ant1's output encode LUT, the output levels sit in the gap, and one staging
+// slot [FrameInfo (128 B)][station 1][station 2] follows the buffers.  Wide
+// stations: [4608, 12800) holds the byte LUTs of 4- and 8-bit generic
+// shuffles, the encode LUT and up to 256 output levels follow the buffers, and
+// the staging slot is a row buffer.
 constexpr uint32_t kPpFi = 4352, kPpBar = 4400, kPpFlag = 4408, kPpTicket = 4412;
 constexpr uint32_t kPpQl = 4416;  // 16 levels max
 constexpr uint32_t kPpEnc = kTabLut;  // [4][256] u32
@@ -62,6 +68,17 @@ __host__ __device__ constexpr uint32_t pp_smem_bytes(uint32_t bpf1, uint32_t bpf
   return kPpStage + ((128u + bpf1 + bpf2 + 127u) & ~127u);
 }
 static_assert(pp_smem_bytes(kN2 / 4, kN2 / 4) <= kPpMaxSmem, "2-bit stations fit");
+constexpr uint32_t kPpWideEnc = kPpStage, kPpWideQl = kPpStage + 4096;
+constexpr uint32_t kPpWideSmem = kPpWideQl + 256 * 4;
+static_assert(kPpWideSmem <= pp_smem_bytes(kN2 / 4, kN2 / 4), "one batch layout serves both");
+static_assert(128u + 2u * kN2 <= kPpBuf, "8-bit stations' words fit a row buffer");
+
+// Narrow stations take the separate staging slot (and the encode LUT and
+// output levels at their narrow places); any wider station or output selects
+// the wide layout.
+__host__ __device__ inline bool pp_wide(uint32_t bits1, uint32_t bits2, uint32_t bits_out) {
+  return bits1 > 2 || bits2 > 2 || bits_out > 2;
+}
 
 using rows::first_pass_regs;
 using rows::row1_twiddle;
@@ -109,39 +126,51 @@ __device__ __forceinline__ void pp_cta_drain(uint8_t* smem, const PpCta& c) {
 // Frame pairs [it0, it1) of the sector described by p, phased power summed
 // into the f64 partials at part ([H]) and .raw frames written when asked.
 // Opens with a CTA barrier (the previous span, if any, is past its last use
-// of the tables and the staging slot).  Returns false when a bounded wait
-// gave up (the CTA must stop).
+// of the tables, the buffers and the staging slot).  Returns false when a
+// bounded wait gave up (the CTA must stop).
+//
+// Buffers P, Q, S: row 0 forward into P, row 1 into Q, the secondary
+// station's spectrum by bin into S, cb into P; the inverse row 0 into Q, row
+// 1 into S (into P, in place of cb, when WIDE), the scratch of each FFT a free
+// buffer.  WIDE: the frame's words arrive in S, the next frame's go there once
+// the inverse is done with it.
+template <bool WIDE>
 __device__ __forceinline__ bool pp_span(const PhasedParams& p, uint64_t it0, uint64_t it1,
                                         double* part, uint8_t* smem, PpCta& c) {
   const int tid = threadIdx.x;
   FrameInfo* finfo = reinterpret_cast<FrameInfo*>(smem + kPpFi);
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kPpBar);
   int* flag = reinterpret_cast<int*>(smem + kPpFlag);
-  float* ql = reinterpret_cast<float*>(smem + kPpQl);
-  uint32_t* elut = reinterpret_cast<uint32_t*>(smem + kPpEnc);
+  float* ql = reinterpret_cast<float*>(smem + (WIDE ? kPpWideQl : kPpQl));
+  uint32_t* elut = reinterpret_cast<uint32_t*>(smem + (WIDE ? kPpWideEnc : kPpEnc));
+  const uint32_t* lut = reinterpret_cast<const uint32_t*>(smem + kTabLut);
   const uint32_t* pos = reinterpret_cast<const uint32_t*>(smem + kTabPos);
-  float2* B0 = reinterpret_cast<float2*>(smem + kPpB0);
-  float2* B1 = reinterpret_cast<float2*>(smem + kPpB1);
-  float2* B2 = reinterpret_cast<float2*>(smem + kPpB2);
-  uint8_t* stage = smem + kPpStage;
+  float2* P = reinterpret_cast<float2*>(smem + kPpB0);
+  float2* Q = reinterpret_cast<float2*>(smem + kPpB1);
+  float2* S = reinterpret_cast<float2*>(smem + kPpB2);
 
   const StationParams& s1 = p.st[0];
   const StationParams& s2 = p.st[1];
   const uint32_t bpf1 = s1.bpf, bpf2 = s2.bpf;
+  // 4- and 8-bit stations with a non-identity shuffle: words rewritten in place
+  const bool pre1 = WIDE && s1.bits > 2 && s1.shkind != SH_IDENTITY;
+  const bool pre2 = WIDE && s2.bits > 2 && s2.shkind != SH_IDENTITY;
 
-  auto issue = [&](uint64_t it) {
+  auto issue = [&](uint64_t it, uint8_t* stage) {
     mbar_expect_tx(bar, kFiBytes + bpf1 + bpf2);
     bulk_g2s(stage, p.finfo + it, kFiBytes, bar);
     bulk_g2s(stage + 128, s1.raw + it * bpf1, bpf1, bar);
     bulk_g2s(stage + 128 + bpf1, s2.raw + it * bpf2, bpf2, bar);
   };
+  uint8_t* stage = WIDE ? reinterpret_cast<uint8_t*>(S) : smem + kPpStage;
   __syncthreads();
   if (tid == 0 && it0 < it1) {
     fence_proxy_async();
-    issue(it0);
+    issue(it0, stage);
   }
-  build_decode_tables(s1, s2, false, false, smem, tid, kT);
-  for (int i = tid; i < 16; i += kT) ql[i] = i < (int)p.nqlevels ? p.qlevels[i] : 0.f;
+  build_decode_tables(s1, s2, pre1, pre2, smem, tid, kT);
+  const int nql = WIDE ? 256 : 16;
+  for (int i = tid; i < nql; i += kT) ql[i] = i < (int)p.nqlevels ? p.qlevels[i] : 0.f;
   for (int i = tid; i < 1024; i += kT) elut[i] = p.enc_lut[i];
   const bool split1 = split_2bit(s1), split2 = split_2bit(s2);
   const Twiddles<kM>& tw = c.tw;
@@ -195,11 +224,16 @@ __device__ __forceinline__ bool pp_span(const PhasedParams& p, uint64_t it0, uin
       ok = false;
       break;
     }
-    const uint32_t* w1 = reinterpret_cast<const uint32_t*>(stage + 128);
-    const uint32_t* w2 = reinterpret_cast<const uint32_t*>(stage + 128 + bpf1);
+    uint32_t* w1 = reinterpret_cast<uint32_t*>(stage + 128);
+    uint32_t* w2 = reinterpret_cast<uint32_t*>(stage + 128 + bpf1);
     const FrameInfo* fs = reinterpret_cast<const FrameInfo*>(stage);
     const int sh1 = fs->s1, sh2 = fs->s2;
-    if (tid == 0) *finfo = *fs;  // before the refill overwrites the slot
+    if (tid == 0) *finfo = *fs;  // before the slot is refilled or reused
+    if (pre1 || pre2) {
+      preshuffle_slot(w1, bpf1 / 4, pre1 ? s1.shkind : SH_IDENTITY, lut, w2, bpf2 / 4,
+                      pre2 ? s2.shkind : SH_IDENTITY, lut + 1024, tid, kT);
+      __syncthreads();
+    }
     const float sg = (it & 1u) ? -1.0f : 1.0f;  // station 2 enters odd frames negated
 
     // ---- 1. forward: rows 0 and 1 of the radix-2 DIF, decoded into their first pass
@@ -215,19 +249,21 @@ __device__ __forceinline__ bool pp_span(const PhasedParams& p, uint64_t it0, uin
         fold::fold_station<true, 2>(s2.bits, split2, w2, smem, sh2, pos[32 + c2], tb2, v, tid,
                                     q == 1);
         if (q == 1) row1_twiddle(v, dtw0, dtw1);
-        first_pass_regs(v, q == 0 ? B0 : B1, tid);
-        if (q == 0) fft_rest<kM, true>(B0, B2, tid, tw);  // row 0's last pass output in B0
+        // WIDE: row 0's FFT took Q as its scratch (S holds the words)
+        if (WIDE && q == 1) __syncthreads();
+        first_pass_regs(v, q == 0 ? P : Q, tid);
+        if (q == 0) fft_rest<kM, true>(P, WIDE ? Q : S, tid, tw);  // row 0's spectrum in P
       }
     }
-    fft_rest<kM, true>(B1, B2, tid, tw);  // row 1's spectrum in B1
+    fft_rest<kM, true>(Q, S, tid, tw);  // row 1's spectrum in Q
     // the staged words are consumed (fft_rest opened with a barrier): refill
-    if (tid == 0 && it + 1 < it1) {
+    if (!WIDE && tid == 0 && it + 1 < it1) {
       fence_proxy_async();
-      issue(it + 1);
+      issue(it + 1, stage);
     }
     __syncthreads();
 
-    // ---- 2. per bin: both stations rotated; the secondary one into B2 by bin
+    // ---- 2. per bin: both stations rotated; the secondary one into S by bin
     const FrameInfo& F = *finfo;
     auto station = [&](float2 u, float2 w, int k, int s) -> float2 {
       // spectrum of station s at its own bin k: unscaled, rotated by the
@@ -252,24 +288,24 @@ __device__ __forceinline__ bool pp_span(const PhasedParams& p, uint64_t it0, uin
         // the rows' trailing radix-2 pass folded in: Z_q[j] and Z[N - k],
         // which is row 1's index M - 1 - j or row 0's index M - j
         const int k = 2 * j + q;
-        const float2* Y = q ? B1 : B0;
+        const float2* Y = q ? Q : P;
         const float2 u = fold_lower(Y, j, wj);
         const float2 w = fold_mirror(Y, j, q == 0, wj, wj1);
         prim[2 * i2 + q] = station(u, w, k, sp);
-        B2[k] = station(u, w, k, 1 - sp);
+        S[k] = station(u, w, k, 1 - sp);
       }
     }
     prim[2 * kJ] = make_float2(0.f, 0.f);
     if (half) {  // Z[N/2] = row 0's index M/2 (Y[0] - Y[M/2]) pairs with itself
-      const float2 u = csub(B0[0], B0[kM / 2]);
+      const float2 u = csub(P[0], P[kM / 2]);
       prim[2 * kJ] = station(u, u, kN2 / 2, sp);
-      B2[kN2 / 2] = station(u, u, kN2 / 2, 1 - sp);
+      S[kN2 / 2] = station(u, u, kN2 / 2, 1 - sp);
     }
     __syncthreads();
-    // ---- band alignment and the weighted sum; cb by bin into B0
+    // ---- band alignment and the weighted sum; cb by bin into P
     auto combine = [&](int b, float2 pv) -> float2 {
       float2 sv = make_float2(0.f, 0.f);
-      if ((unsigned)(b - ovs) < (unsigned)ov) sv = B2[b + qoff];
+      if ((unsigned)(b - ovs) < (unsigned)ov) sv = S[b + qoff];
       // cb = w1 a1 + w2 a2 with a1 / a2 the station-1 / station-2 terms
       const float2 a1 = g0 ? pv : sv, a2 = g0 ? sv : pv;
       return make_float2(a1.x * p.w1 + a2.x * p.w2, a1.y * p.w1 + a2.y * p.w2);
@@ -280,13 +316,13 @@ __device__ __forceinline__ bool pp_span(const PhasedParams& p, uint64_t it0, uin
       float2 cb = combine(b, prim[i]);
       acc[i] += cnorm2(cb);
       if (b == 0) cb.y = 0.f;
-      B0[b] = cb;
+      P[b] = cb;
     }
     if (half) {
       float2 cb = combine(kN2 / 2, prim[2 * kJ]);
       acc[2 * kJ] += cnorm2(cb);
       cb.y = 0.f;
-      B0[kN2 / 2] = cb;
+      P[kN2 / 2] = cb;
     }
     if (++since_flush >= p.flush_every) flush();
 
@@ -299,20 +335,31 @@ __device__ __forceinline__ bool pp_span(const PhasedParams& p, uint64_t it0, uin
 #pragma unroll
         for (int r = 0; r < 16; ++r) {
           const int m = tid + kT * r;
-          const float2 lo = B0[m], hi = B0[kM - m];
+          const float2 lo = P[m], hi = P[kM - m];
           v[r] = q == 0 ? make_float2(lo.x + hi.x, hi.y - lo.y) : make_float2(lo.x - hi.x, -lo.y - hi.y);
         }
         if (q == 1) row1_twiddle(v, dtw0, dtw1);
         if (q == 0) {
-          first_pass_regs(v, B1, tid);
-          fft_rest<kM, true>(B1, B2, tid, tw);  // X[2 k] (pre radix-2) in B1
+          first_pass_regs(v, Q, tid);
+          fft_rest<kM, true>(Q, S, tid, tw);  // X[2 k] (pre radix-2) in Q
           __syncthreads();
-          row_radix2(B1, tid, tw);
+          row_radix2(Q, tid, tw);
+        } else if (!WIDE) {
+          first_pass_regs(v, S, tid);
+          fft_rest<kM, true>(S, P, tid, tw);  // X[2 k + 1] in S (cb consumed)
+          __syncthreads();
+          row_radix2(S, tid, tw);
         } else {
-          first_pass_regs(v, B2, tid);
-          fft_rest<kM, true>(B2, B0, tid, tw);  // X[2 k + 1] in B2 (cb consumed)
+          __syncthreads();  // every thread has read its cb values
+          first_pass_regs(v, P, tid);
+          fft_rest<kM, true>(P, S, tid, tw);  // X[2 k + 1] in P
           __syncthreads();
-          row_radix2(B2, tid, tw);
+          // S is free until the next frame's decode: its words go there
+          if (tid == 0 && it + 1 < it1) {
+            fence_proxy_async();
+            issue(it + 1, stage);
+          }
+          row_radix2(P, tid, tw);
         }
       }
       __syncthreads();
@@ -327,7 +374,7 @@ __device__ __forceinline__ bool pp_span(const PhasedParams& p, uint64_t it0, uin
         for (uint32_t i = 0; i < spw; ++i) {
           const uint32_t ii = (i + rot) & (spw - 1u);
           const uint32_t n = wdx * spw + ii;
-          float x = ((n & 1u) ? B2 : B1)[n >> 1].x * inv_n;
+          float x = ((n & 1u) ? (WIDE ? P : S) : Q)[n >> 1].x * inv_n;
           if (p.out_lsb && (n & 1u)) x = -x;
           word |= (nearest_level(x, ql, (int)p.nqlevels, p.qmonotonic) & qmask) << (ii * p.bits_out);
         }
@@ -337,6 +384,10 @@ __device__ __forceinline__ bool pp_span(const PhasedParams& p, uint64_t it0, uin
       }
     }
     __syncthreads();  // the buffers are free for the next frame
+    if (WIDE && !p.want_raw && tid == 0 && it + 1 < it1) {
+      fence_proxy_async();
+      issue(it + 1, stage);
+    }
   }
   if (since_flush > 0 || first_flush) flush();
   c.phase = phase;
@@ -344,21 +395,22 @@ __device__ __forceinline__ bool pp_span(const PhasedParams& p, uint64_t it0, uin
   return ok;
 }
 
+template <bool WIDE>
 __global__ void __launch_bounds__(kT, 1) phased_pair_kernel(const __grid_constant__ PhasedParams p) {
   extern __shared__ __align__(128) uint8_t smem[];
   PpCta c;
   pp_cta_init(smem, c);
   const uint64_t it0 = ((uint64_t)blockIdx.x * p.nf) / gridDim.x;
   const uint64_t it1 = ((uint64_t)(blockIdx.x + 1) * p.nf) / gridDim.x;
-  pp_span(p, it0, it1, p.partials + (size_t)blockIdx.x * kH2, smem, c);
+  pp_span<WIDE>(p, it0, it1, p.partials + (size_t)blockIdx.x * kH2, smem, c);
   pp_cta_drain(smem, c);
 }
 
 // Batched: a persistent grid takes the items of batch group `grp` by ticket;
 // an item is a frame range of one scan's phased FFT-16384 sector (its own
 // tables, frame records, raw words and .raw output) with its own H partials.
-// Shared memory is sized for 2-bit stations, so one launch serves 1- and
-// 2-bit sectors, and every frame is computed exactly as by phased_pair_kernel.
+// Shared memory is sized for the larger (narrow) layout, so one launch serves
+// every bit depth, and every frame is computed exactly as by phased_pair_kernel.
 __global__ void __launch_bounds__(kT, 1) phased_pair_batch_kernel(const BatchArgs a, int grp) {
   extern __shared__ __align__(128) uint8_t smem[];
   uint32_t* ticket = reinterpret_cast<uint32_t*>(smem + kPpTicket);
@@ -373,7 +425,11 @@ __global__ void __launch_bounds__(kT, 1) phased_pair_batch_kernel(const BatchArg
     const uint32_t k = *ticket;  // pp_span opens with a barrier before the next write
     if (k >= n_items) break;
     const BatchItem w = items[k];
-    if (!pp_span(scans[w.scan].pp, w.f0, w.f1, a.partials + w.part, smem, c)) break;
+    const PhasedParams& pp = scans[w.scan].pp;
+    const bool ok = pp_wide(pp.st[0].bits, pp.st[1].bits, pp.bits_out)
+                        ? pp_span<true>(pp, w.f0, w.f1, a.partials + w.part, smem, c)
+                        : pp_span<false>(pp, w.f0, w.f1, a.partials + w.part, smem, c);
+    if (!ok) break;
   }
   pp_cta_drain(smem, c);
 }
@@ -381,7 +437,7 @@ __global__ void __launch_bounds__(kT, 1) phased_pair_batch_kernel(const BatchArg
 }  // namespace
 
 bool phased_pair_supported(uint32_t n, const PhasedParams& p) {
-  return n == (uint32_t)kN2 && p.st[0].bits <= 2 && p.st[1].bits <= 2 && p.bits_out <= 2;
+  return n == (uint32_t)kN2 && p.nqlevels <= 256;
 }
 
 int phased_pair_grid(int sms, uint64_t nf) {
@@ -389,14 +445,17 @@ int phased_pair_grid(int sms, uint64_t nf) {
 }
 
 cudaError_t launch_phased_pair(const PhasedParams& p, int grid, cudaStream_t s) {
-  cudaError_t e = cudaFuncSetAttribute(phased_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const bool wide = pp_wide(p.st[0].bits, p.st[1].bits, p.bits_out);
+  auto* kern = wide ? phased_pair_kernel<true> : phased_pair_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kPpMaxSmem);
   if (e != cudaSuccess) return e;
-  phased_pair_kernel<<<grid, kT, pp_smem_bytes(p.st[0].bpf, p.st[1].bpf), s>>>(p);
+  kern<<<grid, kT, wide ? kPpWideSmem : pp_smem_bytes(p.st[0].bpf, p.st[1].bpf), s>>>(p);
   return cudaGetLastError();
 }
 
-// The batch group's kernel, its layout sized for 2-bit stations.
+// The batch group's kernel, its shared memory sized for the narrow layout with
+// 2-bit stations (the larger of the two layouts).
 cudaError_t phased_pair_batch_prepare() {
   return cudaFuncSetAttribute(phased_pair_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)pp_smem_bytes(kN2 / 4, kN2 / 4));

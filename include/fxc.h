@@ -290,12 +290,11 @@ FXC_API fxc_status fxc_server_destroy(fxc_server* sv);
  * autotuner that times the kernel variants on a synthetic batch (at first use
  * of the length when opts.autotune is set, or by fxc_batch_autotune).
  * Phased sectors (yi-phasedarray: phased power and .raw frames, FFT
- * 1024..8192, and FFT 16384 with 1- and 2-bit stations) run in persistent
- * phased kernels of the same batch.  Sectors the batch kernels do not cover
- * (phased products above FFT 16384 or at 16384 with 4- or 8-bit stations,
- * correlation above 16384, correlation at FFT 16384 with an odd band shift,
- * scans with both correlation and phased products, empty sectors) run
- * through the per-scan path on the same stream.  A sector's products equal fxc_sector_run_device's within the
+ * 1024..16384) run in persistent phased kernels of the same batch.  Sectors
+ * the batch kernels do not cover (phased products or correlation above FFT
+ * 16384, correlation at FFT 16384 with an odd band shift, scans with both
+ * correlation and phased products, empty sectors) run through the per-scan
+ * path on the same stream.  A sector's products equal fxc_sector_run_device's within the
  * library's FP32 tolerance (phased .raw frames byte for byte), and are
  * identical bit for bit whatever else shares the batch (the item split
  * depends only on the sector's frame count and the batch's tuning). */

@@ -250,8 +250,10 @@ PH_MIX = [
     (dict(fft=8192, bits1=2, bits2=2, band=(0, 0, 4096, 0), products=oracle.PROD_PHASED), 40),
     # FFT 16384 with 2-bit stations: the two-row kernel's batch group
     (dict(fft=16384, bits1=2, bits2=2, band=(128, 0, 8064, 128), products=PHASED), 9),
-    # per-scan path inside the same call: 4-bit stations above FFT 8192
+    # the same group's wide layout (a 4-bit station)
     (dict(fft=16384, bits1=4, bits2=2, band=(0, 0, 8192, 0), products=PHASED), 5),
+    # per-scan path inside the same call: phased above FFT 16384
+    (dict(fft=32768, bits1=2, bits2=2, band=(0, 0, 16384, 0), products=PHASED), 4),
     # a correlation sector beside them
     (dict(fft=4096, bits1=2, bits2=2, shuffle="generic", band=(40, 0, 2008, 40)), 200),
 ]
@@ -327,13 +329,17 @@ PH16_MIX = [
           products=PHASED), 3200),
     (dict(fft=16384, bits1=1, bits2=2, shuffle="pairswap", band=(96, 0, 8096, 96), grid=1,
           products=PHASED, w1=0.6, w2=1.4), 2900),
+    (dict(fft=16384, bits1=4, bits2=4, shuffle="generic", band=(0, 0, 8192, 0),
+          products=PHASED), 1500),
 ]
 
 
 def test_batch_phased_16384_spans(fxc_lib, engine):
     """FFT-16384 phased sectors in the two-row kernel's persistent batch group,
-    cut into 32-frame items: two sectors give more items than resident CTAs,
-    so CTAs run spans of both scans back to back on one staging barrier.
+    cut into 32-frame items: three sectors (1-, 2- and 4-bit stations, the
+    last in the wide layout) give more items than resident CTAs, so CTAs run
+    spans of several scans and both layouts back to back on one staging
+    barrier.
     .raw frames equal the per-scan kernel's byte for byte, the phased power
     is within the FP32 tolerance of it, and the call is three launches (frame
     records, the group's kernel, the reduction)."""

@@ -41,10 +41,13 @@ CASES = [
     dict(fft=4096, grid=0, band=(40, 0, 2008, 40), shuffle="pairswap", lsb1=True),
     dict(fft=8192, grid=0, band=(-128, 128, 4096, 0), shuffle="generic", lsb1=True, lsb2=True),
     dict(fft=4096, bits1=2, bits2=4, grid=1, band=(12, 0, 2036, 12)),
-    # FFT lengths above 8192: the two-row kernel (16384), the cluster pair
-    # kernel (32768 / 65536 with the band shift a multiple of N / 8192) and the
-    # four-step path (any other shift, 4- and 8-bit stations)
+    # FFT lengths above 8192: the two-row kernel (16384; 4- and 8-bit stations
+    # staged in a row buffer), the cluster pair kernel (32768 / 65536 with the
+    # band shift a multiple of N / 8192) and the four-step path (any other
+    # shift, 4- and 8-bit stations)
     dict(fft=16384, grid=0, band=(-64, 64, 8192, 0), shuffle="generic", lsb1=True, lsb2=True),
+    dict(fft=16384, bits1=4, bits2=2, grid=1, band=(32, 0, 8160, 32), shuffle="generic"),
+    dict(fft=16384, bits1=8, bits2=8, grid=0, band=(-16, 16, 8192, 0), lsb1=True, lsb2=True),
     dict(fft=32768, bits1=1, bits2=2, grid=1, band=(100, 0, 16284, 100), w1=0.8, w2=1.2),
     dict(fft=65536, grid=0, band=(-64, 64, 32768, 0), shuffle="generic", lsb1=True, lsb2=True),
     dict(fft=32768, grid=1, band=(6, 0, 16378, 6), shuffle="pairswap"),
