@@ -1,8 +1,9 @@
 """Writes tests/golden/kat.json: known-answer vectors for the fx-corr hot path.
 
 The reference ships no fixtures for this path and cannot be built here, so
-every expected value below was derived by hand from the cited reference lines
-and is written as a literal (nothing here calls an oracle or the product).
+every expected value below is a literal: derived by hand from the cited
+reference lines, or (the `readme` section) a worked example the reference's
+README states itself.  Nothing here calls an oracle or the product.
 Run:  python tests/golden/make_golden.py
 """
 import json
@@ -128,6 +129,24 @@ quantise = [  # utils.rs:378-410: nearest level, first index wins ties, LSB-firs
 
 level_power = [dict(levels=L2, expect=1.25), dict(levels=[-3.0, -1.0, 1.0, 3.0], expect=5.0)]
 
+# Known answers the reference documents itself (README.md), beside the
+# hand-derived vectors above:
+readme = dict(
+    # README.md:225-235: n = round(tau fs), eps = tau - n/fs; "12.983 samples is
+    # handled as n=13, eps=-0.017 sample", "12.345 samples ... n=12, eps=+0.345"
+    delay_split=[dict(samples=12.983, fs=1e6, n=13, eps_samples=-0.017),
+                 dict(samples=12.345, fs=1e6, n=12, eps_samples=0.345)],
+    # README.md:241-243: "For 2-bit sampling: n=12 samples means 24 bits (3 bytes)"
+    bit_offset=[dict(bits=2, samples=12, offset_bits=24, offset_bytes=3)],
+    # README.md:276-293: inv = 1/(0.5 P nf fft^2), P11 = mean(level1^2),
+    # P12 = sqrt(P11 P22); "typical 2-bit levels [-1.5, 0.5, -0.5, 1.5]:
+    # mean(level^2) = 1.25".  fft = 8, nf = 10: inv = 1/(0.5 1.25 10 64) = 1/400
+    normalize=[dict(levels=[-1.5, 0.5, -0.5, 1.5], p=1.25, fft=8, nf=10,
+                    acc=[400.0, 800.0, 1200.0, 1600.0, 2000.0], expect=[1.0, 2.0, 3.0, 4.0])],
+    # P12 of the typical 2-bit levels against +-1/+-3 (P22 = 5): sqrt(1.25 * 5) = 2.5
+    cross_power=[dict(levels1=[-1.5, 0.5, -0.5, 1.5], levels2=[-3.0, -1.0, 1.0, 3.0], p12=2.5)],
+)
+
 normalize = [  # main.rs:2645-2683: inv = 1/(0.5*P*nf*N^2), first N/2 bins
     dict(fft=4, nf=2, p=1.25, acc=[20.0, 40.0, 60.0], expect=[1.0, 2.0]),
 ]
@@ -139,6 +158,6 @@ rfft = [  # unnormalised DFT (utils.rs:47-59)
 
 out = dict(decode=decode, shift=shift, parse_shuffle=parse_shuffle, band=band, delay=delay,
            xcf_phase=xcf_phase, quantise=quantise, level_power=level_power,
-           normalize=normalize, rfft=rfft)
+           normalize=normalize, rfft=rfft, readme=readme)
 Path(__file__).with_name("kat.json").write_text(json.dumps(out, indent=1))
 print("wrote", Path(__file__).with_name("kat.json"))

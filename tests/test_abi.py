@@ -70,6 +70,11 @@ def test_level_power_and_normalize(fxc_lib):
     for c in KAT["normalize"]:
         out = fxc_lib.normalize(c["fft"], c["nf"], c["p"], acc_real=np.array(c["acc"]))
         np.testing.assert_allclose(out.real, c["expect"], rtol=1e-7)
+    # the reference's own worked example (README.md:276-293)
+    for c in KAT["readme"]["normalize"]:
+        assert fxc_lib.level_power(c["levels"]) == c["p"]
+        out = fxc_lib.normalize(c["fft"], c["nf"], c["p"], acc_real=np.array(c["acc"]))
+        np.testing.assert_allclose(out.real, c["expect"], rtol=1e-7)
 
 
 def test_normalize_matches_oracle(fxc_lib, oracle_lib):

@@ -144,6 +144,22 @@ def test_delay_model_bit_exact(engine, branch):
     s.close()
 
 
+@pytest.mark.gpu
+def test_delay_split_readme_examples(engine):
+    """The reference's worked examples of the delay split (README.md:225-235):
+    12.983 samples -> integer shift 13 and fraction -0.017 sample, 12.345 ->
+    12 and +0.345, through the product's FP64 frame records on the GPU."""
+    kat = json.loads((Path(__file__).parent / "golden" / "kat.json").read_text())
+    for c in kat["readme"]["delay_split"]:
+        fs = 1024e6
+        scan = make_scan(fft=1024, fs=fs, delay=dict(net_d1_base=c["samples"] / fs))
+        s = engine.open_scan(to_fxc(scan))
+        e = s.delay_entries(0, 4)
+        s.close()
+        assert int(e["int1"][0]) == c["n"]
+        assert abs(float(e["frac1"][0]) * fs - c["eps_samples"]) < 1e-9
+
+
 # ----------------------------------------------------------------- spectra
 
 @pytest.mark.parametrize("n", [1024, 2048, 4096, 8192])

@@ -110,6 +110,47 @@ def test_level_power_and_normalize_kat(oracle_lib):
         assert np.all(out.imag == 0)
 
 
+@pytest.mark.parametrize("case", KAT["readme"]["delay_split"], ids=lambda c: str(c["samples"]))
+def test_readme_delay_split(oracle_lib, case):
+    """The reference's own worked examples of the integer / fractional delay
+    split (README.md:225-235) through both oracles' delay model."""
+    fs = case["fs"]
+    s = _delay_scan(dict(cfg=dict(frame_dt=1024 / fs, fs=fs, net_d1_base=case["samples"] / fs)))
+    e = oracle.c_delay_entries(s, 0, 1)[0]
+    assert e["int1"] == case["n"]
+    assert math.isclose(e["frac1"] * fs, case["eps_samples"], rel_tol=1e-9)
+    i1, _, f1, _, _, _ = oracle.np_delay_entries(s, 0, 1)[0]
+    assert i1 == case["n"] and math.isclose(f1 * fs, case["eps_samples"], rel_tol=1e-9)
+
+
+@pytest.mark.parametrize("case", KAT["readme"]["bit_offset"])
+def test_readme_bit_offset(oracle_lib, case):
+    """README.md:241-243: at 2 bits an n-sample shift is an n*bits-bit offset;
+    decoding from that byte on equals dropping the first n decoded samples."""
+    bits, n = case["bits"], case["samples"]
+    assert n * bits == case["offset_bits"] and case["offset_bits"] // 8 == case["offset_bytes"]
+    raw = np.random.default_rng(12).integers(0, 256, 64, dtype=np.uint8)
+    lv = oracle.default_levels(bits)
+    total = len(raw) * 8 // bits
+    full = oracle.c_decode(raw, total, bits, list(range(32)), lv, False)
+    tail = oracle.c_decode(raw[case["offset_bytes"]:], total - n, bits, list(range(32)), lv, False)
+    np.testing.assert_array_equal(tail, full[n:])
+    # and as the integer delay: the n-sample shift brings sample m to position m + n
+    np.testing.assert_array_equal(oracle.c_shift(full, n)[n:], full[:-n])
+
+
+def test_readme_normalization(oracle_lib):
+    """README.md:276-293: inv = 1/(0.5 P nf fft^2) with P = mean(level^2),
+    P12 = sqrt(P11 P22); the typical 2-bit levels give P = 1.25."""
+    for c in KAT["readme"]["normalize"]:
+        assert oracle.level_power(c["levels"]) == c["p"]
+        out = oracle.c_normalize(c["fft"], c["nf"], c["p"], acc_real=np.array(c["acc"]))
+        np.testing.assert_allclose(out.real, c["expect"], rtol=1e-7)
+    for c in KAT["readme"]["cross_power"]:
+        p12 = math.sqrt(oracle.level_power(c["levels1"]) * oracle.level_power(c["levels2"]))
+        assert p12 == c["p12"]
+
+
 def test_rfft_kat(oracle_lib):
     n = 16
     x = np.cos(2 * np.pi * 3 * np.arange(n) / n).astype(np.float32)
