@@ -59,13 +59,14 @@ def shuffle_internal(seed: int):
 PROD_ACF, PROD_XCF = 1, 2  # product bits (same values in fxc and the oracle)
 
 
-def scan_fields(band_alignment, fft=N):
+def scan_fields(band_alignment, fft=N, rot2_hz=ROT2_HZ):
     """Resolve the scan the way run_once does (src/main.rs:1186-1212,
     1317-1328, 1618-1673) for the synthetic schedule above.  Returns the
     fields shared by fxc.ScanConfig and oracle.Scan; `band_alignment` is
     either's restatement of compute_band_alignment (src/main.rs:360-372).
     `fft` other than 8192: the same schedule at another FFT length (the
-    --fft-sweep mode)."""
+    --fft-sweep mode); `rot2_hz`: another band offset of station 2."""
+    ROT2_HZ = rot2_hz
     bw = FS / 2e6
     c1 = OBS_MHZ + ROT1_HZ / 1e6 + 0.5 * bw
     c2 = OBS_MHZ + ROT2_HZ / 1e6 + 0.5 * bw
@@ -750,7 +751,8 @@ def fft_sweep(args):
     of --sweep-samples samples per station per call, CUDA events on the
     calling stream over --steps calls after --warmup.  --sweep-bits other than
     2: both stations at that bit depth (odd-integer levels) with random .raw
-    bytes.  One JSON line; not the benchmark line."""
+    bytes.  --sweep-offset-mhz: station 2's band offset (16.0625 MHz gives an
+    odd band shift at FFT 16384).  One JSON line; not the benchmark line."""
     import torch
 
     import fxc
@@ -760,10 +762,11 @@ def fft_sweep(args):
     stream = torch.cuda.Stream()
     bits = args.sweep_bits
     out = {"mode": "fft-sweep", "unit": f"Gsample/s (device-resident, {bits}-bit)",
-           "samples_per_station_per_call": args.sweep_samples, "calls": args.steps}
+           "samples_per_station_per_call": args.sweep_samples, "calls": args.steps,
+           "band_offset_mhz": args.sweep_offset_mhz}
     for fft in [int(v) for v in args.sweep_ffts.split(",")]:
         for prod in args.sweep_products.split(","):
-            fields = scan_fields(fxc.band_alignment, fft=fft)
+            fields = scan_fields(fxc.band_alignment, fft=fft, rot2_hz=args.sweep_offset_mhz * 1e6)
             if bits != BITS:
                 lv = [float(v) for v in range(1 - (1 << bits), 1 << bits, 2)]
                 fields.update(bits1=bits, bits2=bits, levels1=lv, levels2=lv)
@@ -827,6 +830,8 @@ def main():
                     help="--fft-sweep: both stations' bit depth")
     ap.add_argument("--sweep-samples", type=int, default=1 << 29,
                     help="samples per station per call in --fft-sweep")
+    ap.add_argument("--sweep-offset-mhz", type=float, default=ROT2_HZ / 1e6,
+                    help="station 2's band offset in --fft-sweep")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.fft_sweep:

@@ -64,7 +64,8 @@ __host__ __device__ constexpr uint32_t pr_stage_bytes(int c, int bits_p, int bit
 __host__ __device__ constexpr uint32_t pr_smem_bytes(int c, int bits_p, int bits_s) {
   return kPrStage + pr_stage_bytes(c, bits_p, bits_s);
 }
-static_assert(pr_smem_bytes(8, 2, 2) <= kPrMaxSmem && pr_smem_bytes(4, 2, 2) <= kPrMaxSmem,
+static_assert(pr_smem_bytes(8, 2, 2) <= kPrMaxSmem && pr_smem_bytes(4, 2, 2) <= kPrMaxSmem &&
+                  pr_smem_bytes(2, 2, 2) <= kPrMaxSmem,
               "2-bit stations fit");
 
 // Owner CTA of row k (the CTA holding the mirror pair {k, C - k}) and whether
@@ -197,14 +198,33 @@ __global__ void __cluster_dims__(C / 2, 1, 1) __launch_bounds__(kT, 1)
     sincospi(-2.0 * (double)(tid + 1) / (double)kM, &sn, &cs);
     wb1 = make_float2((float)cs, (float)sn);
   }
-  // radix-C step twiddle bases W_N^m of the thread's columns m = r CW + t + T u
-  float2 dbase[U];
+  // radix-C step twiddle bases W_N^m of the thread's columns m = r CW + t + T u;
+  // C = 2 keeps W_N^t and W_N^(t + T) only: W_N^(t + T u) = W_N^(t + T (u mod 2)) W_16^(u / 2)
+  constexpr int ND = C == 2 ? 2 : U;
+  float2 dbase[ND];
 #pragma unroll
-  for (int u = 0; u < U; ++u) {
+  for (int u = 0; u < ND; ++u) {
     double sn, cs;
     sincospi(-2.0 * (double)(r * CW + tid + kT * u) / (double)N, &sn, &cs);
     dbase[u] = make_float2((float)cs, (float)sn);
   }
+  auto dtw = [&](int u) -> float2 {  // u is a compile-time constant after unrolling
+    if constexpr (C != 2) {
+      return dbase[u];
+    } else {
+      const float2 b = dbase[u & 1];
+      switch (u >> 1) {
+        case 0: return b;
+        case 1: return mul_w16<1>(b);
+        case 2: return mul_w16<2>(b);
+        case 3: return mul_w16<3>(b);
+        case 4: return mul_w16<4>(b);
+        case 5: return mul_w16<5>(b);
+        case 6: return mul_w16<6>(b);
+        default: return mul_w16<7>(b);
+      }
+    }
+  };
   // every CTA of the cluster has started, zeroed its flag and built its
   // tables before any CTA stores into another's shared memory
   cl_sync();
@@ -215,7 +235,7 @@ __global__ void __cluster_dims__(C / 2, 1, 1) __launch_bounds__(kT, 1)
   const int sb = a2s - a1s;
   const int ovs = g0 ? a1s : a2s;   // overlap on the primary grid: [ovs, ovs + ov)
   const int qoff = g0 ? sb : -sb;   // secondary bin = primary bin + qoff (a multiple of C)
-  const int dq = -qoff / C;         // the primary bin of a secondary bin: row index + dq
+  const int dq = -qoff / C;         // the primary bin of a secondary bin: row index + dq (C > 2)
   const bool want_acf = (p.products & 1u) != 0;
   const bool want_xcf = (p.products & 2u) != 0;
   const bool ov_only = (p.products & 16u) != 0;
@@ -292,7 +312,7 @@ __global__ void __cluster_dims__(C / 2, 1, 1) __launch_bounds__(kT, 1)
           dft_c<C>(s);
 #pragma unroll
           for (int k = 0; k < C; ++k) z[k] = s[out_pos<C>(k)];
-          twiddle<C, 0>(z, dbase[ubase + u]);  // z[k] *= W_N^(m k)
+          twiddle<C, 0>(z, dtw(ubase + u));  // z[k] *= W_N^(m k)
           const int col = r * CW + tid + kT * (ubase + u);
 #pragma unroll
           for (int k = 0; k < C; ++k) {
@@ -363,88 +383,198 @@ __global__ void __cluster_dims__(C / 2, 1, 1) __launch_bounds__(kT, 1)
     float sn, cs;
     __sincosf((float)(C * kT) * F.dphi, &sn, &cs);
     const float2 rstep = make_float2(cs, sn);
-    // row: 0 = A (spectrum in Y, mirror in XA; row 0 is its own mirror),
-    //      1 = B (spectrum in XA, mirror in Y; row C/2 is its own mirror)
-    auto row_pass = [&](auto rb) {
-      constexpr int RB = decltype(rb)::value;
-      const int row = RB ? rowB : rowA;
-      // the rows' last radix-16 pass outputs (unpadded): Z[j] = Yo[j] + W^j Yo[j + M/2];
-      // the mirror row's upper half Z[c + M/2] = Ym[c] - W^c Ym[c + M/2] with
-      // W^c = -conj(W^(M/2 - c)), folded here instead of a radix-2 pass in place
-      const float2* Yo = RB ? XA : Y;
-      const float2* Ym = RB ? (r == 0 ? XA : Y) : (r == 0 ? Y : XA);
-      constexpr bool kSelf0Row = RB == 0;  // row 0 (CTA 0's row A) mirrors at M - j
-      float2* Q = RB ? QB : QA;
-      float2 prim[kJ];
+    if constexpr (C == 2) {
+      // Slot of primary bin kp's secondary spectrum: with both rows in the CTA,
+      // bin kp is row kp mod 2 at index kp / 2 (any band shift).
+      auto q_slot = [&](int kp) -> float2* {
+        return ((kp & 1) ? QB : QA) + (kp >> 1);
+      };
+      // split: the row's primary spectrum into prim, its secondary spectra into
+      // their primary bins' slots.
+      // row: 0 = A (spectrum in Y, mirror in XA; row 0 is its own mirror),
+      //      1 = B (spectrum in XA, mirror in Y; row C/2 is its own mirror)
+      auto split_row = [&](auto rb, float2 (&prim)[kJ], float2& prim_h) {
+        constexpr int RB = decltype(rb)::value;
+        const int row = RB ? rowB : rowA;
+        // the rows' last radix-16 pass outputs (unpadded): Z[j] = Yo[j] + W^j Yo[j + M/2];
+        // the mirror row's upper half Z[c + M/2] = Ym[c] - W^c Ym[c + M/2] with
+        // W^c = -conj(W^(M/2 - c)), folded here instead of a radix-2 pass in place
+        const float2* Yo = RB ? XA : Y;
+        const float2* Ym = RB ? (r == 0 ? XA : Y) : (r == 0 ? Y : XA);
+        constexpr bool kSelf0Row = RB == 0;  // row 0 (CTA 0's row A) mirrors at M - j
 #pragma unroll
-      for (int i = 0; i < kJ; ++i) {
-        const int j = tid + kT * i;
-        float2 wj, wj1;  // W_M^j = W_M^t W_16^i, W_M^(j+1) = W_M^(t+1) W_16^i
-        switch (i) {  // compile-time after unrolling
-          case 0: wj = tw.w[Geom<kM>::P16]; wj1 = wb1; break;
-          case 1: wj = mul_w16<1>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<1>(wb1); break;
-          case 2: wj = mul_w16<2>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<2>(wb1); break;
-          case 3: wj = mul_w16<3>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<3>(wb1); break;
-          case 4: wj = mul_w16<4>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<4>(wb1); break;
-          case 5: wj = mul_w16<5>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<5>(wb1); break;
-          case 6: wj = mul_w16<6>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<6>(wb1); break;
-          default: wj = mul_w16<7>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<7>(wb1); break;
+        for (int i = 0; i < kJ; ++i) {
+          const int j = tid + kT * i;
+          float2 wj, wj1;  // W_M^j = W_M^t W_16^i, W_M^(j+1) = W_M^(t+1) W_16^i
+          switch (i) {  // compile-time after unrolling
+            case 0: wj = tw.w[Geom<kM>::P16]; wj1 = wb1; break;
+            case 1: wj = mul_w16<1>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<1>(wb1); break;
+            case 2: wj = mul_w16<2>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<2>(wb1); break;
+            case 3: wj = mul_w16<3>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<3>(wb1); break;
+            case 4: wj = mul_w16<4>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<4>(wb1); break;
+            case 5: wj = mul_w16<5>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<5>(wb1); break;
+            case 6: wj = mul_w16<6>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<6>(wb1); break;
+            default: wj = mul_w16<7>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<7>(wb1); break;
+          }
+          const float2 u = cadd(Yo[j], cmul(wj, Yo[j + kM / 2]));  // Z[j]
+          // Z[N - k], k = C j + row: the mirror row's index M - 1 - j (row 0: M - j)
+          const bool self0 = kSelf0Row && r == 0;
+          const int c = self0 ? ((kM / 2 - j) & (kM / 2 - 1)) : kM / 2 - 1 - j;
+          float2 w = cadd(Ym[c], cmulc(Ym[c + kM / 2], self0 ? wj : wj1));
+          if (self0 && j == 0) w = u;  // bin 0 pairs with itself
+          prim[i] = make_float2(u.x + w.x, u.y - w.y);
+          const int kp = C * j + row - qoff;
+          if ((unsigned)(kp - ovs) < (unsigned)ov)
+            *q_slot(kp) = make_float2(sgn * (u.y + w.y), sgn * (w.x - u.x));
         }
-        const float2 u = cadd(Yo[j], cmul(wj, Yo[j + kM / 2]));  // Z[j]
-        // Z[N - k], k = C j + row: the mirror row's index M - 1 - j (row 0: M - j)
-        const bool self0 = kSelf0Row && r == 0;
-        const int c = self0 ? ((kM / 2 - j) & (kM / 2 - 1)) : kM / 2 - 1 - j;
-        float2 w = cadd(Ym[c], cmulc(Ym[c + kM / 2], self0 ? wj : wj1));
-        if (self0 && j == 0) w = u;  // bin 0 pairs with itself
-        prim[i] = make_float2(u.x + w.x, u.y - w.y);
-        const int kp = C * j + row - qoff;
-        if ((unsigned)(kp - ovs) < (unsigned)ov)
-          Q[j + dq] = make_float2(sgn * (u.y + w.y), sgn * (w.x - u.x));
-      }
-      float2 prim_h = make_float2(0.f, 0.f);
-      if (RB == 0 && half) {  // Z[N/2] = Y[0] - Y[M/2] pairs with itself
-        const float2 u = csub(Y[0], Y[kM / 2]);
-        prim_h = make_float2(2.f * u.x, 0.f);
-        const int kp = N / 2 - qoff;
-        if ((unsigned)(kp - ovs) < (unsigned)ov) Q[kM / 2 + dq] = make_float2(sgn * 2.f * u.y, 0.f);
-      }
-      // fringe x ramp rotation of the thread's bins of this row
-      __sincosf(fmaf((float)(C * tid + row - ovs), F.dphi, F.phi0), &sn, &cs);
-      float2 rot = cmul(F.fr_mix, make_float2(cs, sn));
-      float2 rhalf = make_float2(0.f, 0.f);
-      if (RB == 0 && half) {
-        __sincosf(fmaf((float)(N / 2 - ovs), F.dphi, F.phi0), &sn, &cs);
-        rhalf = cmul(F.fr_mix, make_float2(cs, sn));
-      }
-      __syncthreads();  // this row's secondary spectra are in place
-      float t[32];
-      tmem_ld32(taddr + (uint32_t)(32 * RB), t);
+        if (RB == 0 && half) {  // Z[N/2] = Y[0] - Y[M/2] pairs with itself
+          const float2 u = csub(Y[0], Y[kM / 2]);
+          prim_h = make_float2(2.f * u.x, 0.f);
+          const int kp = N / 2 - qoff;
+          if ((unsigned)(kp - ovs) < (unsigned)ov)
+            *q_slot(kp) = make_float2(sgn * 2.f * u.y, 0.f);
+        }
+      };
+      // accumulation of a row's bins into TMEM (its secondary spectra in place)
+      auto acc_row = [&](auto rb, const float2 (&prim)[kJ], float2 prim_h) {
+        constexpr int RB = decltype(rb)::value;
+        const int row = RB ? rowB : rowA;
+        const float2* Q = RB ? QB : QA;
+        // fringe x ramp rotation of the thread's bins of this row
+        __sincosf(fmaf((float)(C * tid + row - ovs), F.dphi, F.phi0), &sn, &cs);
+        float2 rot = cmul(F.fr_mix, make_float2(cs, sn));
+        float2 rhalf = make_float2(0.f, 0.f);
+        if (RB == 0 && half) {
+          __sincosf(fmaf((float)(N / 2 - ovs), F.dphi, F.phi0), &sn, &cs);
+          rhalf = cmul(F.fr_mix, make_float2(cs, sn));
+        }
+        float t[32];
+        tmem_ld32(taddr + (uint32_t)(32 * RB), t);
 #pragma unroll
-      for (int i = 0; i < kJ; ++i) {
-        const int j = tid + kT * i;
-        bin_acc(C * j + row, Q + j, prim[i], rot, &t[4 * i]);
-        rot = cmul(rot, rstep);
-      }
-      if (RB == 0 && half) bin_acc(N / 2, Q + kM / 2, prim_h, rhalf, acc_h);
-      if (flush_now) {
+        for (int i = 0; i < kJ; ++i) {
+          const int j = tid + kT * i;
+          bin_acc(C * j + row, Q + j, prim[i], rot, &t[4 * i]);
+          rot = cmul(rot, rstep);
+        }
+        if (RB == 0 && half) bin_acc(N / 2, Q + kM / 2, prim_h, rhalf, acc_h);
+        if (flush_now) {
 #pragma unroll
-        for (int i = 0; i < kJ; ++i)
+          for (int i = 0; i < kJ; ++i)
 #pragma unroll
-          for (int v = 0; v < 4; ++v) {
-            add_part(C * (tid + kT * i) + row, v, t[4 * i + v]);
-            t[4 * i + v] = 0.f;
+            for (int v = 0; v < 4; ++v) {
+              add_part(C * (tid + kT * i) + row, v, t[4 * i + v]);
+              t[4 * i + v] = 0.f;
+            }
+          if (RB == 0 && half)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+              add_part(N / 2, v, acc_h[v]);
+              acc_h[v] = 0.f;
+            }
+        }
+        tmem_st32(taddr + (uint32_t)(32 * RB), t);
+      };
+      const std::integral_constant<int, 0> kRowA{};
+      const std::integral_constant<int, 1> kRowB{};
+      // both rows in this CTA, an odd band shift: each row's secondary
+      // spectra land in the other row's slots, so both splits come first.
+      // Row A's split reads Y only and row B's XA only: row A's primary
+      // spectrum waits in Y while row B is split.
+      float2 prim[kJ], prim_h = make_float2(0.f, 0.f), unused = prim_h;
+      split_row(kRowA, prim, prim_h);
+      __syncthreads();  // every thread has read Y
+#pragma unroll
+      for (int i = 0; i < kJ; ++i) Y[tid + kT * i] = prim[i];
+      split_row(kRowB, prim, unused);
+      __syncthreads();  // both rows' secondary spectra are in place
+      acc_row(kRowB, prim, unused);
+#pragma unroll
+      for (int i = 0; i < kJ; ++i) prim[i] = Y[tid + kT * i];
+      acc_row(kRowA, prim, prim_h);
+    } else {
+      // row: 0 = A (spectrum in Y, mirror in XA; row 0 is its own mirror),
+      //      1 = B (spectrum in XA, mirror in Y; row C/2 is its own mirror)
+      auto row_pass = [&](auto rb) {
+        constexpr int RB = decltype(rb)::value;
+        const int row = RB ? rowB : rowA;
+        // the rows' last radix-16 pass outputs (unpadded): Z[j] = Yo[j] + W^j Yo[j + M/2];
+        // the mirror row's upper half Z[c + M/2] = Ym[c] - W^c Ym[c + M/2] with
+        // W^c = -conj(W^(M/2 - c)), folded here instead of a radix-2 pass in place
+        const float2* Yo = RB ? XA : Y;
+        const float2* Ym = RB ? (r == 0 ? XA : Y) : (r == 0 ? Y : XA);
+        constexpr bool kSelf0Row = RB == 0;  // row 0 (CTA 0's row A) mirrors at M - j
+        float2* Q = RB ? QB : QA;
+        float2 prim[kJ];
+#pragma unroll
+        for (int i = 0; i < kJ; ++i) {
+          const int j = tid + kT * i;
+          float2 wj, wj1;  // W_M^j = W_M^t W_16^i, W_M^(j+1) = W_M^(t+1) W_16^i
+          switch (i) {  // compile-time after unrolling
+            case 0: wj = tw.w[Geom<kM>::P16]; wj1 = wb1; break;
+            case 1: wj = mul_w16<1>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<1>(wb1); break;
+            case 2: wj = mul_w16<2>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<2>(wb1); break;
+            case 3: wj = mul_w16<3>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<3>(wb1); break;
+            case 4: wj = mul_w16<4>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<4>(wb1); break;
+            case 5: wj = mul_w16<5>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<5>(wb1); break;
+            case 6: wj = mul_w16<6>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<6>(wb1); break;
+            default: wj = mul_w16<7>(tw.w[Geom<kM>::P16]); wj1 = mul_w16<7>(wb1); break;
           }
-        if (RB == 0 && half)
+          const float2 u = cadd(Yo[j], cmul(wj, Yo[j + kM / 2]));  // Z[j]
+          // Z[N - k], k = C j + row: the mirror row's index M - 1 - j (row 0: M - j)
+          const bool self0 = kSelf0Row && r == 0;
+          const int c = self0 ? ((kM / 2 - j) & (kM / 2 - 1)) : kM / 2 - 1 - j;
+          float2 w = cadd(Ym[c], cmulc(Ym[c + kM / 2], self0 ? wj : wj1));
+          if (self0 && j == 0) w = u;  // bin 0 pairs with itself
+          prim[i] = make_float2(u.x + w.x, u.y - w.y);
+          const int kp = C * j + row - qoff;
+          if ((unsigned)(kp - ovs) < (unsigned)ov)
+            Q[j + dq] = make_float2(sgn * (u.y + w.y), sgn * (w.x - u.x));
+        }
+        float2 prim_h = make_float2(0.f, 0.f);
+        if (RB == 0 && half) {  // Z[N/2] = Y[0] - Y[M/2] pairs with itself
+          const float2 u = csub(Y[0], Y[kM / 2]);
+          prim_h = make_float2(2.f * u.x, 0.f);
+          const int kp = N / 2 - qoff;
+          if ((unsigned)(kp - ovs) < (unsigned)ov) Q[kM / 2 + dq] = make_float2(sgn * 2.f * u.y, 0.f);
+        }
+        // fringe x ramp rotation of the thread's bins of this row
+        __sincosf(fmaf((float)(C * tid + row - ovs), F.dphi, F.phi0), &sn, &cs);
+        float2 rot = cmul(F.fr_mix, make_float2(cs, sn));
+        float2 rhalf = make_float2(0.f, 0.f);
+        if (RB == 0 && half) {
+          __sincosf(fmaf((float)(N / 2 - ovs), F.dphi, F.phi0), &sn, &cs);
+          rhalf = cmul(F.fr_mix, make_float2(cs, sn));
+        }
+        __syncthreads();  // this row's secondary spectra are in place
+        float t[32];
+        tmem_ld32(taddr + (uint32_t)(32 * RB), t);
 #pragma unroll
-          for (int v = 0; v < 4; ++v) {
-            add_part(N / 2, v, acc_h[v]);
-            acc_h[v] = 0.f;
-          }
-      }
-      tmem_st32(taddr + (uint32_t)(32 * RB), t);
-    };
-    row_pass(std::integral_constant<int, 0>{});
-    row_pass(std::integral_constant<int, 1>{});
+        for (int i = 0; i < kJ; ++i) {
+          const int j = tid + kT * i;
+          bin_acc(C * j + row, Q + j, prim[i], rot, &t[4 * i]);
+          rot = cmul(rot, rstep);
+        }
+        if (RB == 0 && half) bin_acc(N / 2, Q + kM / 2, prim_h, rhalf, acc_h);
+        if (flush_now) {
+#pragma unroll
+          for (int i = 0; i < kJ; ++i)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+              add_part(C * (tid + kT * i) + row, v, t[4 * i + v]);
+              t[4 * i + v] = 0.f;
+            }
+          if (RB == 0 && half)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+              add_part(N / 2, v, acc_h[v]);
+              acc_h[v] = 0.f;
+            }
+        }
+        tmem_st32(taddr + (uint32_t)(32 * RB), t);
+      };
+      row_pass(std::integral_constant<int, 0>{});
+      row_pass(std::integral_constant<int, 1>{});
+    }
     if (flush_now) {
       first_flush = false;
       since_flush = 0;
@@ -511,15 +641,19 @@ int pair_capacity() {
 
 }  // namespace
 
+// FFT 32768 / 65536: band shifts that are a multiple of C.  FFT 16384 (C = 2,
+// both rows in one CTA): odd band shifts, where the two-row kernel does not
+// apply (an even shift keeps each bin's secondary spectrum in its own row).
 bool corr_pair_supported(uint32_t n, const CorrParams& p) {
-  const int c = n == 32768 ? 4 : (n == 65536 ? 8 : 0);
+  const int c = n == 16384 ? 2 : (n == 32768 ? 4 : (n == 65536 ? 8 : 0));
   if (c == 0 || p.st[0].bits > 2 || p.st[1].bits > 2) return false;
-  if (((p.a2s - p.a1s) % c) != 0) return false;
+  if (c == 2 ? ((p.a2s - p.a1s) & 1) == 0 : ((p.a2s - p.a1s) % c) != 0) return false;
   return corr_pair_capacity(n) > 0;
 }
 
 int corr_pair_capacity(uint32_t n) {
-  return n == 32768 ? pair_capacity<4>() : (n == 65536 ? pair_capacity<8>() : 0);
+  return n == 16384 ? pair_capacity<2>()
+                    : (n == 32768 ? pair_capacity<4>() : (n == 65536 ? pair_capacity<8>() : 0));
 }
 
 int corr_pair_count(uint32_t n, uint64_t nf) {
@@ -531,7 +665,10 @@ int corr_pair_count(uint32_t n, uint64_t nf) {
 cudaError_t launch_corr_pair(uint32_t n, const CorrParams& p, int clusters, cudaStream_t s) {
   const int bp = p.st[p.grid == 0 ? 0 : 1].bits, bs = p.st[p.grid == 0 ? 1 : 0].bits;
   cudaError_t e;
-  if (n == 32768) {
+  if (n == 16384) {
+    if ((e = pair_prepare<2>()) != cudaSuccess) return e;
+    corr_pair_kernel<2><<<clusters, kT, pr_smem_bytes(2, bp, bs), s>>>(p);
+  } else if (n == 32768) {
     if ((e = pair_prepare<4>()) != cudaSuccess) return e;
     corr_pair_kernel<4><<<2 * clusters, kT, pr_smem_bytes(4, bp, bs), s>>>(p);
   } else if (n == 65536) {

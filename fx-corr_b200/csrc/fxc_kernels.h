@@ -84,7 +84,8 @@ int corr_cluster_count(uint32_t n, uint64_t nf);  // clusters of a sector's laun
 cudaError_t launch_corr_cluster(uint32_t n, const CorrParams& p, int clusters, cudaStream_t s);
 // FFT 32768 / 65536 with 1- and 2-bit stations and a band shift that is a
 // multiple of C: clusters of C/2 CTAs, each owning a mirror pair of rows
-// (corr_pair.cu); partials [clusters][4][H].
+// (corr_pair.cu); FFT 16384 (C = 2) with 1- and 2-bit stations and an odd
+// band shift: both rows in one CTA.  Partials [clusters][4][H].
 bool corr_pair_supported(uint32_t n, const CorrParams& p);
 int corr_pair_capacity(uint32_t n);
 int corr_pair_count(uint32_t n, uint64_t nf);

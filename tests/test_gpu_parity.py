@@ -432,8 +432,13 @@ LARGE_CASES = [
     dict(fft=16384, band=(-40, 40, 8192, 0), grid=1, shuffle="generic", lsb2=True),
     dict(fft=16384, bits1=4, bits2=2, band=(12, 0, 8180, 12), grid=0, shuffle="pairswap",
          products=oracle.PROD_ACF | oracle.PROD_ACF_OVERLAP_ONLY | oracle.PROD_XCF),
-    # odd band shift: the cluster kernel, secondary spectra exchanged between CTAs
+    # odd band shift, 1- and 2-bit stations: both rows in one CTA, each row's
+    # secondary spectra in the other row's slots
     dict(fft=16384, band=(-7, 7, 8192, 0), grid=0, lsb1=True),
+    dict(fft=16384, band=(5, 0, 8187, 5), grid=1, bits1=1, bits2=2, shuffle="pairswap", lsb2=True,
+         products=oracle.PROD_ACF | oracle.PROD_ACF_OVERLAP_ONLY | oracle.PROD_XCF),
+    # odd band shift, 8-bit stations: the cluster kernel, secondary spectra
+    # exchanged between CTAs
     dict(fft=16384, band=(3, 0, 8190, 3), grid=1, bits1=8, bits2=8, shuffle="generic"),
     dict(fft=32768, band=(-6, 6, 16385, 0), grid=0, bits1=2, bits2=1, shuffle="sample2",
          lsb2=True),
