@@ -1,7 +1,8 @@
 // corr_pair.cu — correlation for FFT 32768 and 65536 (N = C * M, M = 8192,
 // C = 4, 8) with 1- and 2-bit stations and a band shift that is a multiple of
 // C: one thread-block cluster of C/2 CTAs per frame pair, each CTA owning a
-// mirror pair of rows.
+// mirror pair of rows.  FFT 16384 (C = 2) with an odd band shift: a cluster
+// of one CTA holding both rows.
 //
 // Same contract and decomposition as corr_cluster_kernel (src/main.rs:
 // 2491-2568 per frame pair; y_q[m] = W_N^(m q) sum_c z[m + M c] W_C^(c q),
@@ -11,10 +12,12 @@
 //     both rows from the CTA's own shared memory (no mirror exchange);
 //   * the radix-C step's rows that leave the CTA are (C - 2) of C (48 KB per
 //     row at C = 8 instead of 56 KB plus the 32 KB mirror half row);
-//   * a cluster has C/2 CTAs: 37 clusters of 4 fit the B200 where only 15
-//     clusters of 8 do (148 SMs instead of 120);
+//   * a cluster has C/2 CTAs: 33 clusters of 4 fit the B200 where only 15
+//     clusters of 8 do (132 SMs instead of 120), and 148 clusters of one;
 //   * the band-shifted secondary spectrum of a bin lies in the same row (the
-//     shift is a multiple of C), so it never leaves the CTA.
+//     shift is a multiple of C), so it never leaves the CTA; at C = 2 it may
+//     lie in the other row, which is in the same CTA: both rows are split
+//     before either is accumulated.
 // The accumulators of both rows' bins (32 f32 per thread and row) live in
 // tensor memory (TMEM, 256 columns of the SM's 512): registers could hold one
 // row's, not two, beside the FFT; each row's are loaded and stored once per
@@ -234,7 +237,7 @@ __global__ void __cluster_dims__(C / 2, 1, 1) __launch_bounds__(kT, 1)
   const int ov = a1e - a1s;
   const int sb = a2s - a1s;
   const int ovs = g0 ? a1s : a2s;   // overlap on the primary grid: [ovs, ovs + ov)
-  const int qoff = g0 ? sb : -sb;   // secondary bin = primary bin + qoff (a multiple of C)
+  const int qoff = g0 ? sb : -sb;   // secondary bin = primary bin + qoff (a multiple of C if C > 2)
   const int dq = -qoff / C;         // the primary bin of a secondary bin: row index + dq (C > 2)
   const bool want_acf = (p.products & 1u) != 0;
   const bool want_xcf = (p.products & 2u) != 0;
@@ -492,6 +495,8 @@ __global__ void __cluster_dims__(C / 2, 1, 1) __launch_bounds__(kT, 1)
       for (int i = 0; i < kJ; ++i) prim[i] = Y[tid + kT * i];
       acc_row(kRowA, prim, prim_h);
     } else {
+      // one row at a time (split, then accumulate), so that one row's primary
+      // spectrum is live at a time: these kernels run at the register limit.
       // row: 0 = A (spectrum in Y, mirror in XA; row 0 is its own mirror),
       //      1 = B (spectrum in XA, mirror in Y; row C/2 is its own mirror)
       auto row_pass = [&](auto rb) {
