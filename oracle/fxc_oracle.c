@@ -192,6 +192,8 @@ typedef struct {
   int radix[40];
   uint32_t ns[40];
   cf32* tw[40];
+  float* twr[40]; /* the same twiddles split: [(q - 1) * ns + k] */
+  float* twi[40];
   cf32* post; /* real-FFT split twiddles exp(-2 pi i k / (2n)), k < n */
 } cfft_plan;
 
@@ -211,12 +213,18 @@ static cfft_plan* plan_get(uint32_t n) {
     p->radix[p->npass] = r;
     p->ns[p->npass] = ns;
     cf32* tw = (cf32*)malloc(sizeof(cf32) * (size_t)ns * (size_t)(r - 1) + sizeof(cf32));
+    float* twr = (float*)malloc(sizeof(float) * ((size_t)ns * (size_t)(r - 1) + 1));
+    float* twi = (float*)malloc(sizeof(float) * ((size_t)ns * (size_t)(r - 1) + 1));
     for (uint32_t k = 0; k < ns; ++k)
       for (int q = 1; q < r; ++q) {
         double ang = -2.0 * ORC_PI * (double)k * (double)q / ((double)ns * (double)r);
         tw[k * (r - 1) + (q - 1)].re = (float)cos(ang);
         tw[k * (r - 1) + (q - 1)].im = (float)sin(ang);
+        twr[(size_t)(q - 1) * ns + k] = tw[k * (r - 1) + (q - 1)].re;
+        twi[(size_t)(q - 1) * ns + k] = tw[k * (r - 1) + (q - 1)].im;
       }
+    p->twr[p->npass] = twr;
+    p->twi[p->npass] = twi;
     p->tw[p->npass++] = tw;
     ns *= (uint32_t)r;
     rem /= (uint32_t)r;
@@ -280,6 +288,132 @@ static cf32* cfft_forward(const cfft_plan* p, cf32* a, cf32* b) {
   return in;
 }
 
+/* One radix-4 pass of cfft_forward on split (re, im) arrays: every
+ * operation and its order are those of cfft_forward, so the results are
+ * identical bit for bit.  The innermost loop walks k, the position inside a
+ * block of ns outputs, contiguously in its inputs and outputs (vectorised
+ * for ns >= 8); the first pass (ns = 1, no twiddles) loops over blocks. */
+static void pass4_split(size_t n, size_t ns, const float* restrict inr,
+                        const float* restrict ini, float* restrict outr, float* restrict outi,
+                        const float* restrict wr, const float* restrict wi) {
+  const size_t stride = n / 4;
+  if (ns == 1) {
+    for (size_t j = 0; j < stride; ++j) {
+      const float v0r = inr[j], v0i = ini[j], v1r = inr[j + stride], v1i = ini[j + stride];
+      const float v2r = inr[j + 2 * stride], v2i = ini[j + 2 * stride];
+      const float v3r = inr[j + 3 * stride], v3i = ini[j + 3 * stride];
+      const float t0r = v0r + v2r, t0i = v0i + v2i;
+      const float t1r = v0r - v2r, t1i = v0i - v2i;
+      const float t2r = v1r + v3r, t2i = v1i + v3i;
+      const float t3r = v1i - v3i, t3i = v3r - v1r; /* (v1 - v3) * (-i) */
+      outr[4 * j] = t0r + t2r;
+      outi[4 * j] = t0i + t2i;
+      outr[4 * j + 1] = t1r + t3r;
+      outi[4 * j + 1] = t1i + t3i;
+      outr[4 * j + 2] = t0r - t2r;
+      outi[4 * j + 2] = t0i - t2i;
+      outr[4 * j + 3] = t1r - t3r;
+      outi[4 * j + 3] = t1i - t3i;
+    }
+    return;
+  }
+  for (size_t blk = 0; blk < stride / ns; ++blk) {
+    const size_t j = blk * ns, od = blk * ns * 4;
+#pragma GCC ivdep
+    for (size_t k = 0; k < ns; ++k) {
+      const float v0r = inr[j + k], v0i = ini[j + k];
+      const float a1r = inr[j + k + stride], a1i = ini[j + k + stride];
+      const float a2r = inr[j + k + 2 * stride], a2i = ini[j + k + 2 * stride];
+      const float a3r = inr[j + k + 3 * stride], a3i = ini[j + k + 3 * stride];
+      const float v1r = a1r * wr[k] - a1i * wi[k];
+      const float v1i = a1r * wi[k] + a1i * wr[k];
+      const float v2r = a2r * wr[ns + k] - a2i * wi[ns + k];
+      const float v2i = a2r * wi[ns + k] + a2i * wr[ns + k];
+      const float v3r = a3r * wr[2 * ns + k] - a3i * wi[2 * ns + k];
+      const float v3i = a3r * wi[2 * ns + k] + a3i * wr[2 * ns + k];
+      const float t0r = v0r + v2r, t0i = v0i + v2i;
+      const float t1r = v0r - v2r, t1i = v0i - v2i;
+      const float t2r = v1r + v3r, t2i = v1i + v3i;
+      const float t3r = v1i - v3i, t3i = v3r - v1r; /* (v1 - v3) * (-i) */
+      outr[od + k] = t0r + t2r;
+      outi[od + k] = t0i + t2i;
+      outr[od + ns + k] = t1r + t3r;
+      outi[od + ns + k] = t1i + t3i;
+      outr[od + 2 * ns + k] = t0r - t2r;
+      outi[od + 2 * ns + k] = t0i - t2i;
+      outr[od + 3 * ns + k] = t1r - t3r;
+      outi[od + 3 * ns + k] = t1i - t3i;
+    }
+  }
+}
+
+/* The final radix-2 pass (odd log2 n) of cfft_forward on split arrays. */
+static void pass2_split(size_t n, size_t ns, const float* restrict inr,
+                        const float* restrict ini, float* restrict outr, float* restrict outi,
+                        const float* restrict wr, const float* restrict wi) {
+  const size_t stride = n / 2;
+  for (size_t blk = 0; blk < stride / ns; ++blk) {
+    const size_t j = blk * ns, od = blk * ns * 2;
+    for (size_t k = 0; k < ns; ++k) {
+      const float v0r = inr[j + k], v0i = ini[j + k];
+      float v1r = inr[j + k + stride], v1i = ini[j + k + stride];
+      if (ns > 1) {
+        const float ar1 = v1r, ai1 = v1i;
+        v1r = ar1 * wr[k] - ai1 * wi[k];
+        v1i = ar1 * wi[k] + ai1 * wr[k];
+      }
+      outr[od + k] = v0r + v1r;
+      outi[od + k] = v0i + v1i;
+      outr[od + k + ns] = v0r - v1r;
+      outi[od + k + ns] = v0i - v1i;
+    }
+  }
+}
+
+/* cfft_forward on split (re, im) arrays; returns the pair holding the result. */
+static void cfft_forward_split(const cfft_plan* p, float* ar, float* ai, float* br, float* bi,
+                               float** zr, float** zi) {
+  float* inr = ar;
+  float* ini = ai;
+  float* outr = br;
+  float* outi = bi;
+  for (int ps = 0; ps < p->npass; ++ps) {
+    if (p->radix[ps] == 4)
+      pass4_split(p->n, p->ns[ps], inr, ini, outr, outi, p->twr[ps], p->twi[ps]);
+    else
+      pass2_split(p->n, p->ns[ps], inr, ini, outr, outi, p->twr[ps], p->twi[ps]);
+    float* t = inr;
+    inr = outr;
+    outr = t;
+    t = ini;
+    ini = outi;
+    outi = t;
+  }
+  *zr = inr;
+  *zi = ini;
+}
+
+/* Bin k of the real FFT from the half-length complex FFT z (split arrays):
+ * E = (Z[kk] + conj Z[kc]) / 2, O = (Z[kk] - conj Z[kc]) / (2i), X[k] = E + w^k O. */
+static inline void split_bins(const float* restrict zr, const float* restrict zi,
+                              const cf32* restrict post, size_t m, size_t k, size_t kk, size_t kc,
+                              float* restrict out) {
+  (void)m;
+  const float zkr = zr[kk], zki = zi[kk];
+  const float zcr = zr[kc], zci = -zi[kc];
+  const float er = 0.5f * (zkr + zcr), ei = 0.5f * (zki + zci);
+  const float dr = zkr - zcr, di = zki - zci;
+  const float orr = 0.5f * di, oi = -0.5f * dr; /* d / (2i) */
+  const float wor = post[k].re * orr - post[k].im * oi;
+  const float woi = post[k].re * oi + post[k].im * orr;
+  out[2 * k] = er + wor;
+  out[2 * k + 1] = ei + woi;
+}
+
+/* Per-thread scratch of the real FFT (test infrastructure: kept until exit). */
+static __thread float* g_rfft_buf = NULL;
+static __thread size_t g_rfft_cap = 0;
+
 int orc_rfft_f32(uint32_t n, const float* in, float* out) {
   /* realfft R2C via an n/2-point complex FFT of (x[2m], x[2m+1]) and the
    * even/odd split X[k] = E[k] + exp(-2 pi i k / n) O[k], k = 0..n/2. */
@@ -287,24 +421,31 @@ int orc_rfft_f32(uint32_t n, const float* in, float* out) {
   const uint32_t m = n / 2;
   cfft_plan* p = plan_get(m);
   if (!p) return -1;
-  cf32* a = (cf32*)malloc(sizeof(cf32) * m * 2);
-  cf32* b = a + m;
+  if (g_rfft_cap < 4 * (size_t)m) {
+    free(g_rfft_buf);
+    g_rfft_buf = (float*)malloc(sizeof(float) * 4 * (size_t)m);
+    if (!g_rfft_buf) {
+      g_rfft_cap = 0;
+      return -1;
+    }
+    g_rfft_cap = 4 * (size_t)m;
+  }
+  float* ar = g_rfft_buf;
+  float* ai = ar + m;
+  float* br = ai + m;
+  float* bi = br + m;
   for (uint32_t i = 0; i < m; ++i) {
-    a[i].re = in[2 * i];
-    a[i].im = in[2 * i + 1];
+    ar[i] = in[2 * i];
+    ai[i] = in[2 * i + 1];
   }
-  cf32* z = cfft_forward(p, a, b);
-  for (uint32_t k = 0; k <= m; ++k) {
-    cf32 zk = z[k % m];
-    cf32 zc = cconj(z[(m - k) % m]);
-    cf32 e = {0.5f * (zk.re + zc.re), 0.5f * (zk.im + zc.im)};
-    cf32 d = {zk.re - zc.re, zk.im - zc.im};
-    cf32 o = {0.5f * d.im, -0.5f * d.re}; /* d / (2i) */
-    cf32 wo = cmul(p->post[k], o);
-    out[2 * k] = e.re + wo.re;
-    out[2 * k + 1] = e.im + wo.im;
-  }
-  free(a);
+  float *zr, *zi;
+  cfft_forward_split(p, ar, ai, br, bi, &zr, &zi);
+  /* X[k] from Z[k mod m] and conj Z[(m - k) mod m]: k = 0 and k = m both pair
+   * Z[0] with itself, 0 < k < m pairs Z[k] with Z[m - k] */
+  const cf32* restrict post = p->post;
+  split_bins(zr, zi, post, m, 0, 0, 0, out);
+  for (size_t k = 1; k < m; ++k) split_bins(zr, zi, post, m, k, k, m - k, out);
+  split_bins(zr, zi, post, m, m, 0, 0, out);
   return 0;
 }
 
