@@ -168,6 +168,18 @@ def test_rfft_kat(oracle_lib):
     assert np.abs(oracle.c_irfft(oracle.c_rfft(x), 256) - x).max() < 1e-5
 
 
+@pytest.mark.parametrize("n", [2, 4, 8, 32, 128, 512])
+def test_rfft_small_sizes(oracle_lib, n):
+    """The real FFT's edge shapes: half-length transforms of 1, 2 and 4 points
+    (no radix-4 pass, a lone radix-2 pass, the first pass only) and the
+    first passes of the vectorised form."""
+    x = np.random.default_rng(n).standard_normal(n).astype(np.float32)
+    s = oracle.c_rfft(x)
+    r = np.fft.rfft(x.astype(np.float64))
+    assert s.shape == r.shape
+    assert np.abs(s - r).max() / max(np.abs(r).max(), 1e-30) < 5e-7
+
+
 @pytest.mark.parametrize("n", [1024, 4096, 8192, 65536])
 def test_rfft_matches_fp64(oracle_lib, n):
     x = np.random.default_rng(n).standard_normal(n).astype(np.float32)
