@@ -34,7 +34,8 @@ def injection(fxc_lib):
 
 
 # FFT 8192 and 16384 (even band shift): the fold kernels; 16384 with an odd
-# band shift and 65536: the cluster kernel, whose CTAs stop together
+# band shift (2-bit stations): the one-CTA pair kernel; 65536 (a band shift
+# that is a multiple of 8): the pair kernel, whose clusters' CTAs stop together
 @pytest.mark.parametrize("fft,sb", [(8192, 128), (16384, 128), (16384, 129), (65536, 136)])
 def test_bounded_wait_runs_out_and_is_reported(engine, fxc_lib, injection, fft, sb):
     scan = make_scan(fft=fft, fs=1024e6, shuffle="generic", lsb1=True,
